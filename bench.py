@@ -1,0 +1,313 @@
+"""Benchmark of the UMAP hot path on B200: end-to-end seconds and SGD edge-updates/s.
+
+Workload (default): 1,000,000 observations x 50 dims, float32 Gaussian mixture
+of 100 clusters (centres N(0, 25 I), within-cluster sd 1, Dirichlet(1)
+weights), exact kNN with k = 15, 2-d output, 200 epochs, default Options
+otherwise.  Seeded synthetic data (no public dataset is named).
+
+One step = umappp's initialize(data, builder, ...) + Status::run() on the
+whole data set: device kNN, similarities, fuzzy union, initial layout,
+schedule and 200 SGD epochs.
+
+  value       seconds per step with the data already in HBM (device pointers
+              passed to the C ABI); time on the device with CUDA events around
+              the step, max over ranks.
+  e2e         the same through the public API with pageable->pinned host
+              buffers: the H2D copy of the data and the D2H copy of the
+              embedding are inside the timed region.
+  --impl reference   times the reference (libscran/umappp headers compiled in
+              oracle/_ref) on the host cores on a bounded sample and scales it
+              to the full workload (see cpu_sample()).
+
+Launch: python bench.py [--gpus N --steps K --warmup W]; for N > 1 under
+torchrun, each rank runs an independent replica (UMAP's SGD has no exchange
+step), scaling "weak".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    # name: (n, dim, clusters, centre_sd, weights, k, epochs)
+    "mixture_1m": (1_000_000, 50, 100, 5.0, "dirichlet", 15, 200),
+    "mixture_100k": (100_000, 50, 20, 4.0, "equal", 15, 500),
+    "small_2k": (2_000, 10, 1, 0.0, "equal", 15, 500),
+}
+METRIC = "end-to-end s & SGD edge-updates/s, 1M pts; FP32/batched vs plain at equal trust"
+
+
+def make_data(cfg: str, seed: int = 20241203) -> np.ndarray:
+    n, dim, nc, sd, weights, _, _ = CONFIGS[cfg]
+    rng = np.random.default_rng(seed)
+    centres = rng.normal(0.0, sd, size=(nc, dim)).astype(np.float32)
+    p = rng.dirichlet(np.ones(nc)) if weights == "dirichlet" else np.full(nc, 1.0 / nc)
+    labels = rng.choice(nc, size=n, p=p)
+    out = rng.standard_normal(size=(n, dim), dtype=np.float32)
+    out += centres[labels]
+    return out
+
+
+def load_peaks() -> dict:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return {"hbm_gbs": d["hbm_gbs"], "bf16_tflops": d["bf16_tflops"], "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv") if os.path.isdir(
+            os.path.join(ROOT, "gpurun_out")) else f"/tmp/umapb_clocks_{os.getpid()}.csv"
+        self.index = index
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        try:
+            self.f.close()
+        except Exception:
+            pass
+
+    def summary(self) -> dict:
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except Exception:
+            rows = []
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for name, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(name)
+            except Exception:
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------ our arm ---
+
+def run_ours(args, rank: int, world: int) -> dict | None:
+    import torch
+    import umappp_b200 as U
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    n, dim, _, _, _, k, epochs = CONFIGS[args.config]
+    X = make_data(args.config, seed=20241203 + rank)
+    opt = U.Options(num_neighbors=k, num_epochs=epochs)
+
+    d_data = torch.from_numpy(X).to(dev)
+    d_emb = torch.zeros((n, 2), dtype=torch.float32, device=dev)
+    h_data = torch.from_numpy(X).pin_memory()
+    h_emb = torch.zeros((n, 2), dtype=torch.float32).pin_memory()
+
+    def step_device():
+        st = U.initialize_from_data(d_data, 2, d_emb, opt)
+        st.run(d_emb)
+        return st
+
+    def step_host():
+        st = U.initialize_from_data(h_data.numpy(), 2, h_emb.numpy(), opt)
+        st.run(h_emb.numpy())
+        return st
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def timed(fn, steps):
+        barrier()
+        l0 = U.lib().umapb_launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        last = None
+        for _ in range(steps):
+            last = fn()
+        e1.record()
+        barrier()
+        ms = e0.elapsed_time(e1) / steps
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, last, U.lib().umapb_launch_count() - l0
+
+    for _ in range(args.warmup):
+        step_device()
+    with ClockSampler(dev.index) as clk:
+        ms, st, launches = timed(step_device, args.steps)
+    clocks = clk.summary()
+    stages = st.stage_ms()
+    counts = st.schedule_counts()
+    firing = int(counts[:, 0].sum())
+    negs = int(counts[:, 1].sum())
+    nnz = st.num_edges()
+    sgd_ms = stages["sgd"]
+    for _ in range(max(1, args.warmup // 2)):
+        step_host()
+    e2e_ms, _, _ = timed(step_host, args.steps)
+
+    peaks = load_peaks()
+    # SGD roofline (algorithmic bytes per epoch: 4 nnz + 56 F + 8 N_neg, F and N_neg exact)
+    sgd_bytes = 4.0 * nnz * epochs + 56.0 * firing + 8.0 * negs
+    sgd_gbs = sgd_bytes / (sgd_ms * 1e-3) / 1e9
+    knn_flops = 2.0 * n * n * dim
+    knn_tflops = knn_flops / (stages["knn"] * 1e-3) / 1e12
+    out = {
+        "metric": METRIC, "value": round(ms / 1e3, 4), "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Gaussian mixture)",
+        "config": {"workload": f"{args.config}: n={n} dim={dim} k={k} out_dim=2 epochs={epochs}",
+                   "l2": "inputs (200 MB data) larger than L2", "parallelism": f"replicas x{world}"},
+        "sgd_edge_updates_per_s": round(firing / (sgd_ms * 1e-3), 1),
+        "stage_ms": {k_: round(v, 3) for k_, v in stages.items()},
+        "roofline": {"bound": "hbm", "kernel": "sgd_epoch_2d_f32", "achieved": round(sgd_gbs, 1),
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": round(sgd_gbs / peaks["hbm_gbs"], 4),
+                     "traffic": None, "peak_source": peaks["source"],
+                     "note": "algorithmic bytes 4*nnz*epochs + 56*F + 8*N_neg over the SGD stage time"},
+        "knn": {"kernel": "knn (device)", "achieved_tflops": round(knn_tflops, 2),
+                "peak_bf16_tflops": peaks["bf16_tflops"], "algorithmic_flops": knn_flops},
+        "e2e": {"value": round(e2e_ms / 1e3, 4), "unit": "s", "h2d_bytes_per_step": int(n * dim * 4 + n * 2 * 4),
+                "d2h_bytes_per_step": int(2 * n * 2 * 4)},
+        "gpu_launches": int(launches // max(args.steps, 1)),
+        "clocks": clocks,
+        "schedule": {"nnz": int(nnz), "firing_edges": firing, "negative_samples": negs},
+    }
+    return out
+
+
+# --------------------------------------------------- reference on CPU ---
+
+def cpu_sample(cfg: str, budget_queries: int = 1000, sub_n: int = 50_000, sgd_epochs: int = 10) -> dict:
+    """Times the reference (oracle/_ref) on the host cores and scales it to the full workload:
+    - kNN: the stand-in exact brute force on the full data for 'budget_queries'
+      queries, scaled by n / queries (the cost is linear in queries);
+    - similarities, union, initial layout, schedule: the reference's stages on a
+      'sub_n'-point sample of the same mixture (its own exact kNN graph), scaled
+      by n / sub_n (each is linear in the number of edges);
+    - SGD: the first 'sgd_epochs' epochs of optimize_layout_parallel on that
+      sample, scaled by (epochs / sgd_epochs) * (n / sub_n)."""
+    import ctypes
+
+    import oracle
+
+    R = oracle.ref()
+    R.ref_pipeline_timed_f32.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+    n, dim, _, _, _, k, epochs = CONFIGS[cfg]
+    cores = os.cpu_count() or 1
+    X = make_data(cfg)
+    q = min(budget_queries, n)
+    t0 = time.perf_counter()
+    oracle.ref_knn(X, k, qstart=0, qcount=q, nthreads=cores)
+    t_knn = (time.perf_counter() - t0) * n / q
+    m = min(sub_n, n)
+    rng = np.random.default_rng(7)
+    S = np.ascontiguousarray(X[rng.choice(n, size=m, replace=False)])
+    emb = np.zeros((m, 2), dtype=np.float32)
+    secs = np.zeros(6, dtype=np.float64)
+    e_s = min(sgd_epochs, epochs)
+    R.ref_pipeline_timed_f32(dim, m, S.ctypes.data, k, epochs, e_s, cores, emb.ctypes.data, secs.ctypes.data)
+    scale = n / m
+    stages = {"knn": t_knn, "similarities": secs[1] * scale, "union": secs[2] * scale, "init": secs[3] * scale,
+              "epochs": secs[4] * scale, "sgd": secs[5] * scale * epochs / e_s}
+    total = sum(stages.values())
+    return {"value": round(total, 2), "unit": "s", "cores": cores, "kind": "reference",
+            "stages_s": {k_: round(v, 2) for k_, v in stages.items()},
+            "sample": f"kNN: {q} queries over all {n} points x{n // q}; other stages: {m}-point sample x{scale:g}; "
+                      f"SGD: {e_s} of {epochs} epochs x{epochs / e_s:g} (num_threads={cores})"}
+
+
+def run_reference(args, rank: int) -> dict | None:
+    if rank != 0:
+        return None
+    n, dim, _, _, _, k, epochs = CONFIGS[args.config]
+    vals = []
+    cb = None
+    for _ in range(args.warmup and 1 or 0):
+        pass
+    for _ in range(max(args.steps, 1)):
+        cb = cpu_sample(args.config)
+        vals.append(cb["value"])
+    v = float(np.median(vals))
+    cb["value"] = v
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Gaussian mixture)",
+            "config": {"workload": f"{args.config}: n={n} dim={dim} k={k} out_dim=2 epochs={epochs}"},
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="mixture_1m", choices=sorted(CONFIGS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    if args.impl == "reference":
+        out = run_reference(args, rank)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        return
+
+    import torch
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        out = run_ours(args, rank, world)
+        if rank == 0 and out is not None:
+            if world == 1 and not args.no_cpu_baseline:
+                out["cpu_baseline"] = cpu_sample(args.config)
+            print(json.dumps(out), flush=True)
+    finally:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,272 @@
+/*
+ * umapb.h -- C ABI of the B200 (sm_100a) UMAP library libumappp_b200.so.
+ *
+ * Every entry point is plain C: pointers, sizes and an int status.  Pointer
+ * arguments may be host memory (pageable or pinned) or device memory on the
+ * current CUDA device; the library detects which and copies as needed.
+ * Layouts follow the reference (libscran/umappp v3.3.2):
+ *   - data and embeddings are column-major with observations as columns,
+ *     i.e. observation i occupies [i * dim, (i + 1) * dim)
+ *     (include/umappp/initialize.hpp:58-63,150-152);
+ *   - neighbour lists and graphs are CSR: row i holds
+ *     indices/values[row_ptr[i] .. row_ptr[i + 1]) with int64 row pointers and
+ *     int32 indices; neighbour rows are sorted by increasing distance
+ *     (include/umappp/NeighborList.hpp:24-29).
+ * dtype selects the reference's Float_ template argument (UMAPB_F32 = float,
+ * UMAPB_F64 = double); value arrays then hold that type.
+ *
+ * Errors: every function returns UMAPB_OK or an error code and leaves a
+ * message for umapb_last_error() (per calling thread).  Nothing throws and no
+ * call falls back to the CPU: without a usable sm_100 device the calls fail
+ * with UMAPB_ERR_NO_DEVICE.
+ */
+#ifndef UMAPB_H
+#define UMAPB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define UMAPB_VERSION 100
+
+enum umapb_code {
+    UMAPB_OK = 0,
+    UMAPB_ERR_INVALID = 1,        /* bad argument (sizes, layout, options) */
+    UMAPB_ERR_OOM = 2,            /* device allocation failed */
+    UMAPB_ERR_CUDA = 3,           /* CUDA runtime error */
+    UMAPB_ERR_DEVICE_TIMEOUT = 4, /* a bounded device-side wait gave up */
+    UMAPB_ERR_OVERFLOW = 5,       /* a size or cast would overflow (sanisizer's role) */
+    UMAPB_ERR_NO_DEVICE = 6       /* no usable CUDA device */
+};
+
+enum umapb_dtype { UMAPB_F32 = 0, UMAPB_F64 = 1 };
+
+/* Mirrors umappp::InitializeMethod (include/umappp/Options.hpp:27). */
+enum umapb_init_method { UMAPB_INIT_SPECTRAL = 0, UMAPB_INIT_RANDOM = 1, UMAPB_INIT_NONE = 2 };
+
+/*
+ * Mirrors umappp::Options (include/umappp/Options.hpp:37-218) field for field.
+ * std::optional fields carry a has_* flag.  irlba_* replace the
+ * irlba::Options member (Options.hpp:110); num_threads* are accepted and
+ * ignored (the device replaces the CPU thread pools).
+ */
+typedef struct umapb_options {
+    double local_connectivity;               /* Options.hpp:43  default 1 */
+    double bandwidth;                        /* :49  default 1 */
+    double mix_ratio;                        /* :57  default 1 */
+    double spread;                           /* :63  default 1 */
+    double min_dist;                         /* :71  default 0.1 */
+    double a;                                /* :79  optional */
+    double b;                                /* :87  optional */
+    int has_a;
+    int has_b;
+    double repulsion_strength;               /* :93  default 1 */
+    int initialize_method;                   /* :98  default SPECTRAL */
+    int initialize_random_on_spectral_fail;  /* :105 default 1 */
+    int irlba_extra_work;                    /* Krylov basis size = num_dim + 1 + max(extra, num_dim + 1) + 8; default 7 */
+    int irlba_max_iterations;                /* restart cap, default 1000 */
+    double irlba_convergence_tolerance;      /* residual <= tol * largest eigenvalue, default 1e-6 */
+    double initialize_spectral_scale;        /* :118 default 10 */
+    int initialize_spectral_jitter;          /* :125 default 0 */
+    double initialize_spectral_jitter_sd;    /* :131 default 1e-4 */
+    double initialize_random_scale;          /* :139 default 10 */
+    uint64_t initialize_seed;                /* :147 default 9876543210 */
+    int num_epochs;                          /* :159 optional */
+    int has_num_epochs;
+    double learning_rate;                    /* :165 default 1 */
+    double negative_sample_rate;             /* :171 default 5 */
+    int num_neighbors;                       /* :178 default 15 */
+    uint64_t optimize_seed;                  /* :183 default 1234567890 */
+    int num_threads;                         /* :192 ignored */
+    int num_threads_spectral;                /* :201 ignored */
+    int num_threads_optimize;                /* :217 ignored */
+} umapb_options;
+
+/* Fills the reference's defaults (Options.hpp:37-218). */
+void umapb_options_init(umapb_options* opt);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* umapb_last_error(void);
+
+int umapb_version(void);
+
+/* sizeof(umapb_options), for bindings that mirror the struct. */
+size_t umapb_options_size(void);
+
+/* Number of kernels this library has launched in this process (all threads). */
+int64_t umapb_launch_count(void);
+
+/* ------------------------------------------------------------------ Status */
+
+typedef struct umapb_status umapb_status;
+
+/*
+ * umappp::initialize(NeighborList, num_dim, embedding, Options)
+ * (include/umappp/initialize.hpp:69-119): similarities, fuzzy union,
+ * initial layout (spectral / random / none, written into 'embedding'),
+ * a/b fit, epoch count and per-edge schedule.  'embedding' holds
+ * num_obs * num_dim values of dtype.  On success *out owns the state.
+ */
+int umapb_initialize_neighbors(int dtype, int32_t num_obs, const int64_t* row_ptr, const int32_t* indices,
+                               const void* distances, size_t num_dim, void* embedding, const umapb_options* opt,
+                               umapb_status** out);
+
+/*
+ * umappp::initialize(data_dim, num_obs, data, builder, num_dim, embedding,
+ * Options) (include/umappp/initialize.hpp:165-177) with an exact Euclidean
+ * neighbour search on the device as the builder: opt->num_neighbors
+ * neighbours per observation (self excluded), then as above.
+ */
+int umapb_initialize_data(int dtype, size_t data_dim, int32_t num_obs, const void* data, size_t num_dim,
+                          void* embedding, const umapb_options* opt, umapb_status** out);
+
+/*
+ * Status::run(embedding, epoch_limit) (include/umappp/Status.hpp:101-128):
+ * advances the layout in 'embedding' (read on entry, written on exit) from
+ * epoch() to epoch_limit.  epoch_limit < 0 means num_epochs()
+ * (Status::run(embedding), Status.hpp:138-140).
+ */
+int umapb_status_run(umapb_status* st, void* embedding, int epoch_limit);
+
+int umapb_status_epoch(const umapb_status* st);                 /* Status.hpp:63-65 */
+int umapb_status_num_epochs(const umapb_status* st);            /* Status.hpp:71-73 */
+int32_t umapb_status_num_observations(const umapb_status* st);  /* Status.hpp:78-80 */
+size_t umapb_status_num_dimensions(const umapb_status* st);     /* Status.hpp:56-58 */
+double umapb_status_a(const umapb_status* st);                  /* the a and b in use */
+double umapb_status_b(const umapb_status* st);
+int64_t umapb_status_num_edges(const umapb_status* st);
+
+/*
+ * Status::get_epoch_data() (Status.hpp:52-54, EpochData optimize_layout.hpp:27-45)
+ * at the current epoch: row_ptr[n + 1], targets[nnz] and the dtype arrays
+ * epochs_per_sample, epoch_of_next_sample, epoch_of_next_negative_sample
+ * (any of them may be NULL).
+ */
+int umapb_status_get_epoch_data(const umapb_status* st, int64_t* row_ptr, int32_t* targets, void* epochs_per_sample,
+                                void* epoch_of_next_sample, void* epoch_of_next_negative_sample);
+
+/*
+ * Exact per-epoch counts of the deterministic schedule over [first, last):
+ * counts[2 * e] = firing edges, counts[2 * e + 1] = negative samples drawn
+ * (self-samples included, as the reference draws and then skips them).
+ */
+int umapb_status_schedule_counts(const umapb_status* st, int first, int last, int64_t* counts);
+
+/*
+ * Device milliseconds of the stages of the last initialize / run on this
+ * status, in the order: knn, similarities, union, init, epochs, schedule,
+ * sgd.  'count' entries are written (at most 7).
+ */
+int umapb_status_stage_ms(const umapb_status* st, double* ms, int count);
+
+void umapb_status_free(umapb_status* st);
+
+/* ----------------------------------------------------------- stage entries */
+
+/*
+ * Exact Euclidean k-nearest neighbours of every observation among all
+ * others (the knncolle search called at include/umappp/initialize.hpp:140):
+ * out_indices and out_distances are num_obs x k, sorted by increasing
+ * distance, ties by index.  For F32 data the candidates are found with
+ * split-precision tensor-core distances and the k-th boundary is rescored in
+ * FP64; for F64 data distances are computed in FP64.  k must be below num_obs.
+ */
+int umapb_knn(int dtype, size_t data_dim, int32_t num_obs, const void* data, int k, int32_t* out_indices,
+              void* out_distances);
+
+/*
+ * neighbor_similarities (include/umappp/neighbor_similarities.hpp:53-207):
+ * replaces the distances of each CSR row by membership weights in place.
+ * rho_out / sigma_out (may be NULL) receive per-row rho and sigma as double
+ * (NaN for rows the reference returns early).  use_newton selects the
+ * Newton-with-bisection search (the default) or bisection only.
+ */
+int umapb_neighbor_similarities(int dtype, int32_t num_obs, const int64_t* row_ptr, void* distances,
+                                double local_connectivity, double bandwidth, double min_k_dist_scale, int use_newton,
+                                double* rho_out, double* sigma_out);
+
+/*
+ * combine_neighbor_sets (include/umappp/combine_neighbor_sets.hpp:16-99):
+ * symmetrises a weighted CSR neighbour list into out_* (rows sorted by
+ * index).  out_indices/out_weights must hold 'capacity' entries
+ * (2 * row_ptr[num_obs] always suffices); *out_nnz receives the count.
+ */
+int umapb_combine_neighbor_sets(int dtype, int32_t num_obs, const int64_t* row_ptr, const int32_t* indices,
+                                const void* weights, double mix_ratio, int64_t* out_row_ptr, int32_t* out_indices,
+                                void* out_weights, int64_t capacity, int64_t* out_nnz);
+
+/*
+ * similarities_to_epochs (include/umappp/optimize_layout.hpp:47-92): keeps
+ * edges with weight >= max / num_epochs and writes the per-edge schedule.
+ * Output arrays must hold row_ptr[num_obs] entries; *out_nnz receives the
+ * kept count.
+ */
+int umapb_similarities_to_epochs(int dtype, int32_t num_obs, const int64_t* row_ptr, const int32_t* indices,
+                                 const void* weights, int num_epochs, double negative_sample_rate,
+                                 int64_t* out_row_ptr, int32_t* out_targets, void* epochs_per_sample,
+                                 void* epoch_of_next_sample, void* epoch_of_next_negative_sample, int64_t* out_nnz);
+
+/* has_multiple_components (include/umappp/spectral_init.hpp:142-168); *out = 0 or 1. */
+int umapb_has_multiple_components(int32_t num_obs, const int64_t* row_ptr, const int32_t* indices, int* out);
+
+/*
+ * spectral_init (include/umappp/spectral_init.hpp:171-207): *ok = 1 and the
+ * scaled eigenvectors of the normalised Laplacian in 'embedding'
+ * (num_obs x num_dim), or *ok = 0 (several components / no convergence,
+ * embedding untouched).  evals_out (may be NULL) receives num_dim + 1
+ * eigenvalues of I + D^-1/2 W D^-1/2 in decreasing order.
+ */
+int umapb_spectral_init(int dtype, int32_t num_obs, const int64_t* row_ptr, const int32_t* indices,
+                        const void* weights, size_t num_dim, void* embedding, int extra_work, int max_iterations,
+                        double tolerance, double scale, int jitter, double jitter_sd, uint64_t seed, int* ok,
+                        double* evals_out);
+
+/* random_init (include/umappp/spectral_init.hpp:209-225): uniform on (-scale, scale). */
+int umapb_random_init(int dtype, int32_t num_obs, size_t num_dim, void* embedding, uint64_t seed, double scale);
+
+/* find_ab (include/umappp/find_ab.hpp:44-168). */
+int umapb_find_ab(double spread, double min_dist, double* a, double* b);
+
+/* choose_num_epochs (include/umappp/initialize.hpp:27-47). */
+int umapb_choose_num_epochs(int has_value, int value, int64_t num_obs);
+
+/*
+ * optimize_layout (include/umappp/optimize_layout.hpp:116-185) on the device
+ * from the given schedule state: advances epochs [*current_epoch,
+ * epoch_limit), updating the embedding and epoch_of_next_* in place and
+ * *current_epoch.  Negative samples come from a counter-based generator keyed
+ * by (seed, epoch, edge), so the result does not depend on how the epochs
+ * are split across calls.
+ */
+int umapb_optimize_layout(int dtype, size_t num_dim, void* embedding, int32_t num_obs, const int64_t* row_ptr,
+                          const int32_t* targets, const void* epochs_per_sample, void* epoch_of_next_sample,
+                          void* epoch_of_next_negative_sample, double negative_sample_rate, int total_epochs,
+                          int* current_epoch, double a, double b, double gamma, double learning_rate, uint64_t seed,
+                          int epoch_limit);
+
+/* ----------------------------------------------------------------- adjoint */
+
+/*
+ * Loss and gradient of the UMAP fuzzy cross-entropy (no counterpart in the
+ * reference, which only applies its per-edge derivatives,
+ * include/umappp/optimize_layout.hpp:148-149,171):
+ *   L = sum over stored edges (i -> j, w) of
+ *       w * (-log q) + (1 - w) * (-log(1 - q)) [+ w log w + (1 - w) log(1 - w) if with_constant]
+ *   q = 1 / (1 + a d^(2b)),  d = |y_i - y_j|.
+ * With eps_rep > 0 the repulsive derivative uses 1 / (d^2 + eps_rep) in place
+ * of 1 / d^2, as the reference's step does (eps 0.001).  Outputs: *loss,
+ * grad_embedding (num_obs x num_dim, may be NULL), grad_ab[2] = dL/da, dL/db
+ * (may be NULL).  Accumulation is FP64 for both dtypes.
+ */
+int umapb_loss_grad(int dtype, size_t num_dim, const void* embedding, int32_t num_obs, const int64_t* row_ptr,
+                    const int32_t* indices, const void* weights, double a, double b, double eps_rep,
+                    int with_constant, double* loss, void* grad_embedding, double* grad_ab);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

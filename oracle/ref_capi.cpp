@@ -272,4 +272,59 @@ REF_FLOAT_FUNCS(f32, float)
 // Size of the options struct, so the Python side can check its mirror.
 int ref_options_size() { return static_cast<int>(sizeof(RefOptions)); }
 
+// The stages of initialize(data, builder, ...) and Status::run
+// (include/umappp/initialize.hpp:69-119,165-177; Status.hpp:101-128) called
+// one by one through the reference's own functions, timed in seconds:
+// secs[0] kNN, [1] similarities, [2] union, [3] initial layout, [4] a/b +
+// epochs, [5] the first 'sgd_epochs' epochs of optimize_layout(_parallel).
+// The data is float, n x dim; the embedding n x 2.
+int ref_pipeline_timed_f32(int dim, int n, const float* data, int k, int num_epochs, int sgd_epochs, int nthreads,
+                           float* embedding, double* secs) {
+    REF_TRY({
+        using clock = std::chrono::steady_clock;
+        umappp::Options opt;
+        opt.num_neighbors = k;
+        opt.num_epochs = num_epochs;
+        opt.num_threads = nthreads;
+        opt.num_threads_spectral = nthreads;
+        opt.num_threads_optimize = nthreads;
+        auto t0 = clock::now();
+        knncolle::BruteforcePrebuilt<int, float, float> index(static_cast<std::size_t>(dim), n, data);
+        auto x = knncolle::find_nearest_neighbors(index, k, nthreads);
+        secs[0] = seconds_since(t0);
+
+        t0 = clock::now();
+        umappp::NeighborSimilaritiesOptions<float> nsopt;
+        nsopt.num_threads = nthreads;
+        umappp::neighbor_similarities(x, nsopt);
+        secs[1] = seconds_since(t0);
+
+        t0 = clock::now();
+        umappp::combine_neighbor_sets(x, 1.0f);
+        secs[2] = seconds_since(t0);
+
+        t0 = clock::now();
+        const bool ok = umappp::spectral_init(x, 2, embedding, opt.initialize_spectral_irlba_options, nthreads,
+                                              opt.initialize_spectral_scale, false, 0.0, opt.initialize_seed);
+        if (!ok) umappp::random_init<int, float>(n, 2, embedding, opt.initialize_seed, opt.initialize_random_scale);
+        secs[3] = seconds_since(t0);
+
+        t0 = clock::now();
+        const auto ab = umappp::find_ab(opt.spread, opt.min_dist);
+        auto ep = umappp::similarities_to_epochs<int, float>(x, num_epochs, static_cast<float>(opt.negative_sample_rate));
+        secs[4] = seconds_since(t0);
+
+        t0 = clock::now();
+        std::mt19937_64 rng(opt.optimize_seed);
+        if (nthreads <= 1) {
+            umappp::optimize_layout<int, float>(2, embedding, ep, ab.first, ab.second, 1.0f, 1.0f, rng, sgd_epochs);
+        } else {
+            umappp::optimize_layout_parallel<int, float>(2, embedding, ep, ab.first, ab.second, 1.0f, 1.0f, rng,
+                                                         sgd_epochs, nthreads);
+        }
+        secs[5] = seconds_since(t0);
+        return ok ? 1 : 0;
+    })
+}
+
 }

@@ -19,6 +19,13 @@
 #include <utility>
 #include <vector>
 
+// Vectorised exact search (oracle/ref_knn.cpp): squared distances, sorted by
+// (distance, index), self excluded, k per query.
+void oracle_bruteforce_knn(const float* data, std::size_t dim, int nobs, int qstart, int qcount, int k, int nthreads,
+                           int* out_idx, float* out_d2);
+void oracle_bruteforce_knn(const double* data, std::size_t dim, int nobs, int qstart, int qcount, int k, int nthreads,
+                           int* out_idx, double* out_d2);
+
 namespace knncolle {
 
 template<typename Index_, typename Distance_>
@@ -80,55 +87,23 @@ public:
     Index_ num_observations() const override { return my_obs; }
 
     void search_range(Index_ start, Index_ count, int k, int num_threads, NeighborList<Index_, Distance_>& out) const override {
-        const Index_ kk = std::min<Index_>(k, my_obs > 0 ? my_obs - 1 : 0);
+        const int kk = std::min<int>(k, my_obs > 0 ? static_cast<int>(my_obs) - 1 : 0);
         if (static_cast<Index_>(out.size()) < count) {
             out.resize(count);
         }
-        auto work = [&](Index_ qs, Index_ qe) {
-            std::vector<std::pair<Data_, Index_> > heap;
-            heap.reserve(kk + 1);
-            for (Index_ q = qs; q < qe; ++q) {
-                const Data_* xq = my_data.data() + my_dim * static_cast<std::size_t>(q);
-                heap.clear();
-                for (Index_ j = 0; j < my_obs; ++j) {
-                    if (j == q) {
-                        continue;
-                    }
-                    const Data_* xj = my_data.data() + my_dim * static_cast<std::size_t>(j);
-                    Data_ d2 = 0;
-                    for (std::size_t d = 0; d < my_dim; ++d) {
-                        const Data_ diff = xq[d] - xj[d];
-                        d2 += diff * diff;
-                    }
-                    if (static_cast<Index_>(heap.size()) < kk) {
-                        heap.emplace_back(d2, j);
-                        std::push_heap(heap.begin(), heap.end());
-                    } else if (kk > 0 && std::make_pair(d2, j) < heap.front()) {
-                        std::pop_heap(heap.begin(), heap.end());
-                        heap.back() = std::make_pair(d2, j);
-                        std::push_heap(heap.begin(), heap.end());
-                    }
-                }
-                std::sort_heap(heap.begin(), heap.end());
-                auto& row = out[q - start];
-                row.clear();
-                for (const auto& h : heap) {
-                    row.emplace_back(h.second, static_cast<Distance_>(std::sqrt(h.first)));
-                }
-            }
-        };
-        const int nt = std::max(1, num_threads);
-        std::vector<std::thread> threads;
-        const Index_ per = (count + nt - 1) / nt;
-        for (int t = 0; t < nt; ++t) {
-            const Index_ s = start + per * t;
-            const Index_ e = std::min<Index_>(start + count, s + per);
-            if (s < e) {
-                threads.emplace_back(work, s, e);
-            }
+        std::vector<int> idx(static_cast<std::size_t>(count) * kk);
+        std::vector<Data_> d2(static_cast<std::size_t>(count) * kk);
+        if (kk > 0) {
+            oracle_bruteforce_knn(my_data.data(), my_dim, static_cast<int>(my_obs), static_cast<int>(start),
+                                  static_cast<int>(count), kk, num_threads, idx.data(), d2.data());
         }
-        for (auto& t : threads) {
-            t.join();
+        for (Index_ q = 0; q < count; ++q) {
+            auto& row = out[q];
+            row.clear();
+            for (int t = 0; t < kk; ++t) {
+                const std::size_t o = static_cast<std::size_t>(q) * kk + t;
+                row.emplace_back(static_cast<Index_>(idx[o]), static_cast<Distance_>(std::sqrt(d2[o])));
+            }
         }
     }
 

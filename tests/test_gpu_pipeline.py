@@ -1,0 +1,186 @@
+"""End-to-end parity of initialize() / Status::run() with the reference.
+
+The reference path is the oracle's serial optimize_layout (bit-identical to
+the reference headers compiled in oracle/_ref) from the same initial layout.
+Parallel SGD reorders updates and draws its negative samples from a
+different generator, so layouts are compared by quality:
+trustworthiness(k=15) within 0.005 and fuzzy cross-entropy within 1%.
+Everything RNG-free is compared exactly.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from helpers import csr_tuple, mock_neighbors, neighbors_of, normal_data, two_populations
+
+pytestmark = pytest.mark.gpu
+
+
+def _oracle_pipeline(nl: oracle.CSR, dtype, num_epochs, rate=5.0):
+    """Similarities (FP64, stored in dtype) -> union -> epochs, as the device computes them."""
+    w64, _, _ = oracle.neighbor_similarities(nl.astype(np.float64))
+    w = oracle.CSR(nl.ptr, nl.idx, w64.val.astype(dtype))
+    g = oracle.combine_neighbor_sets(w, 1.0)
+    return g, oracle.similarities_to_epochs(g, num_epochs, rate)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_epoch_data_matches_oracle(umap, dtype):
+    nl = neighbors_of(normal_data(500, 10, seed=2), 15, dtype=dtype)
+    Y = np.zeros((500, 2), dtype=dtype)
+    st = umap.initialize(csr_tuple(nl), 2, Y, umap.Options(initialize_method=umap.InitializeMethod.NONE))
+    assert st.epoch() == 0 and st.num_epochs() == 500 and st.num_observations() == 500
+    a, b = oracle.find_ab(1.0, 0.1)
+    assert (st.a, st.b) == (a, b)
+    _, ref = _oracle_pipeline(nl, dtype, 500)
+    ep = st.get_epoch_data()
+    assert np.array_equal(ep.cumulative_num_edges, ref.ptr)
+    assert np.array_equal(ep.edge_targets, ref.targets)
+    assert np.array_equal(ep.epochs_per_sample, ref.eps)
+    assert np.array_equal(ep.epoch_of_next_sample, ref.enext)
+    assert np.array_equal(ep.epoch_of_next_negative_sample, ref.enneg)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_layout_quality_matches_reference(umap, dtype):
+    n = 2000
+    X = normal_data(n, 10, seed=1000, dtype=dtype)        # the README's 2000 x 10 N(0,1) example shape
+    nl = neighbors_of(X, 15)
+    g, ep = _oracle_pipeline(nl, dtype, 500)
+    ok, Y0, _ = oracle.spectral_init(g, 2)
+    assert ok
+    # device run from the oracle's initial layout
+    Y = np.ascontiguousarray(Y0.copy())
+    st = umap.initialize(csr_tuple(nl), 2, Y, umap.Options(initialize_method=umap.InitializeMethod.NONE))
+    st.run(Y)
+    assert st.epoch() == 500
+    assert np.all(np.isfinite(Y))
+    # reference serial run from the same layout
+    R = Y0.copy()
+    a, b = oracle.find_ab(1.0, 0.1)
+    oracle.optimize_layout(2, R, ep, a, b, 1.0, 1.0, 1234567890, 500)
+    t_dev = oracle.trustworthiness(X, Y, 15)
+    t_ref = oracle.trustworthiness(X, R, 15)
+    assert abs(t_dev - t_ref) <= 0.005, (t_dev, t_ref)
+    ce_dev = oracle.cross_entropy(g.astype(np.float64), Y, a, b)
+    ce_ref = oracle.cross_entropy(g.astype(np.float64), R, a, b)
+    assert abs(ce_dev - ce_ref) <= 0.01 * abs(ce_ref), (ce_dev, ce_ref)
+
+
+def test_spectral_initialize_matches_reference(umap):
+    X = normal_data(2000, 10, seed=1000)
+    nl = neighbors_of(X, 15)
+    Y = np.zeros((2000, 2))
+    st = umap.initialize(csr_tuple(nl), 2, Y)
+    g, _ = _oracle_pipeline(nl, np.float64, 500)
+    ok, R, _ = oracle.spectral_init(g, 2)
+    assert ok
+    for d in range(2):
+        s = np.sign(np.dot(Y[:, d], R[:, d]))
+        assert np.max(np.abs(Y[:, d] - s * R[:, d])) < 1e-3 * 10
+
+
+@pytest.mark.parametrize("n,k", [(50, 5), (100, 10), (200, 15)])
+def test_two_populations_separate(umap, n, k):
+    # tests/src/umappp.cpp:60-90
+    X = two_populations(n, 5, seed=n * k)
+    nl = neighbors_of(X, k)
+    Y = np.zeros((n, 2))
+    st = umap.initialize(csr_tuple(nl), 2, Y)
+    assert st.num_epochs() == 500
+    st.run(Y)
+    assert st.epoch() == 500 and np.all(np.isfinite(Y))
+    even, odd = Y[0::2], Y[1::2]
+    sep = any(even[:, d].max() < odd[:, d].min() or odd[:, d].max() < even[:, d].min() for d in range(2))
+    assert sep
+
+
+def test_builder_path_equals_neighbor_path(umap):
+    X = two_populations(300, 5, seed=9, dtype=np.float32)
+    Y1 = np.zeros((300, 2), np.float32)
+    s1 = umap.initialize_from_data(X, 2, Y1, umap.Options(num_neighbors=10))
+    idx, dist = umap.knn(X, 10)
+    Y2 = np.zeros((300, 2), np.float32)
+    s2 = umap.initialize((idx, dist), 2, Y2, umap.Options())
+    assert np.array_equal(Y1, Y2)
+    e1, e2 = s1.get_epoch_data(), s2.get_epoch_data()
+    assert np.array_equal(e1.edge_targets, e2.edge_targets)
+    assert np.array_equal(e1.epochs_per_sample, e2.epochs_per_sample)
+
+
+def test_partial_runs_follow_the_same_schedule(umap):
+    # tests/src/umappp.cpp:104-115: run(200) then run() covers the same epochs as run()
+    X = two_populations(200, 5, seed=5)
+    nl = neighbors_of(X, 15)
+    Y = np.zeros((200, 2))
+    st = umap.initialize(csr_tuple(nl), 2, Y)
+    Y0 = Y.copy()
+    st.run(Y, 200)
+    assert st.epoch() == 200
+    assert not np.array_equal(Y, Y0)
+    mid = st.get_epoch_data()
+    st.run(Y)
+    assert st.epoch() == 500
+    full = umap.initialize(csr_tuple(nl), 2, np.zeros((200, 2)))
+    assert np.array_equal(full.schedule_counts(200, 500), st.schedule_counts(200, 500))
+    # the schedule state after 200 epochs is the reference's
+    _, ep = _oracle_pipeline(nl, np.float64, 500)
+    R = Y0.copy()
+    oracle.optimize_layout(2, R, ep, st.a, st.b, 1.0, 1.0, 1, 200)
+    assert np.array_equal(mid.epoch_of_next_sample, ep.enext)
+    assert np.array_equal(mid.epoch_of_next_negative_sample, ep.enneg)
+
+
+def test_initialize_method_semantics(umap):
+    # tests/src/umappp.cpp:209-313
+    nn = mock_neighbors(87, 5, seed=87)
+    ref = np.zeros((87, 2))
+    umap.initialize(csr_tuple(nn), 2, ref)
+    assert np.all(ref != 0)
+    out = np.zeros((87, 2))
+    umap.initialize(csr_tuple(nn), 2, out, umap.Options(initialize_random_on_spectral_fail=False))
+    assert np.array_equal(ref, out)
+    out = np.zeros((87, 2))
+    umap.initialize(csr_tuple(nn), 2, out, umap.Options(initialize_method=umap.InitializeMethod.RANDOM))
+    assert np.all(out != 0) and not np.array_equal(ref, out)
+    out = np.zeros((87, 2))
+    umap.initialize(csr_tuple(nn), 2, out, umap.Options(initialize_method=umap.InitializeMethod.NONE))
+    assert np.all(out == 0)
+
+    # spectral failure on two components: random fallback, or untouched without it
+    a, b = mock_neighbors(40, 5, seed=40), mock_neighbors(50, 5, seed=50)
+    two = oracle.CSR.from_lists(a.to_lists() + [[(j + 40, v) for j, v in r] for r in b.to_lists()])
+    ref = np.zeros((90, 2))
+    umap.initialize(csr_tuple(two), 2, ref)
+    rnd = np.zeros((90, 2))
+    umap.initialize(csr_tuple(two), 2, rnd, umap.Options(initialize_method=umap.InitializeMethod.RANDOM))
+    assert np.all(ref != 0) and np.array_equal(ref, rnd)
+    keep = np.zeros((90, 2))
+    umap.initialize(csr_tuple(two), 2, keep, umap.Options(initialize_random_on_spectral_fail=False))
+    assert np.all(keep == 0)
+
+
+def test_float32_path_runs(umap):
+    # tests/src/umappp.cpp:150-173
+    X = np.random.default_rng(436).normal(size=(87, 7)).astype(np.float32)
+    Y = np.zeros((87, 2), np.float32)
+    st = umap.initialize_from_data(X, 2, Y, umap.Options(num_neighbors=5))
+    st.run(Y)
+    assert st.epoch() == 500 and np.all(np.isfinite(Y))
+
+
+def test_higher_embedding_dimensions(umap):
+    X = normal_data(300, 8, seed=3)
+    nl = neighbors_of(X, 10)
+    for ndim in (1, 3, 5):
+        Y = np.zeros((300, ndim))
+        st = umap.initialize(csr_tuple(nl), ndim, Y)
+        st.run(Y)
+        assert np.all(np.isfinite(Y))
+
+
+def test_invalid_arguments(umap):
+    with pytest.raises(umap.UmapbError):
+        umap.initialize([[(5, 1.0)], [(0, 1.0)]], 2, np.zeros((2, 2)))   # out-of-range index
+    with pytest.raises(umap.UmapbError):
+        umap.initialize([[(1, 1.0)], [(0, 1.0)]], 0, np.zeros((2, 0)))  # num_dim 0

@@ -1,0 +1,719 @@
+// The C ABI (include/umapb.h) and the host orchestration behind it: the
+// reference's initialize() / Status::run() pipeline
+// (include/umappp/initialize.hpp:69-177, include/umappp/Status.hpp:25-141)
+// driven as a sequence of device stages on one CUDA stream per status.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "stages.cuh"
+#include "umapb.h"
+
+namespace umapb {
+
+std::atomic<long long> g_launches{0};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+void set_error(const std::string& m) { g_last_error = m; }
+
+// Fails unless a compute capability 10.x device is current (the library
+// carries sm_100a code only; there is no CPU path).
+void require_device() {
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        fail(UMAPB_ERR_NO_DEVICE, "no CUDA device is available (libumappp_b200 runs on sm_100 GPUs only)");
+    }
+    int dev = 0;
+    UMAPB_CUDA(cudaGetDevice(&dev));
+    int major = 0;
+    UMAPB_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+    if (major != 10) fail(UMAPB_ERR_NO_DEVICE, "the current CUDA device is not sm_100 (B200/GB200)");
+}
+
+}  // namespace
+
+Context& thread_context() {
+    thread_local Context ctx;
+    int dev = 0;
+    UMAPB_CUDA(cudaGetDevice(&dev));
+    if (ctx.device != dev) {
+        UMAPB_CUDA(cudaStreamCreateWithFlags(&ctx.stream, cudaStreamNonBlocking));
+        UMAPB_CUDA(cudaMalloc(reinterpret_cast<void**>(&ctx.d_status), sizeof(int)));
+        UMAPB_CUDA(cudaMemset(ctx.d_status, 0, sizeof(int)));
+        ctx.device = dev;
+    }
+    return ctx;
+}
+
+// ------------------------------------------------------------- status ---
+
+struct StatusBase {
+    virtual ~StatusBase() = default;
+    virtual void run(void* embedding, int epoch_limit) = 0;
+    virtual int64_t num_edges() const = 0;
+    virtual void epoch_data(int64_t* ptr, int32_t* targets, void* eps, void* enext, void* enneg) = 0;
+    virtual void counts(int first, int last, int64_t* out) = 0;
+};
+
+}  // namespace umapb
+
+struct umapb_status {
+    int dtype = UMAPB_F32;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int* d_status = nullptr;
+    int32_t n = 0;
+    size_t num_dim = 0;
+    umapb_options opt{};
+    double a = 0, b = 0;
+    int num_epochs = 0;
+    int current_epoch = 0;
+    float stage_ms[7] = {0, 0, 0, 0, 0, 0, 0};
+    std::unique_ptr<umapb::StatusBase> impl;
+
+    ~umapb_status() {
+        impl.reset();
+        if (stream) {
+            cudaStreamSynchronize(stream);
+            cudaStreamDestroy(stream);
+        }
+        if (d_status) cudaFree(d_status);
+    }
+};
+
+namespace umapb {
+
+namespace {
+
+enum Stage { ST_KNN = 0, ST_SIM, ST_UNION, ST_INIT, ST_EPOCHS, ST_SCHEDULE, ST_SGD };
+
+// Event pair per stage, resolved at the end of a call.
+struct StageTimer {
+    cudaStream_t s;
+    float* out;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
+    explicit StageTimer(cudaStream_t st, float* o) : s(st), out(o) {}
+    void begin(int stage) {
+        cudaEvent_t a, b;
+        UMAPB_CUDA(cudaEventCreate(&a));
+        UMAPB_CUDA(cudaEventCreate(&b));
+        UMAPB_CUDA(cudaEventRecord(a, s));
+        marks.push_back({stage, {a, b}});
+    }
+    void end() { UMAPB_CUDA(cudaEventRecord(marks.back().second.second, s)); }
+    void resolve() {
+        UMAPB_CUDA(cudaStreamSynchronize(s));
+        for (auto& m : marks) {
+            float t = 0;
+            cudaEventElapsedTime(&t, m.second.first, m.second.second);
+            out[m.first] = t;
+        }
+    }
+    ~StageTimer() {
+        for (auto& m : marks) {
+            cudaEventDestroy(m.second.first);
+            cudaEventDestroy(m.second.second);
+        }
+    }
+};
+
+__global__ void dense_row_ptr_kernel(int32_t n, int32_t k, int64_t* ptr) {
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i <= n; i += int64_t(gridDim.x) * blockDim.x)
+        ptr[i] = i * k;
+}
+
+template <typename T>
+struct StatusImpl final : StatusBase {
+    umapb_status* st;
+    DeviceEpochs<T> epochs;
+    SgdEngine<T> engine;
+
+    explicit StatusImpl(umapb_status* s) : st(s) {}
+
+    // Stages after the neighbour search (initialize.hpp:69-119).  ptr/idx/dist
+    // are device arrays; dist is consumed (turned into weights).
+    void initialize(const int64_t* ptr, const int32_t* idx, T* dist, int64_t nnz, void* embedding, StageTimer& tm) {
+        cudaStream_t s = st->stream;
+        const umapb_options& o = st->opt;
+        const int32_t n = st->n;
+
+        tm.begin(ST_SIM);
+        neighbor_similarities<T>(n, ptr, dist, o.local_connectivity, o.bandwidth, 1e-3, true, nullptr, nullptr, s);
+        tm.end();
+
+        tm.begin(ST_UNION);
+        DeviceCsr<T> g;
+        combine_neighbor_sets<T>(n, ptr, idx, dist, nnz, o.mix_ratio, g, s);
+        tm.end();
+
+        // initial layout (initialize.hpp:79-103)
+        tm.begin(ST_INIT);
+        const size_t total = static_cast<size_t>(n) * st->num_dim;
+        DeviceInOut<T> Y(static_cast<T*>(embedding), total, s, /*load=*/false);
+        bool wrote = false;
+        bool use_random = (o.initialize_method == UMAPB_INIT_RANDOM);
+        if (o.initialize_method == UMAPB_INIT_SPECTRAL) {
+            const SpectralResult r = spectral_init<T>(
+                n, g.ptr.get(), g.idx.get(), g.val.get(), static_cast<int>(st->num_dim), Y.get(), o.irlba_extra_work,
+                o.irlba_max_iterations, o.irlba_convergence_tolerance, o.initialize_spectral_scale,
+                o.initialize_spectral_jitter != 0, o.initialize_spectral_jitter_sd, o.initialize_seed, st->d_status, s);
+            wrote = r.ok;
+            use_random = (o.initialize_random_on_spectral_fail != 0 && !r.ok);
+        }
+        if (use_random) {
+            random_init<T>(n, static_cast<int>(st->num_dim), Y.get(), o.initialize_seed, o.initialize_random_scale, s);
+            wrote = true;
+        }
+        if (wrote) Y.finish();
+        tm.end();
+
+        // a, b (initialize.hpp:105-110) and the epoch count (:112)
+        if (!o.has_a || !o.has_b) {
+            find_ab(o.spread, o.min_dist, &st->a, &st->b);
+        } else {
+            st->a = o.a;
+            st->b = o.b;
+        }
+        st->num_epochs = choose_num_epochs(o.has_num_epochs != 0, o.num_epochs, n);
+
+        tm.begin(ST_EPOCHS);
+        similarities_to_epochs<T>(n, g.ptr.get(), g.idx.get(), g.val.get(), g.nnz, st->num_epochs,
+                                  o.negative_sample_rate, epochs, s);
+        engine.setup(&epochs, s);
+        tm.end();
+        st->current_epoch = 0;
+    }
+
+    void run(void* embedding, int epoch_limit) override {
+        cudaStream_t s = st->stream;
+        if (epoch_limit <= st->current_epoch) return;
+        const size_t total = static_cast<size_t>(st->n) * st->num_dim;
+        DeviceInOut<T> Y(static_cast<T*>(embedding), total, s, /*load=*/true);
+        float ms_sched = 0, ms_sgd = 0;
+        engine.run(Y.get(), static_cast<int>(st->num_dim), st->current_epoch, epoch_limit, st->a, st->b,
+                   st->opt.repulsion_strength, st->opt.learning_rate, st->opt.optimize_seed, s, &ms_sched, &ms_sgd);
+        Y.finish();
+        UMAPB_CUDA(cudaStreamSynchronize(s));
+        st->stage_ms[ST_SCHEDULE] = ms_sched;
+        st->stage_ms[ST_SGD] = ms_sgd;
+        st->current_epoch = epoch_limit;
+    }
+
+    int64_t num_edges() const override { return epochs.nnz; }
+
+    void epoch_data(int64_t* ptr, int32_t* targets, void* eps, void* enext, void* enneg) override {
+        cudaStream_t s = st->stream;
+        const int64_t nnz = epochs.nnz;
+        copy_out(ptr, epochs.ptr.get(), sizeof(int64_t) * (static_cast<size_t>(st->n) + 1), s);
+        copy_out(targets, epochs.targets.get(), sizeof(int32_t) * nnz, s);
+        copy_out(eps, epochs.eps.get(), sizeof(T) * nnz, s);
+        if (enext || enneg) {
+            DevArray<T> a(nnz, s), b(nnz, s);
+            engine.state_at(st->current_epoch, a.get(), b.get(), s);
+            copy_out(enext, a.get(), sizeof(T) * nnz, s);
+            copy_out(enneg, b.get(), sizeof(T) * nnz, s);
+            UMAPB_CUDA(cudaStreamSynchronize(s));
+        }
+        UMAPB_CUDA(cudaStreamSynchronize(s));
+    }
+
+    void counts(int first, int last, int64_t* out) override { engine.counts(first, last, out, st->stream); }
+};
+
+std::unique_ptr<umapb_status> new_status(int dtype, int32_t n, size_t num_dim, const umapb_options* opt) {
+    require_device();
+    require(dtype == UMAPB_F32 || dtype == UMAPB_F64, "dtype must be UMAPB_F32 or UMAPB_F64");
+    require(opt != nullptr, "options must not be NULL");
+    require(n >= 0, "num_obs must be non-negative");
+    require(num_dim >= 1 && num_dim <= 64, "num_dim must be between 1 and 64");
+    auto st = std::make_unique<umapb_status>();
+    st->dtype = dtype;
+    UMAPB_CUDA(cudaGetDevice(&st->device));
+    UMAPB_CUDA(cudaStreamCreateWithFlags(&st->stream, cudaStreamNonBlocking));
+    UMAPB_CUDA(cudaMalloc(reinterpret_cast<void**>(&st->d_status), sizeof(int)));
+    UMAPB_CUDA(cudaMemset(st->d_status, 0, sizeof(int)));
+    st->n = n;
+    st->num_dim = num_dim;
+    st->opt = *opt;
+    return st;
+}
+
+template <typename T>
+void init_from_neighbors(umapb_status* st, const int64_t* row_ptr, const int32_t* indices, const void* distances,
+                         void* embedding) {
+    cudaStream_t s = st->stream;
+    const int32_t n = st->n;
+    require(row_ptr != nullptr, "row_ptr must not be NULL");
+    // the row pointers are needed on the host for the edge count
+    int64_t nnz = 0;
+    if (is_device_pointer(row_ptr)) {
+        UMAPB_CUDA(cudaMemcpyAsync(&nnz, row_ptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        UMAPB_CUDA(cudaStreamSynchronize(s));
+    } else {
+        nnz = row_ptr[n];
+    }
+    require(nnz >= 0, "row_ptr must be non-decreasing from 0");
+    DeviceIn<int64_t> dptr(row_ptr, static_cast<size_t>(n) + 1, s);
+    DeviceIn<int32_t> didx(indices, nnz, s);
+    DevArray<T> w(nnz, s);
+    if (nnz) UMAPB_CUDA(cudaMemcpyAsync(w.get(), distances, sizeof(T) * nnz, cudaMemcpyDefault, s));
+    auto impl = std::make_unique<StatusImpl<T>>(st);
+    StageTimer tm(s, st->stage_ms);
+    impl->initialize(dptr.get(), didx.get(), w.get(), nnz, embedding, tm);
+    tm.resolve();
+    st->impl = std::move(impl);
+}
+
+template <typename T>
+void init_from_data(umapb_status* st, size_t data_dim, const void* data, void* embedding) {
+    cudaStream_t s = st->stream;
+    const int32_t n = st->n;
+    require(data_dim >= 1 && data_dim <= INT32_MAX, "data_dim must be positive");
+    const int k = std::min<int>(st->opt.num_neighbors, n - 1);   // knncolle returns at most n - 1 neighbours
+    require(st->opt.num_neighbors >= 1, "num_neighbors must be positive");
+    StageTimer tm(s, st->stage_ms);
+    DeviceIn<T> d(static_cast<const T*>(data), static_cast<size_t>(n) * data_dim, s);
+    const int64_t nnz = static_cast<int64_t>(n) * k;
+    DevArray<int32_t> idx(nnz, s);
+    DevArray<T> dist(nnz, s);
+    DevArray<int64_t> ptr(static_cast<size_t>(n) + 1, s);
+    tm.begin(ST_KNN);
+    if (k >= 1) knn_exact<T>(d.get(), n, static_cast<int32_t>(data_dim), k, idx.get(), dist.get(), s);
+    dense_row_ptr_kernel<<<grid_for(static_cast<size_t>(n) + 1, 256), 256, 0, s>>>(n, k, ptr.get());
+    UMAPB_LAUNCH_CHECK();
+    tm.end();
+    auto impl = std::make_unique<StatusImpl<T>>(st);
+    impl->initialize(ptr.get(), idx.get(), dist.get(), nnz, embedding, tm);
+    tm.resolve();
+    st->impl = std::move(impl);
+}
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        f();
+        return UMAPB_OK;
+    } catch (const Error& e) {
+        set_error(e.what());
+        cudaGetLastError();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        set_error("host allocation failed");
+        return UMAPB_ERR_OOM;
+    } catch (const std::exception& e) {
+        set_error(e.what());
+        return UMAPB_ERR_INVALID;
+    } catch (...) {
+        set_error("unknown error");
+        return UMAPB_ERR_INVALID;
+    }
+}
+
+size_t dsize(int dtype) { return dtype == UMAPB_F64 ? sizeof(double) : sizeof(float); }
+
+int64_t host_nnz(const int64_t* row_ptr, int32_t n, cudaStream_t s) {
+    require(row_ptr != nullptr, "row_ptr must not be NULL");
+    int64_t nnz = 0;
+    if (is_device_pointer(row_ptr)) {
+        UMAPB_CUDA(cudaMemcpyAsync(&nnz, row_ptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        UMAPB_CUDA(cudaStreamSynchronize(s));
+    } else {
+        nnz = row_ptr[n];
+    }
+    require(nnz >= 0, "row_ptr must be non-decreasing from 0");
+    return nnz;
+}
+
+}  // namespace
+
+void check_device_status(Context& ctx) {
+    int st = 0;
+    UMAPB_CUDA(cudaMemcpyAsync(&st, ctx.d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+    UMAPB_CUDA(cudaStreamSynchronize(ctx.stream));
+    if (st != DEV_OK) {
+        UMAPB_CUDA(cudaMemsetAsync(ctx.d_status, 0, sizeof(int), ctx.stream));
+        if (st == DEV_TIMEOUT) fail(UMAPB_ERR_DEVICE_TIMEOUT, "a bounded device wait gave up");
+        fail(UMAPB_ERR_INVALID, "invalid input detected on the device");
+    }
+}
+
+}  // namespace umapb
+
+using namespace umapb;
+
+extern "C" {
+
+void umapb_options_init(umapb_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->local_connectivity = 1;
+    o->bandwidth = 1;
+    o->mix_ratio = 1;
+    o->spread = 1;
+    o->min_dist = 0.1;
+    o->repulsion_strength = 1;
+    o->initialize_method = UMAPB_INIT_SPECTRAL;
+    o->initialize_random_on_spectral_fail = 1;
+    o->irlba_extra_work = 7;
+    o->irlba_max_iterations = 1000;
+    o->irlba_convergence_tolerance = 1e-6;
+    o->initialize_spectral_scale = 10;
+    o->initialize_spectral_jitter = 0;
+    o->initialize_spectral_jitter_sd = 1e-4;
+    o->initialize_random_scale = 10;
+    o->initialize_seed = 9876543210ULL;
+    o->learning_rate = 1;
+    o->negative_sample_rate = 5;
+    o->num_neighbors = 15;
+    o->optimize_seed = 1234567890ULL;
+    o->num_threads = 1;
+    o->num_threads_spectral = 1;
+    o->num_threads_optimize = 1;
+}
+
+const char* umapb_last_error(void) { return g_last_error.c_str(); }
+
+int umapb_version(void) { return UMAPB_VERSION; }
+
+size_t umapb_options_size(void) { return sizeof(umapb_options); }
+
+int64_t umapb_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+int umapb_initialize_neighbors(int dtype, int32_t num_obs, const int64_t* row_ptr, const int32_t* indices,
+                               const void* distances, size_t num_dim, void* embedding, const umapb_options* opt,
+                               umapb_status** out) {
+    return guarded([&] {
+        require(out != nullptr, "out must not be NULL");
+        *out = nullptr;
+        auto st = new_status(dtype, num_obs, num_dim, opt);
+        if (dtype == UMAPB_F64) {
+            init_from_neighbors<double>(st.get(), row_ptr, indices, distances, embedding);
+        } else {
+            init_from_neighbors<float>(st.get(), row_ptr, indices, distances, embedding);
+        }
+        *out = st.release();
+    });
+}
+
+int umapb_initialize_data(int dtype, size_t data_dim, int32_t num_obs, const void* data, size_t num_dim,
+                          void* embedding, const umapb_options* opt, umapb_status** out) {
+    return guarded([&] {
+        require(out != nullptr, "out must not be NULL");
+        *out = nullptr;
+        auto st = new_status(dtype, num_obs, num_dim, opt);
+        require(num_obs >= 2, "the neighbour search needs at least two observations");
+        if (dtype == UMAPB_F64) {
+            init_from_data<double>(st.get(), data_dim, data, embedding);
+        } else {
+            init_from_data<float>(st.get(), data_dim, data, embedding);
+        }
+        *out = st.release();
+    });
+}
+
+int umapb_status_run(umapb_status* st, void* embedding, int epoch_limit) {
+    return guarded([&] {
+        require(st != nullptr && st->impl, "invalid status");
+        UMAPB_CUDA(cudaSetDevice(st->device));
+        st->impl->run(embedding, epoch_limit < 0 ? st->num_epochs : epoch_limit);
+    });
+}
+
+int umapb_status_epoch(const umapb_status* st) { return st ? st->current_epoch : -1; }
+int umapb_status_num_epochs(const umapb_status* st) { return st ? st->num_epochs : -1; }
+int32_t umapb_status_num_observations(const umapb_status* st) { return st ? st->n : -1; }
+size_t umapb_status_num_dimensions(const umapb_status* st) { return st ? st->num_dim : 0; }
+double umapb_status_a(const umapb_status* st) { return st ? st->a : 0; }
+double umapb_status_b(const umapb_status* st) { return st ? st->b : 0; }
+int64_t umapb_status_num_edges(const umapb_status* st) { return (st && st->impl) ? st->impl->num_edges() : -1; }
+
+int umapb_status_get_epoch_data(const umapb_status* st, int64_t* row_ptr, int32_t* targets, void* eps, void* enext,
+                                void* enneg) {
+    return guarded([&] {
+        require(st != nullptr && st->impl, "invalid status");
+        UMAPB_CUDA(cudaSetDevice(st->device));
+        st->impl->epoch_data(row_ptr, targets, eps, enext, enneg);
+    });
+}
+
+int umapb_status_schedule_counts(const umapb_status* st, int first, int last, int64_t* counts) {
+    return guarded([&] {
+        require(st != nullptr && st->impl, "invalid status");
+        require(first >= 0 && last >= first, "bad epoch range");
+        UMAPB_CUDA(cudaSetDevice(st->device));
+        st->impl->counts(first, last, counts);
+    });
+}
+
+int umapb_status_stage_ms(const umapb_status* st, double* ms, int count) {
+    return guarded([&] {
+        require(st != nullptr && ms != nullptr, "invalid arguments");
+        for (int i = 0; i < count && i < 7; ++i) ms[i] = st->stage_ms[i];
+    });
+}
+
+void umapb_status_free(umapb_status* st) { delete st; }
+
+int umapb_knn(int dtype, size_t data_dim, int32_t num_obs, const void* data, int k, int32_t* out_indices,
+              void* out_distances) {
+    return guarded([&] {
+        require_device();
+        Context& c = thread_context();
+        const size_t total = static_cast<size_t>(num_obs) * data_dim;
+        const size_t nk = static_cast<size_t>(num_obs) * (k > 0 ? k : 0);
+        DeviceInOut<int32_t> oi(out_indices, nk, c.stream, false);
+        if (dtype == UMAPB_F64) {
+            DeviceIn<double> d(static_cast<const double*>(data), total, c.stream);
+            DeviceInOut<double> od(static_cast<double*>(out_distances), nk, c.stream, false);
+            knn_exact<double>(d.get(), num_obs, static_cast<int32_t>(data_dim), k, oi.get(), od.get(), c.stream);
+            od.finish();
+        } else {
+            DeviceIn<float> d(static_cast<const float*>(data), total, c.stream);
+            DeviceInOut<float> od(static_cast<float*>(out_distances), nk, c.stream, false);
+            knn_exact<float>(d.get(), num_obs, static_cast<int32_t>(data_dim), k, oi.get(), od.get(), c.stream);
+            od.finish();
+        }
+        oi.finish();
+        UMAPB_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+int umapb_neighbor_similarities(int dtype, int32_t num_obs, const int64_t* row_ptr, void* distances,
+                                double local_connectivity, double bandwidth, double min_k_dist_scale, int use_newton,
+                                double* rho_out, double* sigma_out) {
+    return guarded([&] {
+        require_device();
+        Context& c = thread_context();
+        const int64_t nnz = host_nnz(row_ptr, num_obs, c.stream);
+        DeviceIn<int64_t> p(row_ptr, static_cast<size_t>(num_obs) + 1, c.stream);
+        DeviceInOut<double> rho(rho_out, rho_out ? num_obs : 0, c.stream, false);
+        DeviceInOut<double> sig(sigma_out, sigma_out ? num_obs : 0, c.stream, false);
+        if (dtype == UMAPB_F64) {
+            DeviceInOut<double> v(static_cast<double*>(distances), nnz, c.stream, true);
+            neighbor_similarities<double>(num_obs, p.get(), v.get(), local_connectivity, bandwidth, min_k_dist_scale,
+                                          use_newton != 0, rho.get(), sig.get(), c.stream);
+            v.finish();
+        } else {
+            DeviceInOut<float> v(static_cast<float*>(distances), nnz, c.stream, true);
+            neighbor_similarities<float>(num_obs, p.get(), v.get(), local_connectivity, bandwidth, min_k_dist_scale,
+                                         use_newton != 0, rho.get(), sig.get(), c.stream);
+            v.finish();
+        }
+        rho.finish();
+        sig.finish();
+        UMAPB_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+int umapb_combine_neighbor_sets(int dtype, int32_t num_obs, const int64_t* row_ptr, const int32_t* indices,
+                                const void* weights, double mix_ratio, int64_t* out_row_ptr, int32_t* out_indices,
+                                void* out_weights, int64_t capacity, int64_t* out_nnz) {
+    return guarded([&] {
+        require_device();
+        Context& c = thread_context();
+        const int64_t nnz = host_nnz(row_ptr, num_obs, c.stream);
+        DeviceIn<int64_t> p(row_ptr, static_cast<size_t>(num_obs) + 1, c.stream);
+        DeviceIn<int32_t> ix(indices, nnz, c.stream);
+        auto body = [&](auto tag) {
+            using T = decltype(tag);
+            DeviceIn<T> w(static_cast<const T*>(weights), nnz, c.stream);
+            DeviceCsr<T> g;
+            combine_neighbor_sets<T>(num_obs, p.get(), ix.get(), w.get(), nnz, mix_ratio, g, c.stream);
+            require(g.nnz <= capacity, "output capacity is too small for the combined graph");
+            copy_out(out_row_ptr, g.ptr.get(), sizeof(int64_t) * (static_cast<size_t>(num_obs) + 1), c.stream);
+            copy_out(out_indices, g.idx.get(), sizeof(int32_t) * g.nnz, c.stream);
+            copy_out(out_weights, g.val.get(), sizeof(T) * g.nnz, c.stream);
+            UMAPB_CUDA(cudaStreamSynchronize(c.stream));
+            if (out_nnz) *out_nnz = g.nnz;
+        };
+        if (dtype == UMAPB_F64) body(double{}); else body(float{});
+    });
+}
+
+int umapb_similarities_to_epochs(int dtype, int32_t num_obs, const int64_t* row_ptr, const int32_t* indices,
+                                 const void* weights, int num_epochs, double negative_sample_rate,
+                                 int64_t* out_row_ptr, int32_t* out_targets, void* eps, void* enext, void* enneg,
+                                 int64_t* out_nnz) {
+    return guarded([&] {
+        require_device();
+        Context& c = thread_context();
+        const int64_t nnz = host_nnz(row_ptr, num_obs, c.stream);
+        DeviceIn<int64_t> p(row_ptr, static_cast<size_t>(num_obs) + 1, c.stream);
+        DeviceIn<int32_t> ix(indices, nnz, c.stream);
+        auto body = [&](auto tag) {
+            using T = decltype(tag);
+            DeviceIn<T> w(static_cast<const T*>(weights), nnz, c.stream);
+            DeviceEpochs<T> ep;
+            similarities_to_epochs<T>(num_obs, p.get(), ix.get(), w.get(), nnz, num_epochs, negative_sample_rate, ep,
+                                      c.stream);
+            copy_out(out_row_ptr, ep.ptr.get(), sizeof(int64_t) * (static_cast<size_t>(num_obs) + 1), c.stream);
+            copy_out(out_targets, ep.targets.get(), sizeof(int32_t) * ep.nnz, c.stream);
+            copy_out(eps, ep.eps.get(), sizeof(T) * ep.nnz, c.stream);
+            copy_out(enext, ep.enext0.get(), sizeof(T) * ep.nnz, c.stream);
+            copy_out(enneg, ep.enneg0.get(), sizeof(T) * ep.nnz, c.stream);
+            UMAPB_CUDA(cudaStreamSynchronize(c.stream));
+            if (out_nnz) *out_nnz = ep.nnz;
+        };
+        if (dtype == UMAPB_F64) body(double{}); else body(float{});
+    });
+}
+
+int umapb_has_multiple_components(int32_t num_obs, const int64_t* row_ptr, const int32_t* indices, int* out) {
+    return guarded([&] {
+        require_device();
+        require(out != nullptr, "out must not be NULL");
+        Context& c = thread_context();
+        const int64_t nnz = host_nnz(row_ptr, num_obs, c.stream);
+        DeviceIn<int64_t> p(row_ptr, static_cast<size_t>(num_obs) + 1, c.stream);
+        DeviceIn<int32_t> ix(indices, nnz, c.stream);
+        // include/umappp/spectral_init.hpp:144-146: an empty graph is not "multiple"
+        *out = (num_obs > 0 && count_components(num_obs, p.get(), ix.get(), c.d_status, c.stream) > 1) ? 1 : 0;
+    });
+}
+
+int umapb_spectral_init(int dtype, int32_t num_obs, const int64_t* row_ptr, const int32_t* indices,
+                        const void* weights, size_t num_dim, void* embedding, int extra_work, int max_iterations,
+                        double tolerance, double scale, int jitter, double jitter_sd, uint64_t seed, int* ok,
+                        double* evals_out) {
+    return guarded([&] {
+        require_device();
+        Context& c = thread_context();
+        const int64_t nnz = host_nnz(row_ptr, num_obs, c.stream);
+        DeviceIn<int64_t> p(row_ptr, static_cast<size_t>(num_obs) + 1, c.stream);
+        DeviceIn<int32_t> ix(indices, nnz, c.stream);
+        auto body = [&](auto tag) {
+            using T = decltype(tag);
+            DeviceIn<T> w(static_cast<const T*>(weights), nnz, c.stream);
+            DeviceInOut<T> Y(static_cast<T*>(embedding), static_cast<size_t>(num_obs) * num_dim, c.stream, true);
+            const SpectralResult r = spectral_init<T>(num_obs, p.get(), ix.get(), w.get(), static_cast<int>(num_dim),
+                                                      Y.get(), extra_work, max_iterations, tolerance, scale,
+                                                      jitter != 0, jitter_sd, seed, c.d_status, c.stream);
+            if (r.ok) Y.finish();
+            UMAPB_CUDA(cudaStreamSynchronize(c.stream));
+            if (ok) *ok = r.ok ? 1 : 0;
+            if (evals_out) for (size_t d = 0; d <= num_dim && d < 64; ++d) evals_out[d] = r.evals[d];
+        };
+        if (dtype == UMAPB_F64) body(double{}); else body(float{});
+    });
+}
+
+int umapb_random_init(int dtype, int32_t num_obs, size_t num_dim, void* embedding, uint64_t seed, double scale) {
+    return guarded([&] {
+        require_device();
+        Context& c = thread_context();
+        auto body = [&](auto tag) {
+            using T = decltype(tag);
+            DeviceInOut<T> Y(static_cast<T*>(embedding), static_cast<size_t>(num_obs) * num_dim, c.stream, false);
+            random_init<T>(num_obs, static_cast<int>(num_dim), Y.get(), seed, scale, c.stream);
+            Y.finish();
+            UMAPB_CUDA(cudaStreamSynchronize(c.stream));
+        };
+        if (dtype == UMAPB_F64) body(double{}); else body(float{});
+    });
+}
+
+int umapb_find_ab(double spread, double min_dist, double* a, double* b) {
+    return guarded([&] {
+        require(a != nullptr && b != nullptr, "outputs must not be NULL");
+        find_ab(spread, min_dist, a, b);
+    });
+}
+
+int umapb_choose_num_epochs(int has_value, int value, int64_t num_obs) {
+    return choose_num_epochs(has_value != 0, value, num_obs);
+}
+
+int umapb_optimize_layout(int dtype, size_t num_dim, void* embedding, int32_t num_obs, const int64_t* row_ptr,
+                          const int32_t* targets, const void* epochs_per_sample, void* epoch_of_next_sample,
+                          void* epoch_of_next_negative_sample, double negative_sample_rate, int total_epochs,
+                          int* current_epoch, double a, double b, double gamma, double learning_rate, uint64_t seed,
+                          int epoch_limit) {
+    return guarded([&] {
+        require_device();
+        require(current_epoch != nullptr, "current_epoch must not be NULL");
+        Context& c = thread_context();
+        const int64_t nnz = host_nnz(row_ptr, num_obs, c.stream);
+        auto body = [&](auto tag) {
+            using T = decltype(tag);
+            DeviceEpochs<T> ep;
+            ep.n = num_obs;
+            ep.nnz = nnz;
+            ep.total_epochs = total_epochs;
+            ep.negative_sample_rate = static_cast<T>(negative_sample_rate);
+            ep.ptr.allocate(static_cast<size_t>(num_obs) + 1, c.stream);
+            ep.heads.allocate(nnz, c.stream);
+            ep.targets.allocate(nnz, c.stream);
+            ep.eps.allocate(nnz, c.stream);
+            ep.enext0.allocate(nnz, c.stream);
+            ep.enneg0.allocate(nnz, c.stream);
+            UMAPB_CUDA(cudaMemcpyAsync(ep.ptr.get(), row_ptr, sizeof(int64_t) * (num_obs + 1), cudaMemcpyDefault, c.stream));
+            if (nnz) {
+                UMAPB_CUDA(cudaMemcpyAsync(ep.targets.get(), targets, sizeof(int32_t) * nnz, cudaMemcpyDefault, c.stream));
+                UMAPB_CUDA(cudaMemcpyAsync(ep.eps.get(), epochs_per_sample, sizeof(T) * nnz, cudaMemcpyDefault, c.stream));
+                UMAPB_CUDA(cudaMemcpyAsync(ep.enext0.get(), epoch_of_next_sample, sizeof(T) * nnz, cudaMemcpyDefault, c.stream));
+                UMAPB_CUDA(cudaMemcpyAsync(ep.enneg0.get(), epoch_of_next_negative_sample, sizeof(T) * nnz, cudaMemcpyDefault, c.stream));
+            }
+            // heads from the row pointers
+            std::vector<int64_t> hp(static_cast<size_t>(num_obs) + 1);
+            UMAPB_CUDA(cudaMemcpyAsync(hp.data(), ep.ptr.get(), sizeof(int64_t) * (num_obs + 1), cudaMemcpyDeviceToHost, c.stream));
+            UMAPB_CUDA(cudaStreamSynchronize(c.stream));
+            std::vector<int32_t> heads(nnz);
+            for (int32_t i = 0; i < num_obs; ++i)
+                for (int64_t q = hp[i]; q < hp[i + 1]; ++q) heads[q] = i;
+            if (nnz) UMAPB_CUDA(cudaMemcpyAsync(ep.heads.get(), heads.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, c.stream));
+            // the given state describes the schedule at *current_epoch
+            SgdEngine<T> eng;
+            const int first = *current_epoch;
+            eng.setup(&ep, c.stream, first);
+            DeviceInOut<T> Y(static_cast<T*>(embedding), static_cast<size_t>(num_obs) * num_dim, c.stream, true);
+            eng.run(Y.get(), static_cast<int>(num_dim), first, epoch_limit, a, b, gamma, learning_rate, seed, c.stream,
+                    nullptr, nullptr);
+            Y.finish();
+            if (epoch_limit > first) {
+                DevArray<T> en(nnz, c.stream), enn(nnz, c.stream);
+                eng.state_at(epoch_limit, en.get(), enn.get(), c.stream);
+                copy_out(epoch_of_next_sample, en.get(), sizeof(T) * nnz, c.stream);
+                copy_out(epoch_of_next_negative_sample, enn.get(), sizeof(T) * nnz, c.stream);
+                *current_epoch = epoch_limit;
+            }
+            UMAPB_CUDA(cudaStreamSynchronize(c.stream));
+        };
+        if (dtype == UMAPB_F64) body(double{}); else body(float{});
+    });
+}
+
+int umapb_loss_grad(int dtype, size_t num_dim, const void* embedding, int32_t num_obs, const int64_t* row_ptr,
+                    const int32_t* indices, const void* weights, double a, double b, double eps_rep, int with_constant,
+                    double* loss, void* grad_embedding, double* grad_ab) {
+    return guarded([&] {
+        require_device();
+        Context& c = thread_context();
+        const int64_t nnz = host_nnz(row_ptr, num_obs, c.stream);
+        DeviceIn<int64_t> p(row_ptr, static_cast<size_t>(num_obs) + 1, c.stream);
+        DeviceIn<int32_t> ix(indices, nnz, c.stream);
+        auto body = [&](auto tag) {
+            using T = decltype(tag);
+            const size_t total = static_cast<size_t>(num_obs) * num_dim;
+            DeviceIn<T> Y(static_cast<const T*>(embedding), total, c.stream);
+            DeviceIn<T> w(static_cast<const T*>(weights), nnz, c.stream);
+            DeviceInOut<T> g(static_cast<T*>(grad_embedding), grad_embedding ? total : 0, c.stream, false);
+            loss_grad<T>(num_obs, static_cast<int>(num_dim), Y.get(), p.get(), ix.get(), w.get(), a, b, eps_rep,
+                         with_constant != 0, loss, grad_embedding ? g.get() : nullptr, grad_ab, c.stream);
+            g.finish();
+            UMAPB_CUDA(cudaStreamSynchronize(c.stream));
+        };
+        if (dtype == UMAPB_F64) body(double{}); else body(float{});
+    });
+}
+
+}  // extern "C"

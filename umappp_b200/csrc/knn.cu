@@ -1,0 +1,283 @@
+// Exact Euclidean k-nearest neighbours on the device (the role of the
+// knncolle search called at include/umappp/initialize.hpp:140).
+//
+// Candidate search (CUDA cores): one thread per query; tiles of 32 reference
+// points and 32 dimensions are staged in shared memory (queries transposed so
+// each thread reads its own column without bank conflicts, points broadcast),
+// squared distances are accumulated from coordinate differences, and each
+// thread keeps a sorted register list of its KCAP best (distance, index)
+// candidates (ties keep the smaller index, as points arrive in index order).
+//
+// Float data: the list holds k + 8 candidates in FP32; a second kernel rescores
+// them in FP64 from the original coordinates and keeps the best k by
+// (distance, index).  A query whose (k+8)-th FP32 candidate is not clear of
+// its k-th FP64 distance by more than the FP32 error bound is recomputed by
+// the FP64 kernel, so the result equals an FP64 brute force except for ties.
+// Double data: the FP64 kernel directly, with multiply and add kept separate
+// so the sums round exactly as a sequential FP64 loop.
+#include <algorithm>
+#include <cfloat>
+#include <vector>
+
+#include "stages.cuh"
+
+namespace umapb {
+
+namespace {
+
+constexpr int KNN_BLOCK = 128;  // queries per block
+constexpr int PT = 32;          // points per tile
+constexpr int CH = 32;          // dimensions per chunk
+
+__device__ __forceinline__ void add_sq(float& acc, float d) { acc = fmaf(d, d, acc); }
+__device__ __forceinline__ void add_sq(double& acc, double d) { acc = __dadd_rn(acc, __dmul_rn(d, d)); }
+
+template <typename A>
+struct Inf;
+template <>
+struct Inf<float> {
+    static __device__ __forceinline__ float v() { return CUDART_INF_F; }
+};
+template <>
+struct Inf<double> {
+    static __device__ __forceinline__ double v() { return CUDART_INF; }
+};
+
+// Sorted insertion into a register list (bd ascending); entries equal to an
+// existing distance go after it, so earlier (smaller) indices win ties.
+template <typename A, int KCAP>
+__device__ __forceinline__ void insert_sorted(A (&bd)[KCAP], int (&bi)[KCAP], A cd, int ci) {
+#pragma unroll
+    for (int i = KCAP - 1; i > 0; --i) {
+        if (cd < bd[i - 1]) {
+            bd[i] = bd[i - 1];
+            bi[i] = bi[i - 1];
+        } else if (cd < bd[i]) {
+            bd[i] = cd;
+            bi[i] = ci;
+        }
+    }
+    if (cd < bd[0]) {
+        bd[0] = cd;
+        bi[0] = ci;
+    }
+}
+
+// Brute-force candidate kernel.  T = storage type, A = accumulation type.
+// If 'queries' is non-null the block's threads take their query ids from it
+// (nq entries), else queries are 0..n-1.
+template <typename T, typename A, int KCAP>
+__global__ void __launch_bounds__(KNN_BLOCK) knn_bruteforce_kernel(const T* __restrict__ data, int32_t n, int32_t dim,
+                                                                   const int32_t* __restrict__ queries, int32_t nq,
+                                                                   int32_t* __restrict__ cand_idx,
+                                                                   A* __restrict__ cand_d2) {
+    __shared__ A qs[CH][KNN_BLOCK];
+    __shared__ A ps[PT][CH + 1];
+    const int tid = threadIdx.x;
+    const int32_t slot = blockIdx.x * KNN_BLOCK + tid;
+    const bool active = slot < nq;
+    const int32_t q = active ? (queries ? queries[slot] : slot) : 0;
+
+    A bd[KCAP];
+    int bi[KCAP];
+#pragma unroll
+    for (int i = 0; i < KCAP; ++i) {
+        bd[i] = Inf<A>::v();
+        bi[i] = -1;
+    }
+
+    for (int32_t base = 0; base < n; base += PT) {
+        A acc[PT];
+#pragma unroll
+        for (int p = 0; p < PT; ++p) acc[p] = 0;
+        for (int c0 = 0; c0 < dim; c0 += CH) {
+            const int cw = min(CH, dim - c0);
+            __syncthreads();
+            // stage this block's queries (transposed) and the point tile
+            for (int c = 0; c < cw; ++c) qs[c][tid] = active ? static_cast<A>(data[static_cast<size_t>(q) * dim + c0 + c]) : A(0);
+            for (int e = tid; e < PT * CH; e += KNN_BLOCK) {
+                const int p = e / CH, c = e % CH;
+                const int32_t j = base + p;
+                ps[p][c] = (j < n && c < cw) ? static_cast<A>(data[static_cast<size_t>(j) * dim + c0 + c]) : A(0);
+            }
+            __syncthreads();
+            for (int c = 0; c < cw; ++c) {
+                const A qv = qs[c][tid];
+#pragma unroll
+                for (int p = 0; p < PT; ++p) add_sq(acc[p], qv - ps[p][c]);
+            }
+        }
+        if (active) {
+#pragma unroll
+            for (int p = 0; p < PT; ++p) {
+                const int32_t j = base + p;
+                if (j < n && j != q && acc[p] < bd[KCAP - 1]) insert_sorted<A, KCAP>(bd, bi, acc[p], j);
+            }
+        }
+    }
+    if (active) {
+#pragma unroll
+        for (int i = 0; i < KCAP; ++i) {
+            cand_idx[static_cast<size_t>(slot) * KCAP + i] = bi[i];
+            cand_d2[static_cast<size_t>(slot) * KCAP + i] = bd[i];
+        }
+    }
+}
+
+// FP64 rescoring of the FP32 candidates of every query: keeps the best k by
+// (FP64 distance, index) and flags queries whose candidate set may miss a
+// true neighbour.
+template <int KCAP>
+__global__ void knn_rescore_kernel(const float* __restrict__ data, int32_t n, int32_t dim, int32_t k,
+                                   const int32_t* __restrict__ cand_idx, const float* __restrict__ cand_d2,
+                                   int32_t* __restrict__ out_idx, float* __restrict__ out_dist,
+                                   double* __restrict__ out_dist64, int32_t* __restrict__ redo,
+                                   int32_t* __restrict__ redo_count) {
+    const int32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    double d64[KCAP];
+    int id[KCAP];
+    const int32_t* ci = cand_idx + static_cast<size_t>(q) * KCAP;
+    const float* xq = data + static_cast<size_t>(q) * dim;
+    int m = 0;
+    for (int c = 0; c < KCAP; ++c) {
+        const int32_t j = ci[c];
+        double s = 0;
+        if (j >= 0) {
+            const float* xj = data + static_cast<size_t>(j) * dim;
+            for (int d = 0; d < dim; ++d) {
+                const double diff = static_cast<double>(xq[d]) - static_cast<double>(xj[d]);
+                s = __dadd_rn(s, __dmul_rn(diff, diff));
+            }
+        } else {
+            s = CUDART_INF;
+        }
+        // insertion by (distance, index); empty slots (j < 0) carry +inf and sort last
+        const uint32_t jkey = static_cast<uint32_t>(j);   // -1 maps above every index
+        int pos = m++;
+        while (pos > 0 && (s < d64[pos - 1] || (s == d64[pos - 1] && jkey < static_cast<uint32_t>(id[pos - 1])))) {
+            d64[pos] = d64[pos - 1];
+            id[pos] = id[pos - 1];
+            --pos;
+        }
+        d64[pos] = s;
+        id[pos] = j;
+    }
+    // Certainty check: every point outside the candidate list has FP32 distance
+    // >= the list's last FP32 value.  FP32 squared distances from differences
+    // carry relative error below (dim + 2) * 2^-24 (plus the rounding of the
+    // inputs, which is exact here); if the k-th FP64 distance could exceed the
+    // true distance of such a point, the query is recomputed in FP64.
+    const float last32 = cand_d2[static_cast<size_t>(q) * KCAP + KCAP - 1];
+    const double rel = (dim + 2) * 1.2e-7 * 2.0;
+    const double kth = d64[k - 1];
+    const bool full_list = (n - 1) <= KCAP;   // every other point is a candidate
+    if (!full_list && !(static_cast<double>(last32) * (1.0 - rel) > kth * (1.0 + rel))) {
+        const int32_t slot = atomicAdd(redo_count, 1);
+        redo[slot] = q;
+    }
+    for (int c = 0; c < k; ++c) {
+        out_idx[static_cast<size_t>(q) * k + c] = id[c];
+        const double dd = sqrt(d64[c]);
+        out_dist[static_cast<size_t>(q) * k + c] = static_cast<float>(dd);
+        if (out_dist64) out_dist64[static_cast<size_t>(q) * k + c] = dd;
+    }
+}
+
+// Writes the first k entries of FP64 candidate lists (sqrt of squared distance).
+template <typename T, int KCAP>
+__global__ void knn_emit_f64_kernel(int32_t nq, const int32_t* __restrict__ queries, int32_t k,
+                                    const int32_t* __restrict__ cand_idx, const double* __restrict__ cand_d2,
+                                    int32_t* __restrict__ out_idx, T* __restrict__ out_dist,
+                                    double* __restrict__ out_dist64) {
+    const int32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= nq) return;
+    const int32_t q = queries ? queries[slot] : slot;
+    for (int c = 0; c < k; ++c) {
+        out_idx[static_cast<size_t>(q) * k + c] = cand_idx[static_cast<size_t>(slot) * KCAP + c];
+        const double dd = sqrt(cand_d2[static_cast<size_t>(slot) * KCAP + c]);
+        out_dist[static_cast<size_t>(q) * k + c] = static_cast<T>(dd);
+        if (out_dist64) out_dist64[static_cast<size_t>(q) * k + c] = dd;
+    }
+}
+
+template <typename T, int KCAP>
+void run_f64(const T* data, int32_t n, int32_t dim, int32_t k, const int32_t* queries, int32_t nq, int32_t* out_idx,
+             T* out_dist, double* out_dist64, cudaStream_t s) {
+    if (nq <= 0) return;
+    DevArray<int32_t> ci(static_cast<size_t>(nq) * KCAP, s);
+    DevArray<double> cd(static_cast<size_t>(nq) * KCAP, s);
+    knn_bruteforce_kernel<T, double, KCAP><<<(nq + KNN_BLOCK - 1) / KNN_BLOCK, KNN_BLOCK, 0, s>>>(
+        data, n, dim, queries, nq, ci.get(), cd.get());
+    UMAPB_LAUNCH_CHECK();
+    knn_emit_f64_kernel<T, KCAP><<<(nq + 127) / 128, 128, 0, s>>>(nq, queries, k, ci.get(), cd.get(), out_idx, out_dist,
+                                                                  out_dist64);
+    UMAPB_LAUNCH_CHECK();
+}
+
+template <int KCAP>
+void run_f32(const float* data, int32_t n, int32_t dim, int32_t k, int32_t* out_idx, float* out_dist,
+             double* out_dist64, cudaStream_t s) {
+    DevArray<int32_t> ci(static_cast<size_t>(n) * KCAP, s);
+    DevArray<float> cd(static_cast<size_t>(n) * KCAP, s);
+    knn_bruteforce_kernel<float, float, KCAP><<<(n + KNN_BLOCK - 1) / KNN_BLOCK, KNN_BLOCK, 0, s>>>(
+        data, n, dim, nullptr, n, ci.get(), cd.get());
+    UMAPB_LAUNCH_CHECK();
+    DevArray<int32_t> redo(n, s), redo_count(1, s);
+    redo_count.zero(s);
+    knn_rescore_kernel<KCAP><<<(n + 127) / 128, 128, 0, s>>>(data, n, dim, k, ci.get(), cd.get(), out_idx, out_dist,
+                                                             out_dist64, redo.get(), redo_count.get());
+    UMAPB_LAUNCH_CHECK();
+    int32_t nredo = 0;
+    UMAPB_CUDA(cudaMemcpyAsync(&nredo, redo_count.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+    if (nredo > 0) {
+        // exact FP64 search for the uncertain queries (same output rows)
+        if (k + 8 <= 32) {
+            run_f64<float, 32>(data, n, dim, k, redo.get(), nredo, out_idx, out_dist, out_dist64, s);
+        } else if (k + 8 <= 64) {
+            run_f64<float, 64>(data, n, dim, k, redo.get(), nredo, out_idx, out_dist, out_dist64, s);
+        } else {
+            run_f64<float, 128>(data, n, dim, k, redo.get(), nredo, out_idx, out_dist, out_dist64, s);
+        }
+    }
+}
+
+}  // namespace
+
+template <typename T>
+void knn_exact(const T* data, int32_t n, int32_t dim, int32_t k, int32_t* out_idx, T* out_dist, cudaStream_t s,
+               double* out_dist_f64) {
+    require(n >= 2, "the neighbour search needs at least two observations");
+    require(dim >= 1, "data_dim must be positive");
+    require(k >= 1 && k < n, "num_neighbors must be in [1, num_obs)");
+    require(k <= 120, "num_neighbors above 120 is not supported by the device search");
+    if constexpr (std::is_same<T, float>::value) {
+        if (k + 8 <= 16) {
+            run_f32<16>(data, n, dim, k, out_idx, out_dist, out_dist_f64, s);
+        } else if (k + 8 <= 24) {
+            run_f32<24>(data, n, dim, k, out_idx, out_dist, out_dist_f64, s);
+        } else if (k + 8 <= 32) {
+            run_f32<32>(data, n, dim, k, out_idx, out_dist, out_dist_f64, s);
+        } else if (k + 8 <= 64) {
+            run_f32<64>(data, n, dim, k, out_idx, out_dist, out_dist_f64, s);
+        } else {
+            run_f32<128>(data, n, dim, k, out_idx, out_dist, out_dist_f64, s);
+        }
+    } else {
+        if (k <= 16) {
+            run_f64<double, 16>(data, n, dim, k, nullptr, n, out_idx, out_dist, out_dist_f64, s);
+        } else if (k <= 32) {
+            run_f64<double, 32>(data, n, dim, k, nullptr, n, out_idx, out_dist, out_dist_f64, s);
+        } else if (k <= 64) {
+            run_f64<double, 64>(data, n, dim, k, nullptr, n, out_idx, out_dist, out_dist_f64, s);
+        } else {
+            run_f64<double, 128>(data, n, dim, k, nullptr, n, out_idx, out_dist, out_dist_f64, s);
+        }
+    }
+}
+
+template void knn_exact<float>(const float*, int32_t, int32_t, int32_t, int32_t*, float*, cudaStream_t, double*);
+template void knn_exact<double>(const double*, int32_t, int32_t, int32_t, int32_t*, double*, cudaStream_t, double*);
+
+}  // namespace umapb

@@ -1,0 +1,555 @@
+// optimize_layout on the device (include/umappp/optimize_layout.hpp:116-185).
+//
+// Schedule.  Which edges fire in an epoch, and how many negative samples each
+// draws, depends only on the per-edge schedule (epochs_per_sample and the two
+// running epoch_of_next_* values), never on the layout.  So the schedule is
+// advanced by itself, in the reference's exact Float_ arithmetic (this file is
+// compiled with -fmad=false), and its firing events are written out for a
+// window of epochs as compact per-epoch lists of (head, tail, #negatives) in
+// the edges' CSR order.  Two passes over the edges build a window: one counts
+// events per (epoch, block), an exclusive scan places them, the second
+// writes them.  The window is sized to a device-memory budget (the whole run
+// fits at a million observations on a 180 GB part).
+//
+// Epoch kernel.  One thread per firing event: the attractive step moves the
+// head (in registers) and the tail (vector atomic add); then the head takes
+// its negative samples in sequence, as the reference does, and its total
+// displacement is added atomically.  Negative samples come from Philox4x32-10
+// keyed by the seed with counter (head, tail, epoch, block), so they do not
+// depend on the launch shape or on how epochs are split across run() calls.
+// Updates of different events race (Hogwild-style), as in any parallel SGD of
+// this kind; per-event arithmetic follows optimize_layout.hpp:145-179.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cfloat>
+#include <type_traits>
+#include <vector>
+
+#include "stages.cuh"
+
+namespace umapb {
+
+namespace {
+
+constexpr int SCHED_BLOCK = 256;
+constexpr int MAX_WINDOW = 512;
+constexpr int MAX_GENERIC_DIM = 64;
+
+template <typename T>
+struct FloatLimits;
+template <>
+struct FloatLimits<float> {
+    static __device__ __forceinline__ float epsilon() { return FLT_EPSILON; }
+};
+template <>
+struct FloatLimits<double> {
+    static __device__ __forceinline__ double epsilon() { return DBL_EPSILON; }
+};
+
+// One schedule step of edge j at 'epoch' (optimize_layout.hpp:141-143,160-161,178-179).
+template <typename T>
+__device__ __forceinline__ bool schedule_step(T epoch, T eps, T epns, T& enext, T& enneg, int& nneg) {
+    if (enext > epoch) return false;
+    nneg = static_cast<int>((epoch - enneg) / epns);
+    enext += eps;
+    enneg += static_cast<T>(nneg) * epns;
+    return true;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(SCHED_BLOCK) sched_count_kernel(int64_t nnz, const T* __restrict__ eps,
+                                                                  const T* __restrict__ enext_in,
+                                                                  const T* __restrict__ enneg_in, T rate, int e0, int W,
+                                                                  int64_t* __restrict__ counts) {
+    const int64_t j = static_cast<int64_t>(blockIdx.x) * SCHED_BLOCK + threadIdx.x;
+    const bool valid = j < nnz;
+    const T ep = valid ? eps[j] : T(1);
+    const T epns = ep / rate;
+    T en = valid ? enext_in[j] : T(0);
+    T enn = valid ? enneg_in[j] : T(0);
+    for (int w = 0; w < W; ++w) {
+        int nn = 0;
+        const bool fire = valid && schedule_step<T>(static_cast<T>(e0 + w), ep, epns, en, enn, nn);
+        const int c = __syncthreads_count(fire);
+        if (threadIdx.x == 0) counts[static_cast<int64_t>(w) * gridDim.x + blockIdx.x] = c;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(SCHED_BLOCK) sched_write_kernel(int64_t nnz, const int32_t* __restrict__ heads,
+                                                                  const int32_t* __restrict__ targets,
+                                                                  const T* __restrict__ eps, T* __restrict__ enext_st,
+                                                                  T* __restrict__ enneg_st, T rate, int e0, int W,
+                                                                  const int64_t* __restrict__ offsets,
+                                                                  int2* __restrict__ ht, uint16_t* __restrict__ nneg_out,
+                                                                  int* __restrict__ status) {
+    __shared__ int warp_counts[SCHED_BLOCK / 32];
+    const int64_t j = static_cast<int64_t>(blockIdx.x) * SCHED_BLOCK + threadIdx.x;
+    const bool valid = j < nnz;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const T ep = valid ? eps[j] : T(1);
+    const T epns = ep / rate;
+    T en = valid ? enext_st[j] : T(0);
+    T enn = valid ? enneg_st[j] : T(0);
+    const int2 pair = valid ? make_int2(heads[j], targets[j]) : make_int2(0, 0);
+    for (int w = 0; w < W; ++w) {
+        int nn = 0;
+        const bool fire = valid && schedule_step<T>(static_cast<T>(e0 + w), ep, epns, en, enn, nn);
+        const unsigned mask = __ballot_sync(0xffffffffu, fire);
+        if (lane == 0) warp_counts[warp] = __popc(mask);
+        __syncthreads();
+        if (fire) {
+            int before = 0;
+            for (int q = 0; q < warp; ++q) before += warp_counts[q];
+            const int64_t pos = offsets[static_cast<int64_t>(w) * gridDim.x + blockIdx.x] + before +
+                                __popc(mask & ((1u << lane) - 1u));
+            ht[pos] = pair;
+            if (nn < 0) nn = 0;   // a negative count draws nothing, as in the reference's loop
+            if (nn > 65535) {
+                atomicExch(status, DEV_BAD_INPUT);
+                nn = 65535;
+            }
+            nneg_out[pos] = static_cast<uint16_t>(nn);
+        }
+        __syncthreads();
+    }
+    if (valid) {
+        enext_st[j] = en;
+        enneg_st[j] = enn;
+    }
+}
+
+// Advances the schedule state by W epochs without recording events.
+template <typename T>
+__global__ void sched_advance_kernel(int64_t nnz, const T* __restrict__ eps, T* __restrict__ enext, T* __restrict__ enneg,
+                                     T rate, int e0, int W) {
+    for (int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; j < nnz; j += int64_t(gridDim.x) * blockDim.x) {
+        const T ep = eps[j];
+        const T epns = ep / rate;
+        T en = enext[j], enn = enneg[j];
+        for (int w = 0; w < W; ++w) {
+            int nn;
+            schedule_step<T>(static_cast<T>(e0 + w), ep, epns, en, enn, nn);
+        }
+        enext[j] = en;
+        enneg[j] = enn;
+    }
+}
+
+// Per-epoch totals of firing edges and negative samples.
+template <typename T>
+__global__ void __launch_bounds__(SCHED_BLOCK) sched_totals_kernel(int64_t nnz, const T* __restrict__ eps,
+                                                                   T* __restrict__ enext, T* __restrict__ enneg, T rate,
+                                                                   int e0, int W,
+                                                                   unsigned long long* __restrict__ totals) {
+    typedef cub::BlockReduce<unsigned long long, SCHED_BLOCK> Reduce;
+    __shared__ typename Reduce::TempStorage tmp;
+    const int64_t j = static_cast<int64_t>(blockIdx.x) * SCHED_BLOCK + threadIdx.x;
+    const bool valid = j < nnz;
+    const T ep = valid ? eps[j] : T(1);
+    const T epns = ep / rate;
+    T en = valid ? enext[j] : T(0);
+    T enn = valid ? enneg[j] : T(0);
+    for (int w = 0; w < W; ++w) {
+        int nn = 0;
+        const bool fire = valid && schedule_step<T>(static_cast<T>(e0 + w), ep, epns, en, enn, nn);
+        const int c = __syncthreads_count(fire);
+        const unsigned long long negs = Reduce(tmp).Sum(fire && nn > 0 ? static_cast<unsigned long long>(nn) : 0ull);
+        if (threadIdx.x == 0) {
+            atomicAdd(&totals[2 * w], static_cast<unsigned long long>(c));
+            atomicAdd(&totals[2 * w + 1], negs);
+        }
+        __syncthreads();
+    }
+    if (valid) {
+        enext[j] = en;
+        enneg[j] = enn;
+    }
+}
+
+__global__ void gather_epoch_starts_kernel(const int64_t* __restrict__ offsets, int64_t nblocks, int W,
+                                           int64_t total_last, int64_t* __restrict__ starts) {
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w <= W; w += gridDim.x * blockDim.x) {
+        starts[w] = (w < W) ? offsets[static_cast<int64_t>(w) * nblocks] : total_last;
+    }
+}
+
+// ---------------------------------------------------------- epoch kernel --
+
+template <typename T>
+struct SgdParams {
+    T a, b;
+    T neg2ab;      // -2ab
+    T gamma2b;     // 2 gamma b
+    T alpha;
+    uint32_t k0, k1;
+    uint32_t epoch;
+    int32_t n;
+};
+
+// Counter-based negative-sample stream of one event.
+struct NegStream {
+    uint32_t c0, c1, c2, c3, k0, k1;
+    Philox4 buf;
+    int used;
+    __device__ __forceinline__ NegStream(uint32_t h, uint32_t t, uint32_t epoch, uint32_t key0, uint32_t key1)
+        : c0(h), c1(t), c2(epoch), c3(0), k0(key0), k1(key1), used(4) {}
+    __device__ __forceinline__ uint32_t next() {
+        if (used == 4) {
+            buf = philox4x32_10(c0, c1, c2, c3++, k0, k1);
+            used = 0;
+        }
+        return buf.v[used++];
+    }
+    // Exactly uniform integer in [0, n) (Lemire, "Fast random integer generation
+    // in an interval", ACM TOMACS 2019): multiply-shift with rejection.
+    __device__ __forceinline__ int32_t bounded(uint32_t n) {
+        uint64_t m = static_cast<uint64_t>(next()) * n;
+        uint32_t l = static_cast<uint32_t>(m);
+        if (l < n) {
+            const uint32_t thr = (0u - n) % n;
+            while (l < thr) {
+                m = static_cast<uint64_t>(next()) * n;
+                l = static_cast<uint32_t>(m);
+            }
+        }
+        return static_cast<int32_t>(m >> 32);
+    }
+};
+
+template <typename T>
+__device__ __forceinline__ T clamp4(T g) {
+    g = (g < T(-4)) ? T(-4) : g;
+    return (T(4) < g) ? T(4) : g;
+}
+
+__device__ __forceinline__ float pow_b(float x, float b) { return powf(x, b); }
+__device__ __forceinline__ double pow_b(double x, double b) { return pow(x, b); }
+
+// Attractive coefficient, optimize_layout.hpp:147-149.
+template <typename T>
+__device__ __forceinline__ T attract_coef(T d2, const SgdParams<T>& p) {
+    const T pd2b = pow_b(d2, p.b);
+    return (p.neg2ab * pd2b) / (d2 * (p.a * pd2b + T(1)));
+}
+
+// Repulsive coefficient, optimize_layout.hpp:170-171.
+template <typename T>
+__device__ __forceinline__ T repulse_coef(T d2, const SgdParams<T>& p) {
+    return p.gamma2b / ((T(0.001) + d2) * (p.a * pow_b(d2, p.b) + T(1)));
+}
+
+template <typename T>
+__device__ __forceinline__ T floor_eps(T d2) {
+    const T e = FloatLimits<T>::epsilon();
+    return (e < d2) ? d2 : e;
+}
+
+// Two-dimensional layouts: float2 coordinates, one vector atomic per update.
+__global__ void __launch_bounds__(256) sgd_epoch_2d_f32(const int64_t* __restrict__ starts, int w,
+                                                        const int2* __restrict__ ht, const uint16_t* __restrict__ nneg,
+                                                        float2* __restrict__ Y, SgdParams<float> p) {
+    const int64_t begin = starts[w], end = starts[w + 1];
+    for (int64_t e = begin + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < end; e += int64_t(gridDim.x) * blockDim.x) {
+        const int2 pr = ht[e];
+        const int nn = nneg[e];
+        const float2 y0 = __ldcg(&Y[pr.x]);
+        const float2 yt = __ldcg(&Y[pr.y]);
+        float hx = y0.x, hy = y0.y;
+        {
+            const float dx = hx - yt.x, dy = hy - yt.y;
+            const float d2 = floor_eps(dx * dx + dy * dy);
+            const float c = attract_coef(d2, p);
+            const float gx = p.alpha * clamp4(c * dx);
+            const float gy = p.alpha * clamp4(c * dy);
+            hx += gx;
+            hy += gy;
+            atomicAdd(&Y[pr.y], make_float2(-gx, -gy));
+        }
+        if (nn > 0) {
+            NegStream rng(static_cast<uint32_t>(pr.x), static_cast<uint32_t>(pr.y), p.epoch, p.k0, p.k1);
+            for (int q = 0; q < nn; ++q) {
+                const int32_t k = rng.bounded(static_cast<uint32_t>(p.n));
+                if (k == pr.x) continue;
+                const float2 yk = __ldcg(&Y[k]);
+                const float dx = hx - yk.x, dy = hy - yk.y;
+                const float d2 = floor_eps(dx * dx + dy * dy);
+                const float c = repulse_coef(d2, p);
+                hx += p.alpha * clamp4(c * dx);
+                hy += p.alpha * clamp4(c * dy);
+            }
+        }
+        atomicAdd(&Y[pr.x], make_float2(hx - y0.x, hy - y0.y));
+    }
+}
+
+// Any dimension (up to MAX_GENERIC_DIM) and either precision.
+template <typename T>
+__global__ void __launch_bounds__(128) sgd_epoch_generic(const int64_t* __restrict__ starts, int w,
+                                                         const int2* __restrict__ ht, const uint16_t* __restrict__ nneg,
+                                                         T* __restrict__ Y, int dim, SgdParams<T> p) {
+    const int64_t begin = starts[w], end = starts[w + 1];
+    T head[MAX_GENERIC_DIM], orig[MAX_GENERIC_DIM];
+    for (int64_t e = begin + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < end; e += int64_t(gridDim.x) * blockDim.x) {
+        const int2 pr = ht[e];
+        const int nn = nneg[e];
+        T* yh = Y + static_cast<size_t>(pr.x) * dim;
+        T* yt = Y + static_cast<size_t>(pr.y) * dim;
+        T d2 = 0;
+        for (int d = 0; d < dim; ++d) {
+            head[d] = orig[d] = __ldcg(yh + d);
+            const T diff = head[d] - __ldcg(yt + d);
+            d2 += diff * diff;
+        }
+        {
+            const T c = attract_coef(floor_eps(d2), p);
+            for (int d = 0; d < dim; ++d) {
+                const T g = p.alpha * clamp4(c * (head[d] - __ldcg(yt + d)));
+                head[d] += g;
+                atomicAdd(yt + d, -g);
+            }
+        }
+        if (nn > 0) {
+            NegStream rng(static_cast<uint32_t>(pr.x), static_cast<uint32_t>(pr.y), p.epoch, p.k0, p.k1);
+            for (int q = 0; q < nn; ++q) {
+                const int32_t k = rng.bounded(static_cast<uint32_t>(p.n));
+                if (k == pr.x) continue;
+                const T* yk = Y + static_cast<size_t>(k) * dim;
+                T dd2 = 0;
+                for (int d = 0; d < dim; ++d) {
+                    const T diff = head[d] - __ldcg(yk + d);
+                    dd2 += diff * diff;
+                }
+                const T c = repulse_coef(floor_eps(dd2), p);
+                for (int d = 0; d < dim; ++d) head[d] += p.alpha * clamp4(c * (head[d] - __ldcg(yk + d)));
+            }
+        }
+        for (int d = 0; d < dim; ++d) atomicAdd(yh + d, head[d] - orig[d]);
+    }
+}
+
+int sm_count() {
+    static int count = 0;
+    if (count == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev);
+        if (count <= 0) count = 148;
+    }
+    return count;
+}
+
+}  // namespace
+
+template <typename T>
+void SgdEngine<T>::setup(const DeviceEpochs<T>* ep, cudaStream_t s, int base_epoch) {
+    ep_ = ep;
+    base_epoch_ = base_epoch;
+    require(static_cast<double>(ep->negative_sample_rate) <= 30000.0,
+            "negative_sample_rate above 30000 is not supported");
+    enext_.allocate(ep->nnz, s);
+    enneg_.allocate(ep->nnz, s);
+    if (ep->nnz) {
+        UMAPB_CUDA(cudaMemcpyAsync(enext_.get(), ep->enext0.get(), ep->nnz * sizeof(T), cudaMemcpyDeviceToDevice, s));
+        UMAPB_CUDA(cudaMemcpyAsync(enneg_.get(), ep->enneg0.get(), ep->nnz * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    }
+    state_epoch_ = base_epoch_;
+    window_begin_ = window_end_ = base_epoch_;
+    ht_.release();
+    nneg_.release();
+    epoch_offsets_.release();
+    host_epoch_offsets_.clear();
+}
+
+template <typename T>
+void SgdEngine<T>::state_at(int epoch, T* enext, T* enneg, cudaStream_t s) {
+    const int64_t nnz = ep_->nnz;
+    if (nnz == 0) return;
+    require(epoch >= base_epoch_, "schedule state requested before its starting epoch");
+    UMAPB_CUDA(cudaMemcpyAsync(enext, ep_->enext0.get(), nnz * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    UMAPB_CUDA(cudaMemcpyAsync(enneg, ep_->enneg0.get(), nnz * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    if (epoch > base_epoch_) {
+        sched_advance_kernel<T><<<grid_for(nnz, 256), 256, 0, s>>>(nnz, ep_->eps.get(), enext, enneg,
+                                                                   ep_->negative_sample_rate, base_epoch_,
+                                                                   epoch - base_epoch_);
+        UMAPB_LAUNCH_CHECK();
+    }
+}
+
+template <typename T>
+void SgdEngine<T>::build_window(int first, int last_wanted, cudaStream_t s) {
+    const int64_t nnz = ep_->nnz;
+    // bring the state to 'first'
+    if (state_epoch_ != first) {
+        if (state_epoch_ > first) {
+            state_at(first, enext_.get(), enneg_.get(), s);
+        } else if (nnz) {
+            sched_advance_kernel<T><<<grid_for(nnz, 256), 256, 0, s>>>(nnz, ep_->eps.get(), enext_.get(), enneg_.get(),
+                                                                       ep_->negative_sample_rate, state_epoch_,
+                                                                       first - state_epoch_);
+            UMAPB_LAUNCH_CHECK();
+        }
+        state_epoch_ = first;
+    }
+    const int W = std::min(last_wanted - first, MAX_WINDOW);
+    const int64_t nblocks = std::max<int64_t>((nnz + SCHED_BLOCK - 1) / SCHED_BLOCK, 1);
+    require(nblocks <= INT32_MAX, "too many edges", UMAPB_ERR_OVERFLOW);
+    const int64_t ncount = nblocks * W;
+    DevArray<int64_t> counts(ncount, s), offsets(ncount, s);
+    if (nnz) {
+        sched_count_kernel<T><<<static_cast<unsigned>(nblocks), SCHED_BLOCK, 0, s>>>(
+            nnz, ep_->eps.get(), enext_.get(), enneg_.get(), ep_->negative_sample_rate, first, W, counts.get());
+        UMAPB_LAUNCH_CHECK();
+    } else {
+        counts.zero(s);
+    }
+    {
+        size_t tb = 0;
+        UMAPB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, counts.get(), offsets.get(), ncount, s));
+        DevArray<unsigned char> temp(tb, s);
+        UMAPB_CUDA(cub::DeviceScan::ExclusiveSum(temp.get(), tb, counts.get(), offsets.get(), ncount, s));
+    }
+    int64_t last_off = 0, last_cnt = 0;
+    UMAPB_CUDA(cudaMemcpyAsync(&last_off, offsets.get() + ncount - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaMemcpyAsync(&last_cnt, counts.get() + ncount - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+    DevArray<int64_t> starts(W + 1, s);
+    gather_epoch_starts_kernel<<<grid_for(W + 1, 128), 128, 0, s>>>(offsets.get(), nblocks, W, last_off + last_cnt,
+                                                                     starts.get());
+    UMAPB_LAUNCH_CHECK();
+    std::vector<int64_t> h(W + 1);
+    UMAPB_CUDA(cudaMemcpyAsync(h.data(), starts.get(), (W + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+
+    // fit the window to the memory budget
+    size_t budget = event_budget_bytes;
+    if (budget == 0) {
+        size_t free_b = 0, total_b = 0;
+        UMAPB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        budget = free_b / 3;
+    }
+    const size_t per_event = sizeof(int2) + sizeof(uint16_t);
+    int Wk = W;
+    while (Wk > 1 && static_cast<size_t>(h[Wk]) * per_event > budget) --Wk;
+    const int64_t events = h[Wk];
+
+    ht_.release();
+    nneg_.release();
+    ht_.allocate(events, s);
+    nneg_.allocate(events, s);
+    DevArray<int> status(1, s);
+    status.zero(s);
+    if (nnz) {
+        sched_write_kernel<T><<<static_cast<unsigned>(nblocks), SCHED_BLOCK, 0, s>>>(
+            nnz, ep_->heads.get(), ep_->targets.get(), ep_->eps.get(), enext_.get(), enneg_.get(),
+            ep_->negative_sample_rate, first, Wk, offsets.get(), ht_.get(), nneg_.get(), status.get());
+        UMAPB_LAUNCH_CHECK();
+    }
+    epoch_offsets_.allocate(Wk + 1, s);
+    UMAPB_CUDA(cudaMemcpyAsync(epoch_offsets_.get(), h.data(), (Wk + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    host_epoch_offsets_.assign(h.begin(), h.begin() + Wk + 1);
+    int st = 0;
+    UMAPB_CUDA(cudaMemcpyAsync(&st, status.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+    require(st == DEV_OK, "a negative-sample count exceeded 65535");
+    window_begin_ = first;
+    window_end_ = first + Wk;
+    state_epoch_ = window_end_;
+}
+
+template <typename T>
+void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double b, double gamma, double learning_rate,
+                       uint64_t seed, cudaStream_t s, float* ms_schedule, float* ms_sgd) {
+    if (ms_schedule) *ms_schedule = 0;
+    if (ms_sgd) *ms_sgd = 0;
+    if (last <= first) return;
+    require(num_dim >= 1 && num_dim <= MAX_GENERIC_DIM, "num_dim must be between 1 and 64");
+    const int total = ep_->total_epochs;
+    SgdParams<T> p;
+    p.a = static_cast<T>(a);
+    p.b = static_cast<T>(b);
+    p.neg2ab = T(-2) * p.a * p.b;
+    p.gamma2b = T(2) * static_cast<T>(gamma) * p.b;
+    p.k0 = static_cast<uint32_t>(seed) ^ RNG_NEGATIVE;
+    p.k1 = static_cast<uint32_t>(seed >> 32);
+    p.n = ep_->n;
+    const T lr = static_cast<T>(learning_rate);
+
+    cudaEvent_t ev[4];
+    for (auto& e : ev) UMAPB_CUDA(cudaEventCreate(&e));
+    float sched_ms = 0, sgd_ms = 0;
+    const int blocks_2d = sm_count() * 8;
+    const int blocks_gen = sm_count() * 8;
+    int e = first;
+    while (e < last) {
+        if (e < window_begin_ || e >= window_end_) {
+            UMAPB_CUDA(cudaEventRecord(ev[0], s));
+            build_window(e, last, s);
+            UMAPB_CUDA(cudaEventRecord(ev[1], s));
+            UMAPB_CUDA(cudaEventSynchronize(ev[1]));
+            float t = 0;
+            UMAPB_CUDA(cudaEventElapsedTime(&t, ev[0], ev[1]));
+            sched_ms += t;
+        }
+        const int stop = std::min(last, window_end_);
+        UMAPB_CUDA(cudaEventRecord(ev[2], s));
+        for (; e < stop; ++e) {
+            // alpha = lr * (1 - epoch / num_epochs) in the reference's types (optimize_layout.hpp:132-133)
+            const T epoch_t = static_cast<T>(e);
+            p.alpha = static_cast<T>(static_cast<double>(lr) * (1.0 - static_cast<double>(epoch_t / static_cast<T>(total))));
+            p.epoch = static_cast<uint32_t>(e);
+            const int w = e - window_begin_;
+            const int64_t nev = host_epoch_offsets_[w + 1] - host_epoch_offsets_[w];
+            if (nev == 0) continue;
+            bool done = false;
+            if constexpr (std::is_same<T, float>::value) {
+                if (num_dim == 2) {
+                    const unsigned g = grid_for(nev, 256, blocks_2d);
+                    sgd_epoch_2d_f32<<<g, 256, 0, s>>>(epoch_offsets_.get(), w, ht_.get(), nneg_.get(),
+                                                       reinterpret_cast<float2*>(Y), p);
+                    done = true;
+                }
+            }
+            if (!done) {
+                const unsigned g = grid_for(nev, 128, blocks_gen);
+                sgd_epoch_generic<T><<<g, 128, 0, s>>>(epoch_offsets_.get(), w, ht_.get(), nneg_.get(), Y, num_dim, p);
+            }
+            UMAPB_LAUNCH_CHECK();
+        }
+        UMAPB_CUDA(cudaEventRecord(ev[3], s));
+        UMAPB_CUDA(cudaEventSynchronize(ev[3]));
+        float t = 0;
+        UMAPB_CUDA(cudaEventElapsedTime(&t, ev[2], ev[3]));
+        sgd_ms += t;
+    }
+    for (auto& x : ev) cudaEventDestroy(x);
+    if (ms_schedule) *ms_schedule = sched_ms;
+    if (ms_sgd) *ms_sgd = sgd_ms;
+}
+
+template <typename T>
+void SgdEngine<T>::counts(int first, int last, int64_t* out, cudaStream_t s) {
+    const int64_t nnz = ep_->nnz;
+    const int W = last - first;
+    if (W <= 0) return;
+    DevArray<T> en(nnz, s), enn(nnz, s);
+    state_at(first, en.get(), enn.get(), s);
+    DevArray<unsigned long long> totals(2 * static_cast<size_t>(W), s);
+    totals.zero(s);
+    if (nnz) {
+        const int64_t nblocks = (nnz + SCHED_BLOCK - 1) / SCHED_BLOCK;
+        sched_totals_kernel<T><<<static_cast<unsigned>(nblocks), SCHED_BLOCK, 0, s>>>(
+            nnz, ep_->eps.get(), en.get(), enn.get(), ep_->negative_sample_rate, first, W, totals.get());
+        UMAPB_LAUNCH_CHECK();
+    }
+    std::vector<unsigned long long> h(2 * static_cast<size_t>(W));
+    UMAPB_CUDA(cudaMemcpyAsync(h.data(), totals.get(), h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+    for (size_t i = 0; i < h.size(); ++i) out[i] = static_cast<int64_t>(h[i]);
+}
+
+template class SgdEngine<float>;
+template class SgdEngine<double>;
+
+}  // namespace umapb

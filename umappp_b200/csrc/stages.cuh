@@ -1,0 +1,120 @@
+// Device-side stage functions of the UMAP pipeline.  All pointers are device
+// pointers; all work is enqueued on the given stream.  Float_ is the storage
+// type of distances, weights, schedules and embeddings (float or double).
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace umapb {
+
+// Weighted graph / neighbour list in CSR form, owned on the device.
+template <typename T>
+struct DeviceCsr {
+    int32_t n = 0;
+    int64_t nnz = 0;
+    DevArray<int64_t> ptr;
+    DevArray<int32_t> idx;
+    DevArray<T> val;
+};
+
+// The reference's EpochData (include/umappp/optimize_layout.hpp:27-45) on the
+// device, plus the head (row) of every edge.
+template <typename T>
+struct DeviceEpochs {
+    int32_t n = 0;
+    int64_t nnz = 0;
+    int total_epochs = 0;
+    T negative_sample_rate = 0;
+    DevArray<int64_t> ptr;
+    DevArray<int32_t> heads;
+    DevArray<int32_t> targets;
+    DevArray<T> eps;     // epochs_per_sample
+    DevArray<T> enext0;  // epoch_of_next_sample at epoch 0
+    DevArray<T> enneg0;  // epoch_of_next_negative_sample at epoch 0
+};
+
+// ---- kNN (knn.cu) ----------------------------------------------------------
+// Exact Euclidean neighbours: out_idx/out_dist are n x k row-major, sorted by
+// (distance, index), self excluded.  Float data: FP32 candidate search then
+// FP64 rescoring of the candidate set; double data: FP64 throughout.
+template <typename T>
+void knn_exact(const T* data, int32_t n, int32_t dim, int32_t k, int32_t* out_idx, T* out_dist, cudaStream_t s,
+               double* out_dist_f64 = nullptr);
+
+// ---- similarities (similarities.cu) -----------------------------------------
+template <typename T>
+void neighbor_similarities(int32_t n, const int64_t* ptr, T* val, double local_connectivity, double bandwidth,
+                           double min_k_dist_scale, bool use_newton, double* rho_out, double* sigma_out,
+                           cudaStream_t s);
+
+// ---- graph (graph.cu) -------------------------------------------------------
+template <typename T>
+void combine_neighbor_sets(int32_t n, const int64_t* ptr, const int32_t* idx, const T* w, int64_t nnz_in,
+                           double mix_ratio, DeviceCsr<T>& out, cudaStream_t s);
+
+template <typename T>
+void similarities_to_epochs(int32_t n, const int64_t* ptr, const int32_t* idx, const T* w, int64_t nnz,
+                            int num_epochs, double negative_sample_rate, DeviceEpochs<T>& out, cudaStream_t s);
+
+// Number of connected components (undirected union-find); status word set on timeout.
+int64_t count_components(int32_t n, const int64_t* ptr, const int32_t* idx, int* d_status, cudaStream_t s);
+
+// ---- initial layouts (spectral.cu) -------------------------------------------
+struct SpectralResult {
+    bool ok = false;
+    int restarts = 0;
+    double evals[64] = {0};
+};
+
+template <typename T>
+SpectralResult spectral_init(int32_t n, const int64_t* ptr, const int32_t* idx, const T* w, int num_dim, T* Y,
+                             int extra_work, int max_iterations, double tol, double scale, bool jitter,
+                             double jitter_sd, uint64_t seed, int* d_status, cudaStream_t s);
+
+template <typename T>
+void random_init(int32_t n, int num_dim, T* Y, uint64_t seed, double scale, cudaStream_t s);
+
+// ---- SGD (sgd.cu) -----------------------------------------------------------
+// Per-epoch event lists of the deterministic schedule, precomputed for a
+// window of epochs: event e of epoch w is (head, tail, negative-sample count),
+// stored in CSR order of the edges.
+template <typename T>
+class SgdEngine {
+public:
+    // ep->enext0 / enneg0 describe the schedule at epoch 'base_epoch'.
+    void setup(const DeviceEpochs<T>* ep, cudaStream_t s, int base_epoch = 0);
+    // Runs epochs [first, last) on Y (n x num_dim, device).
+    void run(T* Y, int num_dim, int first, int last, double a, double b, double gamma, double learning_rate,
+             uint64_t seed, cudaStream_t s, float* ms_schedule, float* ms_sgd);
+    // Exact per-epoch [firing, negatives] counts over [first, last) (host output).
+    void counts(int first, int last, int64_t* out, cudaStream_t s);
+    // Schedule state (enext, enneg) at 'epoch' into device arrays.
+    void state_at(int epoch, T* enext, T* enneg, cudaStream_t s);
+    size_t event_budget_bytes = 0;  // 0: one third of free device memory
+
+private:
+    void build_window(int first, int last_wanted, cudaStream_t s);
+    const DeviceEpochs<T>* ep_ = nullptr;
+    int base_epoch_ = 0;
+    DevArray<T> enext_, enneg_;    // schedule state at state_epoch_
+    int state_epoch_ = 0;          // epoch the state arrays describe
+    int window_begin_ = 0, window_end_ = 0;
+    DevArray<int2> ht_;
+    DevArray<uint16_t> nneg_;
+    DevArray<int64_t> epoch_offsets_;   // window_end_ - window_begin_ + 1 entries
+    std::vector<int64_t> host_epoch_offsets_;
+};
+
+// ---- adjoint (adjoint.cu) ----------------------------------------------------
+template <typename T>
+void loss_grad(int32_t n, int num_dim, const T* Y, const int64_t* ptr, const int32_t* idx, const T* w, double a,
+               double b, double eps_rep, bool with_constant, double* loss_out, T* grad_Y, double* grad_ab,
+               cudaStream_t s);
+
+// ---- host (find_ab.cpp) -------------------------------------------------------
+void find_ab(double spread, double min_dist, double* a, double* b);
+int choose_num_epochs(bool has_value, int value, int64_t n);
+
+}  // namespace umapb
