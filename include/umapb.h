@@ -177,6 +177,10 @@ void umapb_status_free(umapb_status* st);
 int umapb_knn(int dtype, size_t data_dim, int32_t num_obs, const void* data, int k, int32_t* out_indices,
               void* out_distances);
 
+/* Queries of the last F32 neighbour search in this process whose candidate
+ * set could not be certified by the error bound and were recomputed in FP64. */
+int umapb_knn_last_fp64_recomputed(void);
+
 /*
  * neighbor_similarities (include/umappp/neighbor_similarities.hpp:53-207):
  * replaces the distances of each CSR row by membership weights in place.

@@ -11,17 +11,26 @@ import numpy as np
 import pytest
 
 import oracle
-from helpers import csr_tuple, mock_neighbors, neighbors_of, normal_data, two_populations
+from helpers import csr_tuple, mock_neighbors, neighbors_of, normal_data, rel_err, two_populations
 
 pytestmark = pytest.mark.gpu
 
 
-def _oracle_pipeline(nl: oracle.CSR, dtype, num_epochs, rate=5.0):
-    """Similarities (FP64, stored in dtype) -> union -> epochs, as the device computes them."""
-    w64, _, _ = oracle.neighbor_similarities(nl.astype(np.float64))
-    w = oracle.CSR(nl.ptr, nl.idx, w64.val.astype(dtype))
+def _oracle_pipeline(nl: oracle.CSR, dtype, num_epochs, rate=5.0, device_weights=None):
+    """Similarities (FP64, stored in dtype) -> union -> epochs, as the device computes them.
+    With device_weights, the oracle's union and schedule start from the device's weights."""
+    if device_weights is None:
+        w64, _, _ = oracle.neighbor_similarities(nl.astype(np.float64))
+        w = oracle.CSR(nl.ptr, nl.idx, w64.val.astype(dtype))
+    else:
+        w = oracle.CSR(nl.ptr, nl.idx, np.asarray(device_weights, dtype=dtype))
     g = oracle.combine_neighbor_sets(w, 1.0)
     return g, oracle.similarities_to_epochs(g, num_epochs, rate)
+
+
+def _device_weights(umap, nl):
+    _, _, w = umap.neighbor_similarities(csr_tuple(nl))
+    return w
 
 
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
@@ -32,13 +41,21 @@ def test_epoch_data_matches_oracle(umap, dtype):
     assert st.epoch() == 0 and st.num_epochs() == 500 and st.num_observations() == 500
     a, b = oracle.find_ab(1.0, 0.1)
     assert (st.a, st.b) == (a, b)
-    _, ref = _oracle_pipeline(nl, dtype, 500)
     ep = st.get_epoch_data()
+    # from the device's weights, the union and the schedule are bit-exact
+    _, ref = _oracle_pipeline(nl, dtype, 500, device_weights=_device_weights(umap, nl))
     assert np.array_equal(ep.cumulative_num_edges, ref.ptr)
     assert np.array_equal(ep.edge_targets, ref.targets)
     assert np.array_equal(ep.epochs_per_sample, ref.eps)
     assert np.array_equal(ep.epoch_of_next_sample, ref.enext)
     assert np.array_equal(ep.epoch_of_next_negative_sample, ref.enneg)
+    # against the host's weights: the device exp is correctly rounded, the host
+    # libm's exp is not always, so single weights may differ in the last bit
+    _, ref2 = _oracle_pipeline(nl, dtype, 500)
+    assert np.array_equal(ep.edge_targets, ref2.targets)
+    tol = 1e-12 if dtype == np.float64 else 1e-6
+    assert rel_err(ep.epochs_per_sample, ref2.eps) <= tol
+    assert np.mean(ep.epochs_per_sample == ref2.eps) > 0.95
 
 
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
@@ -55,16 +72,24 @@ def test_layout_quality_matches_reference(umap, dtype):
     st.run(Y)
     assert st.epoch() == 500
     assert np.all(np.isfinite(Y))
-    # reference serial run from the same layout
-    R = Y0.copy()
+    # reference serial runs from the same layout, over several optimize seeds:
+    # at 2000 points the reference's own seed-to-seed spread (about 0.007 in
+    # trustworthiness and 1% in cross-entropy) is as large as the bars, so the
+    # device is compared with the mean of the reference runs, with the bar
+    # widened to two standard deviations of that spread where it is larger
     a, b = oracle.find_ab(1.0, 0.1)
-    oracle.optimize_layout(2, R, ep, a, b, 1.0, 1.0, 1234567890, 500)
+    t_ref, ce_ref = [], []
+    for seed in range(4):
+        R = Y0.copy()
+        oracle.optimize_layout(2, R, ep.copy(), a, b, 1.0, 1.0, 1234567890 + seed, 500)
+        t_ref.append(oracle.trustworthiness(X, R, 15))
+        ce_ref.append(oracle.cross_entropy(g.astype(np.float64), R, a, b))
     t_dev = oracle.trustworthiness(X, Y, 15)
-    t_ref = oracle.trustworthiness(X, R, 15)
-    assert abs(t_dev - t_ref) <= 0.005, (t_dev, t_ref)
     ce_dev = oracle.cross_entropy(g.astype(np.float64), Y, a, b)
-    ce_ref = oracle.cross_entropy(g.astype(np.float64), R, a, b)
-    assert abs(ce_dev - ce_ref) <= 0.01 * abs(ce_ref), (ce_dev, ce_ref)
+    t_bar = max(0.005, 2 * float(np.std(t_ref)))
+    ce_bar = max(0.01, 2 * float(np.std(ce_ref) / np.mean(ce_ref)))
+    assert abs(t_dev - np.mean(t_ref)) <= t_bar, (t_dev, t_ref)
+    assert abs(ce_dev - np.mean(ce_ref)) <= ce_bar * np.mean(ce_ref), (ce_dev, ce_ref)
 
 
 def test_spectral_initialize_matches_reference(umap):
@@ -123,8 +148,8 @@ def test_partial_runs_follow_the_same_schedule(umap):
     assert st.epoch() == 500
     full = umap.initialize(csr_tuple(nl), 2, np.zeros((200, 2)))
     assert np.array_equal(full.schedule_counts(200, 500), st.schedule_counts(200, 500))
-    # the schedule state after 200 epochs is the reference's
-    _, ep = _oracle_pipeline(nl, np.float64, 500)
+    # the schedule state after 200 epochs is the reference's (from the same weights)
+    _, ep = _oracle_pipeline(nl, np.float64, 500, device_weights=_device_weights(umap, nl))
     R = Y0.copy()
     oracle.optimize_layout(2, R, ep, st.a, st.b, 1.0, 1.0, 1, 200)
     assert np.array_equal(mid.epoch_of_next_sample, ep.enext)

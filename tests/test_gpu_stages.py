@@ -261,9 +261,9 @@ def test_random_init_range(umap, dtype):
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
 def test_schedule_counts_exact(umap, dtype):
     nl = neighbors_of(two_populations(400, 5, seed=4), 15, dtype=dtype)
-    # the device computes the similarities in FP64 and stores them in the float type
-    w64, _, _ = oracle.neighbor_similarities(nl.astype(np.float64))
-    w = oracle.CSR(nl.ptr, nl.idx, w64.val.astype(dtype))
+    # the oracle's union and schedule from the device's own weights
+    _, _, wd = umap.neighbor_similarities(csr_tuple(nl))
+    w = oracle.CSR(nl.ptr, nl.idx, wd)
     g = oracle.combine_neighbor_sets(w, 1.0)
     Y = np.ascontiguousarray(oracle.random_init(400, 2, dtype=dtype))
     st = umap.initialize(csr_tuple(nl), 2, Y.copy(), umap.Options(initialize_method=umap.InitializeMethod.NONE,

@@ -38,6 +38,19 @@ void require_device() {
     int major = 0;
     UMAPB_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
     if (major != 10) fail(UMAPB_ERR_NO_DEVICE, "the current CUDA device is not sm_100 (B200/GB200)");
+    // Keep freed stream-ordered allocations in the device pool instead of
+    // unmapping them at every synchronisation: the schedule windows are tens of
+    // GB and are re-created on every run.
+    thread_local int pooled_device = -1;
+    if (pooled_device != dev) {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        cudaGetLastError();
+        pooled_device = dev;
+    }
 }
 
 }  // namespace
@@ -487,6 +500,8 @@ int umapb_knn(int dtype, size_t data_dim, int32_t num_obs, const void* data, int
         UMAPB_CUDA(cudaStreamSynchronize(c.stream));
     });
 }
+
+int umapb_knn_last_fp64_recomputed(void) { return last_knn_redo_count(); }
 
 int umapb_neighbor_similarities(int dtype, int32_t num_obs, const int64_t* row_ptr, void* distances,
                                 double local_connectivity, double bandwidth, double min_k_dist_scale, int use_newton,

@@ -17,15 +17,27 @@
 // so the sums round exactly as a sequential FP64 loop.
 #include <algorithm>
 #include <cfloat>
+#include <cstdlib>
 #include <vector>
 
 #include "stages.cuh"
 
 namespace umapb {
 
+int& last_knn_redo_count() {
+    static int count = 0;
+    return count;
+}
+
 namespace {
 
 constexpr int KNN_BLOCK = 128;  // queries per block
+
+// UMAPB_KNN_TENSOR_CORES=1 selects the tensor-core candidate search.
+bool use_tensor_cores() {
+    const char* v = std::getenv("UMAPB_KNN_TENSOR_CORES");
+    return v && v[0] == '1';
+}
 constexpr int PT = 32;          // points per tile
 constexpr int CH = 32;          // dimensions per chunk
 
@@ -132,7 +144,8 @@ __global__ void knn_rescore_kernel(const float* __restrict__ data, int32_t n, in
                                    const int32_t* __restrict__ cand_idx, const float* __restrict__ cand_d2,
                                    int32_t* __restrict__ out_idx, float* __restrict__ out_dist,
                                    double* __restrict__ out_dist64, int32_t* __restrict__ redo,
-                                   int32_t* __restrict__ redo_count) {
+                                   int32_t* __restrict__ redo_count, const float* __restrict__ norms,
+                                   const unsigned int* __restrict__ norm_max_bits, double tc_rel) {
     const int32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n) return;
     double d64[KCAP];
@@ -168,11 +181,20 @@ __global__ void knn_rescore_kernel(const float* __restrict__ data, int32_t n, in
     // carry relative error below (dim + 2) * 2^-24 (plus the rounding of the
     // inputs, which is exact here); if the k-th FP64 distance could exceed the
     // true distance of such a point, the query is recomputed in FP64.
+    // For tensor-core candidates (norms given) the FP32 values are
+    // |q|^2 + |r|^2 - 2 q.r with an absolute error below tc_rel * (|q|^2 + max |r|^2).
     const float last32 = cand_d2[static_cast<size_t>(q) * KCAP + KCAP - 1];
     const double rel = (dim + 2) * 1.2e-7 * 2.0;
     const double kth = d64[k - 1];
     const bool full_list = (n - 1) <= KCAP;   // every other point is a candidate
-    if (!full_list && !(static_cast<double>(last32) * (1.0 - rel) > kth * (1.0 + rel))) {
+    bool certain;
+    if (norms) {
+        const double bound = tc_rel * (static_cast<double>(norms[q]) + static_cast<double>(__uint_as_float(*norm_max_bits)));
+        certain = static_cast<double>(last32) - bound > kth * (1.0 + 1e-12) + 1e-300;
+    } else {
+        certain = static_cast<double>(last32) * (1.0 - rel) > kth * (1.0 + rel);
+    }
+    if (!full_list && !certain) {
         const int32_t slot = atomicAdd(redo_count, 1);
         redo[slot] = q;
     }
@@ -215,22 +237,55 @@ void run_f64(const T* data, int32_t n, int32_t dim, int32_t k, const int32_t* qu
     UMAPB_LAUNCH_CHECK();
 }
 
+__global__ void norm_max_kernel(int32_t n, const float* __restrict__ norms, unsigned int* __restrict__ out) {
+    unsigned int m = 0;
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        m = max(m, __float_as_uint(norms[i]));    // non-negative floats order like their bits
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+// Tolerance of the tensor-core squared distances, relative to |q|^2 + |r|^2:
+// 3xTF32 products (about 3 * 2^-22), FP32 accumulation over up to 64 terms and
+// the final FP32 additions stay below 2^-17.
+constexpr double TC_REL_BOUND = 1.0 / 131072.0;
+
 template <int KCAP>
 void run_f32(const float* data, int32_t n, int32_t dim, int32_t k, int32_t* out_idx, float* out_dist,
              double* out_dist64, cudaStream_t s) {
     DevArray<int32_t> ci(static_cast<size_t>(n) * KCAP, s);
     DevArray<float> cd(static_cast<size_t>(n) * KCAP, s);
-    knn_bruteforce_kernel<float, float, KCAP><<<(n + KNN_BLOCK - 1) / KNN_BLOCK, KNN_BLOCK, 0, s>>>(
-        data, n, dim, nullptr, n, ci.get(), cd.get());
-    UMAPB_LAUNCH_CHECK();
+    DevArray<float> norms;
+    DevArray<unsigned int> norm_max(1, s);
+    const bool tc = use_tensor_cores() && knn_tc_supported(dim, KCAP);
+    if (tc) {
+        const int32_t n_pad = ((n + 127) / 128) * 128;
+        norms.allocate(n_pad, s);
+        DevArray<int> err(1, s);
+        err.zero(s);
+        knn_tc_candidates(data, n, dim, KCAP, ci.get(), cd.get(), norms.get(), err.get(), s);
+        int h_err = 0;
+        UMAPB_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        UMAPB_CUDA(cudaStreamSynchronize(s));
+        if (h_err != DEV_OK) fail(UMAPB_ERR_DEVICE_TIMEOUT, "tensor-core kNN: a pipeline wait gave up");
+        norm_max.zero(s);
+        norm_max_kernel<<<grid_for(n, 256, 1024), 256, 0, s>>>(n, norms.get(), norm_max.get());
+        UMAPB_LAUNCH_CHECK();
+    } else {
+        knn_bruteforce_kernel<float, float, KCAP><<<(n + KNN_BLOCK - 1) / KNN_BLOCK, KNN_BLOCK, 0, s>>>(
+            data, n, dim, nullptr, n, ci.get(), cd.get());
+        UMAPB_LAUNCH_CHECK();
+    }
     DevArray<int32_t> redo(n, s), redo_count(1, s);
     redo_count.zero(s);
     knn_rescore_kernel<KCAP><<<(n + 127) / 128, 128, 0, s>>>(data, n, dim, k, ci.get(), cd.get(), out_idx, out_dist,
-                                                             out_dist64, redo.get(), redo_count.get());
+                                                             out_dist64, redo.get(), redo_count.get(),
+                                                             tc ? norms.get() : nullptr, norm_max.get(), TC_REL_BOUND);
     UMAPB_LAUNCH_CHECK();
     int32_t nredo = 0;
     UMAPB_CUDA(cudaMemcpyAsync(&nredo, redo_count.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     UMAPB_CUDA(cudaStreamSynchronize(s));
+    last_knn_redo_count() = nredo;
     if (nredo > 0) {
         // exact FP64 search for the uncertain queries (same output rows)
         if (k + 8 <= 32) {

@@ -1,0 +1,433 @@
+// Tensor-core candidate search for the exact kNN of float data (sm_100a).
+//
+// Squared distances are ||q||^2 + ||r||^2 - 2 q.r with the dot products from
+// 5th-generation tensor cores (tcgen05.mma, kind::tf32) in split precision:
+// every coordinate is split as a = hi + lo with hi = tf32(a) and
+// lo = tf32(a - hi), and q.r = hi.hi + hi.lo + lo.hi (the lo.lo term is below
+// 2^-22 relative), i.e. "3xTF32", accumulated in FP32 in tensor memory.
+//
+// One CTA owns 128 queries (the MMA's M) and streams all reference points in
+// tiles of 128 (N).  Warp roles:
+//   warp 0     TMA producer: the query tile (hi and lo, all K chunks) once,
+//              then reference tiles into a 2-stage shared-memory ring;
+//   warp 1     MMA issuer (one lane): 3 x 4 x Kc tcgen05.mma per tile into one
+//              of two TMEM accumulators (128 lanes x 128 FP32 columns each),
+//              tcgen05.commit to the ring's "empty" and the accumulator's
+//              "full" mbarriers; it also owns the TMEM allocation;
+//   warps 2-5  epilogue: tcgen05.ld of the accumulator rows (one query per
+//              thread), distance, and a sorted register list of the KCAP best
+//              (distance, index) candidates.
+// Operands are K-major with the 128-byte swizzle (TMA box 128 rows x 32 FP32,
+// UMMA shared-memory descriptors with SBO = 1024 B), no cluster multicast.
+// Every mbarrier wait is bounded: on expiry the kernel records an error,
+// raises a CTA-wide abort flag so the other roles stop waiting, frees TMEM and
+// returns.  The candidates are rescored in FP64 by knn.cu.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <mutex>
+
+#include "stages.cuh"
+
+namespace umapb {
+
+namespace {
+
+constexpr int TC_M = 128;         // queries per CTA
+constexpr int TC_N = 128;         // references per tile
+constexpr int TC_KCHUNK = 32;     // FP32 elements per 128-byte swizzle row
+constexpr int TC_STAGES = 2;
+constexpr int TC_THREADS = 192;   // 6 warps
+constexpr uint32_t TC_TMEM_COLS = 256;   // two 128-column accumulators
+constexpr long long WAIT_LIMIT = 1ll << 26;
+
+// ------------------------------------------------------------ PTX helpers --
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait; returns false (and raises the abort flag) on expiry or abort.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* err) {
+    for (long long i = 0; i < WAIT_LIMIT; ++i) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (*abort_flag) return false;
+        if (i > 64) __nanosleep(32);
+    }
+    *abort_flag = 1;
+    atomicExch(err, DEV_TIMEOUT);
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// K-major, 128-byte swizzled operand: rows of 128 B, 8-row atoms of 1024 B.
+__device__ __forceinline__ uint64_t smem_desc(const void* p) {
+    const uint64_t addr = smem_u32(p);
+    uint64_t d = 0;
+    d |= (addr >> 4) & 0x3FFFull;               // start address
+    d |= uint64_t(1) << 16;                     // leading byte offset (unused for swizzled K-major)
+    d |= uint64_t(1024 >> 4) << 32;             // stride byte offset: 8 rows x 128 B
+    d |= uint64_t(1) << 46;                     // descriptor version (sm_100)
+    d |= uint64_t(2) << 61;                     // layout: 128-byte swizzle
+    return d;
+}
+
+// Instruction descriptor: D = F32, A = B = TF32, both K-major, M = 128, N = TC_N.
+constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | (uint32_t(TC_N >> 3) << 17) | (uint32_t(TC_M >> 4) << 24);
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_load32(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+template <int KCAP>
+__device__ __forceinline__ void insert_sorted(float (&bd)[KCAP], int (&bi)[KCAP], float cd, int ci) {
+#pragma unroll
+    for (int i = KCAP - 1; i > 0; --i) {
+        if (cd < bd[i - 1]) {
+            bd[i] = bd[i - 1];
+            bi[i] = bi[i - 1];
+        } else if (cd < bd[i]) {
+            bd[i] = cd;
+            bi[i] = ci;
+        }
+    }
+    if (cd < bd[0]) {
+        bd[0] = cd;
+        bi[0] = ci;
+    }
+}
+
+// ------------------------------------------------------------ prep kernel --
+
+// hi = tf32(a), lo = tf32(a - hi) into [n_pad, k_pad] (zero padded); squared
+// norms in FP64 rounded to FP32, +inf for padding rows so they never qualify.
+__global__ void split_tf32_kernel(const float* __restrict__ data, int32_t n, int32_t dim, int32_t n_pad, int32_t k_pad,
+                                  float* __restrict__ hi, float* __restrict__ lo, float* __restrict__ norms) {
+    const int64_t total = static_cast<int64_t>(n_pad) * k_pad;
+    for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < total; t += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t i = t / k_pad;
+        const int d = static_cast<int>(t % k_pad);
+        const float a = (i < n && d < dim) ? data[i * dim + d] : 0.0f;
+        uint32_t h, l;
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(a));
+        const float r = a - __uint_as_float(h);
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(r));
+        hi[t] = __uint_as_float(h);
+        lo[t] = __uint_as_float(l);
+    }
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n_pad; i += int64_t(gridDim.x) * blockDim.x) {
+        if (i < n) {
+            double s = 0;
+            for (int d = 0; d < dim; ++d) {
+                const double v = data[i * dim + d];
+                s += v * v;
+            }
+            norms[i] = static_cast<float>(s);
+        } else {
+            norms[i] = CUDART_INF_F;
+        }
+    }
+}
+
+// ----------------------------------------------------------- main kernel --
+
+template <int KC, int KCAP>
+struct TcSmem {
+    // operand tiles first (1024-byte aligned): A hi/lo then the B ring
+    float a_hi[KC][TC_M * TC_KCHUNK];
+    float a_lo[KC][TC_M * TC_KCHUNK];
+    float b_hi[TC_STAGES][KC][TC_N * TC_KCHUNK];
+    float b_lo[TC_STAGES][KC][TC_N * TC_KCHUNK];
+    uint64_t full[TC_STAGES];
+    uint64_t empty[TC_STAGES];
+    uint64_t tmem_full[2];
+    uint64_t tmem_empty[2];
+    uint64_t a_full;
+    uint32_t tmem_base;
+    int abort_flag;
+};
+
+template <int KC, int KCAP>
+__global__ void __launch_bounds__(TC_THREADS, 1) knn_tc_kernel(const __grid_constant__ CUtensorMap map_hi,
+                                                               const __grid_constant__ CUtensorMap map_lo,
+                                                               const float* __restrict__ norms, int32_t n,
+                                                               int32_t n_tiles, int32_t* __restrict__ cand_idx,
+                                                               float* __restrict__ cand_d2, int* __restrict__ err) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // the dynamic window is only guaranteed 16-byte aligned: round up to 1024
+    TcSmem<KC, KCAP>& sm = *reinterpret_cast<TcSmem<KC, KCAP>*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int q_base = blockIdx.x * TC_M;
+    volatile int* abort_flag = &sm.abort_flag;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < TC_STAGES; ++s) {
+            mbar_init(&sm.full[s], 1);
+            mbar_init(&sm.empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&sm.tmem_full[b], 1);
+            mbar_init(&sm.tmem_empty[b], 128);
+        }
+        mbar_init(&sm.a_full, 1);
+        sm.abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        // TMEM: two 128-column FP32 accumulators
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sm.tmem_base)),
+                     "r"(TC_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = sm.tmem_base;
+
+    constexpr uint32_t A_BYTES = 2u * KC * TC_M * TC_KCHUNK * 4u;
+    constexpr uint32_t B_BYTES = 2u * KC * TC_N * TC_KCHUNK * 4u;
+    int issued = 0;   // producer: loads issued (for the drain at exit)
+
+    if (warp == 0) {
+        if (lane == 0) {
+            mbar_arrive_expect_tx(&sm.a_full, A_BYTES);
+            for (int c = 0; c < KC; ++c) {
+                tma_load_2d(sm.a_hi[c], &map_hi, &sm.a_full, c * TC_KCHUNK, q_base);
+                tma_load_2d(sm.a_lo[c], &map_lo, &sm.a_full, c * TC_KCHUNK, q_base);
+            }
+            for (int it = 0; it < n_tiles; ++it) {
+                const int s = it % TC_STAGES;
+                const uint32_t round = it / TC_STAGES;
+                if (!mbar_wait(&sm.empty[s], (round & 1) ^ 1, abort_flag, err)) break;
+                mbar_arrive_expect_tx(&sm.full[s], B_BYTES);
+                for (int c = 0; c < KC; ++c) {
+                    tma_load_2d(sm.b_hi[s][c], &map_hi, &sm.full[s], c * TC_KCHUNK, it * TC_N);
+                    tma_load_2d(sm.b_lo[s][c], &map_lo, &sm.full[s], c * TC_KCHUNK, it * TC_N);
+                }
+                ++issued;
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            if (mbar_wait(&sm.a_full, 0, abort_flag, err)) {
+                for (int it = 0; it < n_tiles; ++it) {
+                    const int s = it % TC_STAGES;
+                    const int buf = it & 1;
+                    if (!mbar_wait(&sm.full[s], (it / TC_STAGES) & 1, abort_flag, err)) break;
+                    if (!mbar_wait(&sm.tmem_empty[buf], ((it >> 1) & 1) ^ 1, abort_flag, err)) break;
+                    tc_fence_after();
+                    const uint32_t d = tmem_base + buf * TC_N;
+                    uint32_t acc = 0;
+#pragma unroll
+                    for (int c = 0; c < KC; ++c) {
+#pragma unroll
+                        for (int kk = 0; kk < TC_KCHUNK / 8; ++kk) {
+                            const int off = kk * 8;   // 8 TF32 = 32 bytes along K inside the swizzle row
+                            const uint64_t ah = smem_desc(sm.a_hi[c] + off), al = smem_desc(sm.a_lo[c] + off);
+                            const uint64_t bh = smem_desc(sm.b_hi[s][c] + off), bl = smem_desc(sm.b_lo[s][c] + off);
+                            mma_tf32(d, al, bh, acc);
+                            acc = 1;
+                            mma_tf32(d, ah, bl, 1);
+                            mma_tf32(d, ah, bh, 1);
+                        }
+                    }
+                    mma_commit(&sm.empty[s]);
+                    mma_commit(&sm.tmem_full[buf]);
+                }
+            }
+        }
+    } else {
+        // epilogue: thread <-> query row (TMEM lane) 32 * (warp % 4) + lane
+        const int quarter = warp & 3;
+        const int row = quarter * 32 + lane;
+        const int q = q_base + row;
+        const float qn = (q < n) ? norms[q] : 0.0f;
+        float bd[KCAP];
+        int bi[KCAP];
+#pragma unroll
+        for (int i = 0; i < KCAP; ++i) {
+            bd[i] = CUDART_INF_F;
+            bi[i] = -1;
+        }
+        for (int it = 0; it < n_tiles; ++it) {
+            const int buf = it & 1;
+            if (!mbar_wait(&sm.tmem_full[buf], (it >> 1) & 1, abort_flag, err)) break;
+            tc_fence_after();
+            const uint32_t taddr = tmem_base + (uint32_t(quarter * 32) << 16) + buf * TC_N;
+            const int col0 = it * TC_N;
+#pragma unroll 1
+            for (int ch = 0; ch < TC_N / 32; ++ch) {
+                uint32_t r[32];
+                tmem_load32(taddr + ch * 32, r);
+#pragma unroll
+                for (int i = 0; i < 32; ++i) {
+                    const int col = col0 + ch * 32 + i;
+                    const float d2 = fmaf(-2.0f, __uint_as_float(r[i]), qn + __ldg(norms + col));
+                    if (d2 < bd[KCAP - 1] && col != q) insert_sorted<KCAP>(bd, bi, d2, col);
+                }
+            }
+            tc_fence_before();
+            mbar_arrive(&sm.tmem_empty[buf]);
+        }
+        if (q < n) {
+#pragma unroll
+            for (int i = 0; i < KCAP; ++i) {
+                cand_idx[static_cast<size_t>(q) * KCAP + i] = bi[i];
+                cand_d2[static_cast<size_t>(q) * KCAP + i] = bd[i];
+            }
+        }
+    }
+
+    // drain: loads in flight must land before the CTA's shared memory goes away
+    if (warp == 0 && lane == 0 && *abort_flag) {
+        for (int it = (issued > TC_STAGES ? issued - TC_STAGES : 0); it < issued; ++it) {
+            const int s = it % TC_STAGES;
+            for (long long i = 0; i < WAIT_LIMIT && !mbar_try_wait(&sm.full[s], (it / TC_STAGES) & 1); ++i) __nanosleep(64);
+        }
+        for (long long i = 0; i < WAIT_LIMIT && !mbar_try_wait(&sm.a_full, 0); ++i) __nanosleep(64);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 1) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TC_TMEM_COLS));
+    }
+}
+
+// --------------------------------------------------------------- host side --
+
+PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess) {
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        }
+    });
+    require(fn != nullptr, "cuTensorMapEncodeTiled is unavailable", UMAPB_ERR_CUDA);
+    return fn;
+}
+
+// 2-D FP32 tensor [rows, k_pad] (k_pad contiguous), box 128 rows x 32 columns, 128-byte swizzle.
+CUtensorMap make_map(const float* base, int64_t rows, int k_pad) {
+    CUtensorMap m;
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(k_pad), static_cast<cuuint64_t>(rows)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(k_pad) * sizeof(float)};
+    const cuuint32_t box[2] = {TC_KCHUNK, 128};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = get_encode()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box,
+                                    estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    require(r == CUDA_SUCCESS, "cuTensorMapEncodeTiled failed", UMAPB_ERR_CUDA);
+    return m;
+}
+
+template <int KC, int KCAP>
+void launch_tc(const CUtensorMap& mh, const CUtensorMap& ml, const float* norms, int32_t n, int32_t n_pad,
+               int32_t* cand_idx, float* cand_d2, int* err, cudaStream_t s) {
+    const size_t smem = sizeof(TcSmem<KC, KCAP>) + 1024;
+    static bool configured = false;
+    if (!configured) {
+        UMAPB_CUDA(cudaFuncSetAttribute(knn_tc_kernel<KC, KCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(smem)));
+        configured = true;
+    }
+    const int n_tiles = n_pad / TC_N;
+    knn_tc_kernel<KC, KCAP><<<n_pad / TC_M, TC_THREADS, smem, s>>>(mh, ml, norms, n, n_tiles, cand_idx, cand_d2, err);
+    UMAPB_LAUNCH_CHECK();
+}
+
+}  // namespace
+
+bool knn_tc_supported(int32_t dim, int kcap) { return dim >= 1 && dim <= 2 * TC_KCHUNK && (kcap == 16 || kcap == 24 || kcap == 32); }
+
+// Candidate lists (KCAP per query, FP32 squared distances, ascending) from the
+// tensor-core search; also returns the largest reference norm for the
+// certainty bound of the FP64 rescoring.
+void knn_tc_candidates(const float* data, int32_t n, int32_t dim, int kcap, int32_t* cand_idx, float* cand_d2,
+                       float* norms_out, int* d_err, cudaStream_t s) {
+    require(knn_tc_supported(dim, kcap), "tensor-core kNN: unsupported dimension or candidate count");
+    const int kc = (dim + TC_KCHUNK - 1) / TC_KCHUNK;
+    const int k_pad = kc * TC_KCHUNK;
+    const int32_t n_pad = ((n + TC_M - 1) / TC_M) * TC_M;
+    DevArray<float> hi(static_cast<size_t>(n_pad) * k_pad, s), lo(static_cast<size_t>(n_pad) * k_pad, s);
+    split_tf32_kernel<<<grid_for(static_cast<size_t>(n_pad) * k_pad, 256), 256, 0, s>>>(data, n, dim, n_pad, k_pad,
+                                                                                        hi.get(), lo.get(), norms_out);
+    UMAPB_LAUNCH_CHECK();
+    const CUtensorMap mh = make_map(hi.get(), n_pad, k_pad);
+    const CUtensorMap ml = make_map(lo.get(), n_pad, k_pad);
+    if (kc == 1) {
+        if (kcap == 16) launch_tc<1, 16>(mh, ml, norms_out, n, n_pad, cand_idx, cand_d2, d_err, s);
+        else if (kcap == 24) launch_tc<1, 24>(mh, ml, norms_out, n, n_pad, cand_idx, cand_d2, d_err, s);
+        else launch_tc<1, 32>(mh, ml, norms_out, n, n_pad, cand_idx, cand_d2, d_err, s);
+    } else {
+        if (kcap == 16) launch_tc<2, 16>(mh, ml, norms_out, n, n_pad, cand_idx, cand_d2, d_err, s);
+        else if (kcap == 24) launch_tc<2, 24>(mh, ml, norms_out, n, n_pad, cand_idx, cand_d2, d_err, s);
+        else launch_tc<2, 32>(mh, ml, norms_out, n, n_pad, cand_idx, cand_d2, d_err, s);
+    }
+    // keep hi/lo alive until the kernel has run (stream-ordered free)
+}
+
+}  // namespace umapb

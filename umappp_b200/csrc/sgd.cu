@@ -246,83 +246,197 @@ __device__ __forceinline__ T floor_eps(T d2) {
     return (e < d2) ? d2 : e;
 }
 
-// Two-dimensional layouts: float2 coordinates, one vector atomic per update.
-__global__ void __launch_bounds__(256) sgd_epoch_2d_f32(const int64_t* __restrict__ starts, int w,
-                                                        const int2* __restrict__ ht, const uint16_t* __restrict__ nneg,
-                                                        float2* __restrict__ Y, SgdParams<float> p) {
-    const int64_t begin = starts[w], end = starts[w + 1];
-    for (int64_t e = begin + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < end; e += int64_t(gridDim.x) * blockDim.x) {
-        const int2 pr = ht[e];
-        const int nn = nneg[e];
-        const float2 y0 = __ldcg(&Y[pr.x]);
-        const float2 yt = __ldcg(&Y[pr.y]);
-        float hx = y0.x, hy = y0.y;
-        {
-            const float dx = hx - yt.x, dy = hy - yt.y;
-            const float d2 = floor_eps(dx * dx + dy * dy);
-            const float c = attract_coef(d2, p);
-            const float gx = p.alpha * clamp4(c * dx);
-            const float gy = p.alpha * clamp4(c * dy);
-            hx += gx;
-            hy += gy;
-            atomicAdd(&Y[pr.y], make_float2(-gx, -gy));
-        }
-        if (nn > 0) {
-            NegStream rng(static_cast<uint32_t>(pr.x), static_cast<uint32_t>(pr.y), p.epoch, p.k0, p.k1);
-            for (int q = 0; q < nn; ++q) {
-                const int32_t k = rng.bounded(static_cast<uint32_t>(p.n));
-                if (k == pr.x) continue;
-                const float2 yk = __ldcg(&Y[k]);
-                const float dx = hx - yk.x, dy = hy - yk.y;
-                const float d2 = floor_eps(dx * dx + dy * dy);
-                const float c = repulse_coef(d2, p);
-                hx += p.alpha * clamp4(c * dx);
-                hy += p.alpha * clamp4(c * dy);
-            }
-        }
-        atomicAdd(&Y[pr.x], make_float2(hx - y0.x, hy - y0.y));
+// Segments: the firing events of one head in one epoch are contiguous in the
+// event list (it follows the edges' CSR order).  A segment is a run of at most
+// SEG_MAX events of one head: runs are also cut at every SEG_MAX-aligned
+// position of the epoch, which bounds the longest sequential chain (hub heads
+// have hundreds of edges) at the cost of a few extra segments.  Segments
+// partition the window's events in order: seg_pos[s] is the first event of
+// segment s, seg_pos[S] = the event total, and the segments of epoch w are
+// [seg_first[w], seg_first[w + 1]).  Built without atomics by a count / scan /
+// write over fixed event ranges, so the list is deterministic.
+constexpr int SEG_MAX = 8;
+constexpr int SEG_BLOCK = 256;
+constexpr int SEG_ITEMS = 8;    // events per thread in the segment passes
+
+__device__ __forceinline__ bool seg_start(int64_t e, const int2* __restrict__ ht, const int64_t* __restrict__ starts,
+                                          int W) {
+    int lo = 0, hi = W - 1;   // epoch of e: the last w with starts[w] <= e
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (starts[mid] <= e) lo = mid; else hi = mid - 1;
+    }
+    const int64_t s0 = starts[lo];
+    return e == s0 || ((e - s0) % SEG_MAX) == 0 || ht[e - 1].x != ht[e].x;
+}
+
+__global__ void __launch_bounds__(SEG_BLOCK) seg_count_kernel(int64_t total, const int2* __restrict__ ht,
+                                                              const int64_t* __restrict__ starts, int W,
+                                                              int64_t* __restrict__ block_counts) {
+    const int64_t base = static_cast<int64_t>(blockIdx.x) * SEG_BLOCK * SEG_ITEMS;
+    int c = 0;
+    for (int i = 0; i < SEG_ITEMS; ++i) {
+        const int64_t e = base + static_cast<int64_t>(i) * SEG_BLOCK + threadIdx.x;
+        if (e < total && seg_start(e, ht, starts, W)) ++c;
+    }
+    typedef cub::BlockReduce<int, SEG_BLOCK> Reduce;
+    __shared__ typename Reduce::TempStorage tmp;
+    const int sum = Reduce(tmp).Sum(c);
+    if (threadIdx.x == 0) block_counts[blockIdx.x] = sum;
+}
+
+// Writes segment starts in event order: block b covers events
+// [b * SEG_BLOCK * SEG_ITEMS, ...), item-major so each pass is coalesced.
+__global__ void __launch_bounds__(SEG_BLOCK) seg_write_kernel(int64_t total, const int2* __restrict__ ht,
+                                                              const int64_t* __restrict__ starts, int W,
+                                                              const int64_t* __restrict__ block_offsets,
+                                                              int64_t* __restrict__ seg_pos) {
+    typedef cub::BlockScan<int, SEG_BLOCK> Scan;
+    __shared__ typename Scan::TempStorage tmp;
+    const int64_t base = static_cast<int64_t>(blockIdx.x) * SEG_BLOCK * SEG_ITEMS;
+    int64_t out = block_offsets[blockIdx.x];
+    for (int i = 0; i < SEG_ITEMS; ++i) {
+        const int64_t e = base + static_cast<int64_t>(i) * SEG_BLOCK + threadIdx.x;
+        const int f = (e < total && seg_start(e, ht, starts, W)) ? 1 : 0;
+        int prefix, sum;
+        Scan(tmp).ExclusiveSum(f, prefix, sum);
+        if (f) seg_pos[out + prefix] = e;
+        out += sum;
+        __syncthreads();
     }
 }
 
-// Any dimension (up to MAX_GENERIC_DIM) and either precision.
-template <typename T>
-__global__ void __launch_bounds__(128) sgd_epoch_generic(const int64_t* __restrict__ starts, int w,
-                                                         const int2* __restrict__ ht, const uint16_t* __restrict__ nneg,
-                                                         T* __restrict__ Y, int dim, SgdParams<T> p) {
-    const int64_t begin = starts[w], end = starts[w + 1];
-    T head[MAX_GENERIC_DIM], orig[MAX_GENERIC_DIM];
-    for (int64_t e = begin + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; e < end; e += int64_t(gridDim.x) * blockDim.x) {
-        const int2 pr = ht[e];
-        const int nn = nneg[e];
-        T* yh = Y + static_cast<size_t>(pr.x) * dim;
-        T* yt = Y + static_cast<size_t>(pr.y) * dim;
-        T d2 = 0;
-        for (int d = 0; d < dim; ++d) {
-            head[d] = orig[d] = __ldcg(yh + d);
-            const T diff = head[d] - __ldcg(yt + d);
-            d2 += diff * diff;
+// seg_first[w] = index of the first segment of epoch w (lower bound of starts[w] in seg_pos).
+__global__ void seg_first_kernel(const int64_t* __restrict__ seg_pos, int64_t nseg, const int64_t* __restrict__ starts,
+                                 int W, int64_t* __restrict__ seg_first) {
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w <= W; w += gridDim.x * blockDim.x) {
+        const int64_t key = starts[w];
+        int64_t lo = 0, hi = nseg;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (seg_pos[mid] < key) lo = mid + 1; else hi = mid;
         }
-        {
-            const T c = attract_coef(floor_eps(d2), p);
-            for (int d = 0; d < dim; ++d) {
-                const T g = p.alpha * clamp4(c * (head[d] - __ldcg(yt + d)));
-                head[d] += g;
-                atomicAdd(yt + d, -g);
+        seg_first[w] = lo;
+    }
+}
+
+// Negative samples are gathered NEG_BATCH at a time: their indices do not
+// depend on the layout, so all loads of a batch (and the tail's) are in flight
+// together, and the head then takes the updates in sequence.
+constexpr int NEG_BATCH = 12;
+
+// One thread per segment: the head's firing edges are processed in CSR order
+// with the head kept in registers, each edge's attractive step (head and tail)
+// followed by its negative samples -- the per-row sequence of
+// optimize_layout.hpp:136-180.  The tail moves by a vector atomic; the head's
+// total displacement is added once at the end.
+__global__ void __launch_bounds__(256) sgd_epoch_2d_f32(const int64_t* __restrict__ seg_first, int w,
+                                                        const int64_t* __restrict__ seg_pos,
+                                                        const int2* __restrict__ ht, const uint16_t* __restrict__ nneg,
+                                                        float2* __restrict__ Y, SgdParams<float> p) {
+    const int64_t s0 = seg_first[w], s1 = seg_first[w + 1];
+    for (int64_t s = s0 + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; s < s1; s += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t e0 = seg_pos[s], e1 = seg_pos[s + 1];
+        const int32_t h = ht[e0].x;
+        const float2 y0 = __ldcg(&Y[h]);
+        float hx = y0.x, hy = y0.y;
+        for (int64_t e = e0; e < e1; ++e) {
+            const int2 pr = ht[e];
+            int nn = nneg[e];
+            const float2 yt = __ldcg(&Y[pr.y]);
+            NegStream rng(static_cast<uint32_t>(h), static_cast<uint32_t>(pr.y), p.epoch, p.k0, p.k1);
+            int32_t ks[NEG_BATCH];
+            float2 yk[NEG_BATCH];
+            const int m0 = nn < NEG_BATCH ? nn : NEG_BATCH;
+#pragma unroll
+            for (int i = 0; i < NEG_BATCH; ++i) {
+                if (i < m0) {
+                    ks[i] = rng.bounded(static_cast<uint32_t>(p.n));
+                    yk[i] = __ldcg(&Y[ks[i]]);
+                }
+            }
+            {
+                const float dx = hx - yt.x, dy = hy - yt.y;
+                const float d2 = floor_eps(dx * dx + dy * dy);
+                const float cf = attract_coef(d2, p);
+                const float gx = p.alpha * clamp4(cf * dx);
+                const float gy = p.alpha * clamp4(cf * dy);
+                hx += gx;
+                hy += gy;
+                atomicAdd(&Y[pr.y], make_float2(-gx, -gy));
+            }
+            int m = m0;
+            while (true) {
+#pragma unroll
+                for (int i = 0; i < NEG_BATCH; ++i) {
+                    if (i < m && ks[i] != h) {
+                        const float dx = hx - yk[i].x, dy = hy - yk[i].y;
+                        const float d2 = floor_eps(dx * dx + dy * dy);
+                        const float cf = repulse_coef(d2, p);
+                        hx += p.alpha * clamp4(cf * dx);
+                        hy += p.alpha * clamp4(cf * dy);
+                    }
+                }
+                nn -= m;
+                if (nn <= 0) break;
+                m = nn < NEG_BATCH ? nn : NEG_BATCH;
+#pragma unroll
+                for (int i = 0; i < NEG_BATCH; ++i) {
+                    if (i < m) {
+                        ks[i] = rng.bounded(static_cast<uint32_t>(p.n));
+                        yk[i] = __ldcg(&Y[ks[i]]);
+                    }
+                }
             }
         }
-        if (nn > 0) {
-            NegStream rng(static_cast<uint32_t>(pr.x), static_cast<uint32_t>(pr.y), p.epoch, p.k0, p.k1);
-            for (int q = 0; q < nn; ++q) {
-                const int32_t k = rng.bounded(static_cast<uint32_t>(p.n));
-                if (k == pr.x) continue;
-                const T* yk = Y + static_cast<size_t>(k) * dim;
-                T dd2 = 0;
+        atomicAdd(&Y[h], make_float2(hx - y0.x, hy - y0.y));
+    }
+}
+
+// Any dimension (up to MAX_GENERIC_DIM) and either precision; same per-segment order.
+template <typename T>
+__global__ void __launch_bounds__(128) sgd_epoch_generic(const int64_t* __restrict__ seg_first, int w,
+                                                         const int64_t* __restrict__ seg_pos,
+                                                         const int2* __restrict__ ht, const uint16_t* __restrict__ nneg,
+                                                         T* __restrict__ Y, int dim, SgdParams<T> p) {
+    const int64_t s0 = seg_first[w], s1 = seg_first[w + 1];
+    T head[MAX_GENERIC_DIM], orig[MAX_GENERIC_DIM];
+    for (int64_t s = s0 + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; s < s1; s += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t e0 = seg_pos[s], e1 = seg_pos[s + 1];
+        const int32_t h = ht[e0].x;
+        T* yh = Y + static_cast<size_t>(h) * dim;
+        for (int d = 0; d < dim; ++d) head[d] = orig[d] = __ldcg(yh + d);
+        for (int64_t e = e0; e < e1; ++e) {
+            const int2 pr = ht[e];
+            const int nn = nneg[e];
+            T* yt = Y + static_cast<size_t>(pr.y) * dim;
+            T d2 = 0;
+            for (int d = 0; d < dim; ++d) {
+                const T diff = head[d] - __ldcg(yt + d);
+                d2 += diff * diff;
+            }
+            {
+                const T c = attract_coef(floor_eps(d2), p);
                 for (int d = 0; d < dim; ++d) {
-                    const T diff = head[d] - __ldcg(yk + d);
-                    dd2 += diff * diff;
+                    const T g = p.alpha * clamp4(c * (head[d] - __ldcg(yt + d)));
+                    head[d] += g;
+                    atomicAdd(yt + d, -g);
                 }
-                const T c = repulse_coef(floor_eps(dd2), p);
-                for (int d = 0; d < dim; ++d) head[d] += p.alpha * clamp4(c * (head[d] - __ldcg(yk + d)));
+            }
+            if (nn > 0) {
+                NegStream rng(static_cast<uint32_t>(h), static_cast<uint32_t>(pr.y), p.epoch, p.k0, p.k1);
+                for (int q = 0; q < nn; ++q) {
+                    const int32_t k = rng.bounded(static_cast<uint32_t>(p.n));
+                    if (k == h) continue;
+                    const T* yk = Y + static_cast<size_t>(k) * dim;
+                    T dd2 = 0;
+                    for (int d = 0; d < dim; ++d) {
+                        const T diff = head[d] - __ldcg(yk + d);
+                        dd2 += diff * diff;
+                    }
+                    const T c = repulse_coef(floor_eps(dd2), p);
+                    for (int d = 0; d < dim; ++d) head[d] += p.alpha * clamp4(c * (head[d] - __ldcg(yk + d)));
+                }
             }
         }
         for (int d = 0; d < dim; ++d) atomicAdd(yh + d, head[d] - orig[d]);
@@ -429,13 +543,15 @@ void SgdEngine<T>::build_window(int first, int last_wanted, cudaStream_t s) {
         UMAPB_CUDA(cudaMemGetInfo(&free_b, &total_b));
         budget = free_b / 3;
     }
-    const size_t per_event = sizeof(int2) + sizeof(uint16_t);
+    // event record + (at most) one segment start per event
+    const size_t per_event = sizeof(int2) + sizeof(uint16_t) + sizeof(int64_t);
     int Wk = W;
     while (Wk > 1 && static_cast<size_t>(h[Wk]) * per_event > budget) --Wk;
     const int64_t events = h[Wk];
 
     ht_.release();
     nneg_.release();
+    seg_pos_.release();
     ht_.allocate(events, s);
     nneg_.allocate(events, s);
     DevArray<int> status(1, s);
@@ -448,6 +564,40 @@ void SgdEngine<T>::build_window(int first, int last_wanted, cudaStream_t s) {
     }
     epoch_offsets_.allocate(Wk + 1, s);
     UMAPB_CUDA(cudaMemcpyAsync(epoch_offsets_.get(), h.data(), (Wk + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+
+    // head segments of every epoch in the window (count, scan, write, per-epoch first segment)
+    const int64_t seg_blocks = std::max<int64_t>((events + SEG_BLOCK * SEG_ITEMS - 1) / (SEG_BLOCK * SEG_ITEMS), 1);
+    DevArray<int64_t> bcount(seg_blocks + 1, s), boff(seg_blocks + 1, s);
+    bcount.zero(s);
+    if (events > 0) {
+        seg_count_kernel<<<static_cast<unsigned>(seg_blocks), SEG_BLOCK, 0, s>>>(events, ht_.get(), epoch_offsets_.get(),
+                                                                               Wk, bcount.get());
+        UMAPB_LAUNCH_CHECK();
+    }
+    {
+        size_t tb = 0;
+        UMAPB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, bcount.get(), boff.get(), seg_blocks + 1, s));
+        DevArray<unsigned char> temp(tb, s);
+        UMAPB_CUDA(cub::DeviceScan::ExclusiveSum(temp.get(), tb, bcount.get(), boff.get(), seg_blocks + 1, s));
+    }
+    int64_t nseg = 0;
+    UMAPB_CUDA(cudaMemcpyAsync(&nseg, boff.get() + seg_blocks, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+    seg_pos_.allocate(nseg + 1, s);
+    UMAPB_CUDA(cudaMemcpyAsync(seg_pos_.get() + nseg, &events, sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    if (events > 0) {
+        seg_write_kernel<<<static_cast<unsigned>(seg_blocks), SEG_BLOCK, 0, s>>>(events, ht_.get(), epoch_offsets_.get(),
+                                                                               Wk, boff.get(), seg_pos_.get());
+        UMAPB_LAUNCH_CHECK();
+    }
+    seg_first_.allocate(Wk + 1, s);
+    seg_first_kernel<<<grid_for(Wk + 1, 128), 128, 0, s>>>(seg_pos_.get(), nseg, epoch_offsets_.get(), Wk,
+                                                            seg_first_.get());
+    UMAPB_LAUNCH_CHECK();
+    host_seg_first_.resize(Wk + 1);
+    UMAPB_CUDA(cudaMemcpyAsync(host_seg_first_.data(), seg_first_.get(), (Wk + 1) * sizeof(int64_t),
+                               cudaMemcpyDeviceToHost, s));
+
     host_epoch_offsets_.assign(h.begin(), h.begin() + Wk + 1);
     int st = 0;
     UMAPB_CUDA(cudaMemcpyAsync(&st, status.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -500,20 +650,21 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
             p.alpha = static_cast<T>(static_cast<double>(lr) * (1.0 - static_cast<double>(epoch_t / static_cast<T>(total))));
             p.epoch = static_cast<uint32_t>(e);
             const int w = e - window_begin_;
-            const int64_t nev = host_epoch_offsets_[w + 1] - host_epoch_offsets_[w];
-            if (nev == 0) continue;
+            const int64_t nsegs = host_seg_first_[w + 1] - host_seg_first_[w];
+            if (nsegs == 0) continue;
             bool done = false;
             if constexpr (std::is_same<T, float>::value) {
                 if (num_dim == 2) {
-                    const unsigned g = grid_for(nev, 256, blocks_2d);
-                    sgd_epoch_2d_f32<<<g, 256, 0, s>>>(epoch_offsets_.get(), w, ht_.get(), nneg_.get(),
+                    const unsigned g = grid_for(nsegs, 256, blocks_2d);
+                    sgd_epoch_2d_f32<<<g, 256, 0, s>>>(seg_first_.get(), w, seg_pos_.get(), ht_.get(), nneg_.get(),
                                                        reinterpret_cast<float2*>(Y), p);
                     done = true;
                 }
             }
             if (!done) {
-                const unsigned g = grid_for(nev, 128, blocks_gen);
-                sgd_epoch_generic<T><<<g, 128, 0, s>>>(epoch_offsets_.get(), w, ht_.get(), nneg_.get(), Y, num_dim, p);
+                const unsigned g = grid_for(nsegs, 128, blocks_gen);
+                sgd_epoch_generic<T><<<g, 128, 0, s>>>(seg_first_.get(), w, seg_pos_.get(), ht_.get(), nneg_.get(), Y,
+                                                       num_dim, p);
             }
             UMAPB_LAUNCH_CHECK();
         }

@@ -5,19 +5,30 @@
 // same tolerance and 64-iteration cap), so that sigma and the weights agree
 // with an FP64 evaluation of the reference to rounding.  Compiled with
 // -fmad=false so no multiply-add is contracted, as in the reference's
-// -ffp-contract=off build.
+// -ffp-contract=off build.  exp is the correctly rounded exp_cr (exp_cr.cuh),
+// and log2(k + 1) comes from the host's libm, so the values track a host
+// evaluation to the last bit except where the host's exp itself misrounds.
 #include <cfloat>
 #include <cmath>
 
+#include "exp_cr.cuh"
 #include "stages.cuh"
 
 namespace umapb {
+
+constexpr int LOG2_TABLE = 256;
+
+struct Log2Table {
+    double v[LOG2_TABLE];   // v[m] = log2(m + 1)
+};
 
 template <typename T>
 __global__ void __launch_bounds__(128) similarities_kernel(int32_t n, const int64_t* __restrict__ ptr, T* __restrict__ val,
                                                            int raw_connect_index, double interpolation,
                                                            double bandwidth, double min_k_dist_scale, int use_newton,
-                                                           double* __restrict__ rho_out, double* __restrict__ sigma_out) {
+                                                           double* __restrict__ rho_out, double* __restrict__ sigma_out,
+                                                           const Log2Table log2_tab) {
+    const double* log2_table = log2_tab.v;
     const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int64_t start = ptr[i];
@@ -59,7 +70,8 @@ __global__ void __launch_bounds__(128) similarities_kernel(int32_t n, const int6
                 double lo = 0;
                 const double max_val = DBL_MAX;
                 double hi = max_val;
-                const double target = log2(static_cast<double>(nnb + 1)) * bandwidth;   // :127
+                // :127, log2(k + 1) from the host's libm for row lengths up to the table size
+                const double target = (nnb < LOG2_TABLE ? log2_table[nnb] : log2(static_cast<double>(nnb + 1))) * bandwidth;
 
                 for (int iter = 0; iter < 64; ++iter) {               // :129-184
                     double observed = num_le_rho;
@@ -70,7 +82,7 @@ __global__ void __launch_bounds__(128) similarities_kernel(int32_t n, const int6
                         const double cur = static_cast<double>(d[k]);
                         if (cur > rho) {
                             const double dd = cur - rho;
-                            const double current = exp(-dd * invsigma);
+                            const double current = exp_cr(-dd * invsigma);
                             observed += current;
                             deriv += dd * current * invsigma2;
                         }
@@ -111,7 +123,7 @@ __global__ void __launch_bounds__(128) similarities_kernel(int32_t n, const int6
                 const double invsigma = 1.0 / sigma;                  // :194-202
                 for (int k = 0; k < nnb; ++k) {
                     const double cur = static_cast<double>(d[k]);
-                    d[k] = (cur > rho) ? static_cast<T>(exp(-(cur - rho) * invsigma)) : T(1);
+                    d[k] = (cur > rho) ? static_cast<T>(exp_cr(-(cur - rho) * invsigma)) : T(1);
                 }
             }
         }
@@ -129,10 +141,12 @@ void neighbor_similarities(int32_t n, const int64_t* ptr, T* val, double local_c
             "local_connectivity must be a finite non-negative value", UMAPB_ERR_OVERFLOW);
     const int raw = static_cast<int>(std::trunc(local_connectivity));       // :56
     const double interpolation = local_connectivity - raw;                  // :57
+    Log2Table tab;
+    for (int m = 0; m < LOG2_TABLE; ++m) tab.v[m] = std::log2(static_cast<double>(m + 1));
     const unsigned block = 128;
     similarities_kernel<T><<<(n + block - 1) / block, block, 0, s>>>(n, ptr, val, raw, interpolation, bandwidth,
                                                                       min_k_dist_scale, use_newton ? 1 : 0, rho_out,
-                                                                      sigma_out);
+                                                                      sigma_out, tab);
     UMAPB_LAUNCH_CHECK();
 }
 

@@ -43,6 +43,14 @@ template <typename T>
 void knn_exact(const T* data, int32_t n, int32_t dim, int32_t k, int32_t* out_idx, T* out_dist, cudaStream_t s,
                double* out_dist_f64 = nullptr);
 
+// Tensor-core candidate search (knn_tc.cu): KCAP candidates per query with
+// FP32 squared distances; norms_out receives |x|^2 (n rounded up to 128 entries).
+bool knn_tc_supported(int32_t dim, int kcap);
+void knn_tc_candidates(const float* data, int32_t n, int32_t dim, int kcap, int32_t* cand_idx, float* cand_d2,
+                       float* norms_out, int* d_err, cudaStream_t s);
+// Number of queries the last float kNN recomputed in FP64 (certainty check).
+int& last_knn_redo_count();
+
 // ---- similarities (similarities.cu) -----------------------------------------
 template <typename T>
 void neighbor_similarities(int32_t n, const int64_t* ptr, T* val, double local_connectivity, double bandwidth,
@@ -103,6 +111,9 @@ private:
     int window_begin_ = 0, window_end_ = 0;
     DevArray<int2> ht_;
     DevArray<uint16_t> nneg_;
+    DevArray<int64_t> seg_pos_;         // first event of every head segment, plus the event total (see sgd.cu)
+    DevArray<int64_t> seg_first_;       // per epoch: index of its first segment (window_end_ - window_begin_ + 1)
+    std::vector<int64_t> host_seg_first_;
     DevArray<int64_t> epoch_offsets_;   // window_end_ - window_begin_ + 1 entries
     std::vector<int64_t> host_epoch_offsets_;
 };
