@@ -33,10 +33,11 @@ namespace {
 
 constexpr int KNN_BLOCK = 128;  // queries per block
 
-// UMAPB_KNN_TENSOR_CORES=1 selects the tensor-core candidate search.
+// The tensor-core candidate search is the default; UMAPB_KNN_TENSOR_CORES=0
+// selects the CUDA-core search instead (used by the precision comparison).
 bool use_tensor_cores() {
     const char* v = std::getenv("UMAPB_KNN_TENSOR_CORES");
-    return v && v[0] == '1';
+    return !(v && v[0] == '0');
 }
 constexpr int PT = 32;          // points per tile
 constexpr int CH = 32;          // dimensions per chunk

@@ -157,39 +157,64 @@ __device__ __forceinline__ void insert_sorted(float (&bd)[KCAP], int (&bi)[KCAP]
 
 // ------------------------------------------------------------ prep kernel --
 
-// hi = tf32(a), lo = tf32(a - hi) into [n_pad, k_pad] (zero padded); squared
-// norms in FP64 rounded to FP32, +inf for padding rows so they never qualify.
-__global__ void split_tf32_kernel(const float* __restrict__ data, int32_t n, int32_t dim, int32_t n_pad, int32_t k_pad,
-                                  float* __restrict__ hi, float* __restrict__ lo, float* __restrict__ norms) {
-    const int64_t total = static_cast<int64_t>(n_pad) * k_pad;
-    for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < total; t += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t i = t / k_pad;
-        const int d = static_cast<int>(t % k_pad);
-        const float a = (i < n && d < dim) ? data[i * dim + d] : 0.0f;
-        uint32_t h, l;
-        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(a));
-        const float r = a - __uint_as_float(h);
-        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(r));
-        hi[t] = __uint_as_float(h);
-        lo[t] = __uint_as_float(l);
-    }
+// Operands of the distance GEMM, [n_pad, k_pad] each (zero padded), as TF32
+// pairs hi = tf32(v), lo = tf32(v - hi):
+//   queries    A = [x, 1]              (column dim holds 1)
+//   references B = [x, -|x|^2 / 2]     (column dim holds minus half the norm)
+// so that the accumulator is q.r - |r|^2 / 2 and d2 = |q|^2 - 2 acc, with no
+// norm look-up in the epilogue.  Padding references carry -1e30 in the norm
+// column, so their distance is huge and never qualifies.  norms[i] = |x_i|^2
+// (FP64, rounded to FP32; +inf for padding rows).
+__device__ __forceinline__ void split_tf32(float a, float& hi, float& lo) {
+    uint32_t h, l;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(a));
+    const float r = a - __uint_as_float(h);
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(r));
+    hi = __uint_as_float(h);
+    lo = __uint_as_float(l);
+}
+
+__global__ void prepare_operands_kernel(const float* __restrict__ data, int32_t n, int32_t dim, int32_t n_pad,
+                                        int32_t k_pad, float* __restrict__ a_hi, float* __restrict__ a_lo,
+                                        float* __restrict__ b_hi, float* __restrict__ b_lo,
+                                        float* __restrict__ norms) {
     for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n_pad; i += int64_t(gridDim.x) * blockDim.x) {
+        double s = 0;
         if (i < n) {
-            double s = 0;
             for (int d = 0; d < dim; ++d) {
                 const double v = data[i * dim + d];
                 s += v * v;
             }
-            norms[i] = static_cast<float>(s);
-        } else {
-            norms[i] = CUDART_INF_F;
+        }
+        norms[i] = (i < n) ? static_cast<float>(s) : CUDART_INF_F;
+        const int64_t row = i * k_pad;
+        for (int d = 0; d < k_pad; ++d) {
+            float v = 0.0f;
+            if (i < n && d < dim) v = data[i * dim + d];
+            float h, l;
+            split_tf32(v, h, l);
+            a_hi[row + d] = h;
+            a_lo[row + d] = l;
+            if (d == dim) {
+                // the norm column: 1 for queries, -|r|^2 / 2 for references
+                a_hi[row + d] = (i < n) ? 1.0f : 0.0f;
+                a_lo[row + d] = 0.0f;
+                if (i < n) {
+                    split_tf32(static_cast<float>(-0.5 * s), h, l);
+                } else {
+                    h = -1e30f;
+                    l = 0.0f;
+                }
+            }
+            b_hi[row + d] = h;
+            b_lo[row + d] = l;
         }
     }
 }
 
 // ----------------------------------------------------------- main kernel --
 
-template <int KC, int KCAP>
+template <int KC>
 struct TcSmem {
     // operand tiles first (1024-byte aligned): A hi/lo then the B ring
     float a_hi[KC][TC_M * TC_KCHUNK];
@@ -205,16 +230,32 @@ struct TcSmem {
     int abort_flag;
 };
 
+// Register-array element by a run-time index via a 5-level select tree
+// (keeps the array in registers; dynamic indexing would spill it).
+__device__ __forceinline__ float select32(const float (&v)[32], int i) {
+    float t16[16], t8[8], t4[4], t2[2];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) t16[j] = (i & 16) ? v[j + 16] : v[j];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) t8[j] = (i & 8) ? t16[j + 8] : t16[j];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) t4[j] = (i & 4) ? t8[j + 4] : t8[j];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) t2[j] = (i & 2) ? t4[j + 2] : t4[j];
+    return (i & 1) ? t2[1] : t2[0];
+}
+
 template <int KC, int KCAP>
-__global__ void __launch_bounds__(TC_THREADS, 1) knn_tc_kernel(const __grid_constant__ CUtensorMap map_hi,
-                                                               const __grid_constant__ CUtensorMap map_lo,
+__global__ void __launch_bounds__(TC_THREADS, 1) knn_tc_kernel(const __grid_constant__ CUtensorMap map_ahi,
+                                                               const __grid_constant__ CUtensorMap map_alo,
+                                                               const __grid_constant__ CUtensorMap map_bhi,
+                                                               const __grid_constant__ CUtensorMap map_blo,
                                                                const float* __restrict__ norms, int32_t n,
                                                                int32_t n_tiles, int32_t* __restrict__ cand_idx,
                                                                float* __restrict__ cand_d2, int* __restrict__ err) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // the dynamic window is only guaranteed 16-byte aligned: round up to 1024
-    TcSmem<KC, KCAP>& sm = *reinterpret_cast<TcSmem<KC, KCAP>*>(
-        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    TcSmem<KC>& sm = *reinterpret_cast<TcSmem<KC>*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int q_base = blockIdx.x * TC_M;
     volatile int* abort_flag = &sm.abort_flag;
@@ -251,8 +292,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_tc_kernel(const __grid_cons
         if (lane == 0) {
             mbar_arrive_expect_tx(&sm.a_full, A_BYTES);
             for (int c = 0; c < KC; ++c) {
-                tma_load_2d(sm.a_hi[c], &map_hi, &sm.a_full, c * TC_KCHUNK, q_base);
-                tma_load_2d(sm.a_lo[c], &map_lo, &sm.a_full, c * TC_KCHUNK, q_base);
+                tma_load_2d(sm.a_hi[c], &map_ahi, &sm.a_full, c * TC_KCHUNK, q_base);
+                tma_load_2d(sm.a_lo[c], &map_alo, &sm.a_full, c * TC_KCHUNK, q_base);
             }
             for (int it = 0; it < n_tiles; ++it) {
                 const int s = it % TC_STAGES;
@@ -260,8 +301,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_tc_kernel(const __grid_cons
                 if (!mbar_wait(&sm.empty[s], (round & 1) ^ 1, abort_flag, err)) break;
                 mbar_arrive_expect_tx(&sm.full[s], B_BYTES);
                 for (int c = 0; c < KC; ++c) {
-                    tma_load_2d(sm.b_hi[s][c], &map_hi, &sm.full[s], c * TC_KCHUNK, it * TC_N);
-                    tma_load_2d(sm.b_lo[s][c], &map_lo, &sm.full[s], c * TC_KCHUNK, it * TC_N);
+                    tma_load_2d(sm.b_hi[s][c], &map_bhi, &sm.full[s], c * TC_KCHUNK, it * TC_N);
+                    tma_load_2d(sm.b_lo[s][c], &map_blo, &sm.full[s], c * TC_KCHUNK, it * TC_N);
                 }
                 ++issued;
             }
@@ -308,21 +349,33 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_tc_kernel(const __grid_cons
             bd[i] = CUDART_INF_F;
             bi[i] = -1;
         }
+        float thr = CUDART_INF_F;
         for (int it = 0; it < n_tiles; ++it) {
             const int buf = it & 1;
             if (!mbar_wait(&sm.tmem_full[buf], (it >> 1) & 1, abort_flag, err)) break;
             tc_fence_after();
             const uint32_t taddr = tmem_base + (uint32_t(quarter * 32) << 16) + buf * TC_N;
-            const int col0 = it * TC_N;
+            const bool diag = (it == static_cast<int>(blockIdx.x));
 #pragma unroll 1
             for (int ch = 0; ch < TC_N / 32; ++ch) {
                 uint32_t r[32];
                 tmem_load32(taddr + ch * 32, r);
+                float d2[32];
+                uint32_t mask = 0;
 #pragma unroll
                 for (int i = 0; i < 32; ++i) {
-                    const int col = col0 + ch * 32 + i;
-                    const float d2 = fmaf(-2.0f, __uint_as_float(r[i]), qn + __ldg(norms + col));
-                    if (d2 < bd[KCAP - 1] && col != q) insert_sorted<KCAP>(bd, bi, d2, col);
+                    d2[i] = fmaf(-2.0f, __uint_as_float(r[i]), qn);
+                    mask |= (d2[i] < thr ? 1u : 0u) << i;
+                }
+                if (diag && ch == (row >> 5)) mask &= ~(1u << (row & 31));   // self
+                while (mask) {   // rare: candidates better than the current k-th
+                    const int i = __ffs(mask) - 1;
+                    mask &= mask - 1;
+                    const float v = select32(d2, i);
+                    if (v < thr) {
+                        insert_sorted<KCAP>(bd, bi, v, it * TC_N + ch * 32 + i);
+                        thr = bd[KCAP - 1];
+                    }
                 }
             }
             tc_fence_before();
@@ -384,10 +437,14 @@ CUtensorMap make_map(const float* base, int64_t rows, int k_pad) {
     return m;
 }
 
+struct Maps {
+    CUtensorMap ahi, alo, bhi, blo;
+};
+
 template <int KC, int KCAP>
-void launch_tc(const CUtensorMap& mh, const CUtensorMap& ml, const float* norms, int32_t n, int32_t n_pad,
-               int32_t* cand_idx, float* cand_d2, int* err, cudaStream_t s) {
-    const size_t smem = sizeof(TcSmem<KC, KCAP>) + 1024;
+void launch_tc(const Maps& m, const float* norms, int32_t n, int32_t n_pad, int32_t* cand_idx, float* cand_d2, int* err,
+               cudaStream_t s) {
+    const size_t smem = sizeof(TcSmem<KC>) + 1024;
     static bool configured = false;
     if (!configured) {
         UMAPB_CUDA(cudaFuncSetAttribute(knn_tc_kernel<KC, KCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -395,39 +452,48 @@ void launch_tc(const CUtensorMap& mh, const CUtensorMap& ml, const float* norms,
         configured = true;
     }
     const int n_tiles = n_pad / TC_N;
-    knn_tc_kernel<KC, KCAP><<<n_pad / TC_M, TC_THREADS, smem, s>>>(mh, ml, norms, n, n_tiles, cand_idx, cand_d2, err);
+    knn_tc_kernel<KC, KCAP><<<n_pad / TC_M, TC_THREADS, smem, s>>>(m.ahi, m.alo, m.bhi, m.blo, norms, n, n_tiles,
+                                                                   cand_idx, cand_d2, err);
     UMAPB_LAUNCH_CHECK();
+}
+
+template <int KC>
+void launch_kcap(int kcap, const Maps& m, const float* norms, int32_t n, int32_t n_pad, int32_t* cand_idx,
+                 float* cand_d2, int* err, cudaStream_t s) {
+    if (kcap == 16) launch_tc<KC, 16>(m, norms, n, n_pad, cand_idx, cand_d2, err, s);
+    else if (kcap == 24) launch_tc<KC, 24>(m, norms, n, n_pad, cand_idx, cand_d2, err, s);
+    else launch_tc<KC, 32>(m, norms, n, n_pad, cand_idx, cand_d2, err, s);
 }
 
 }  // namespace
 
-bool knn_tc_supported(int32_t dim, int kcap) { return dim >= 1 && dim <= 2 * TC_KCHUNK && (kcap == 16 || kcap == 24 || kcap == 32); }
+// The norm rides in one extra K column, so dim + 1 columns must fit in two 32-wide chunks.
+bool knn_tc_supported(int32_t dim, int kcap) {
+    return dim >= 1 && dim + 1 <= 2 * TC_KCHUNK && (kcap == 16 || kcap == 24 || kcap == 32);
+}
 
 // Candidate lists (KCAP per query, FP32 squared distances, ascending) from the
-// tensor-core search; also returns the largest reference norm for the
-// certainty bound of the FP64 rescoring.
+// tensor-core search; norms_out receives |x|^2 for the certainty bound of the
+// FP64 rescoring.
 void knn_tc_candidates(const float* data, int32_t n, int32_t dim, int kcap, int32_t* cand_idx, float* cand_d2,
                        float* norms_out, int* d_err, cudaStream_t s) {
     require(knn_tc_supported(dim, kcap), "tensor-core kNN: unsupported dimension or candidate count");
-    const int kc = (dim + TC_KCHUNK - 1) / TC_KCHUNK;
+    const int kc = (dim + 1 + TC_KCHUNK - 1) / TC_KCHUNK;
     const int k_pad = kc * TC_KCHUNK;
     const int32_t n_pad = ((n + TC_M - 1) / TC_M) * TC_M;
-    DevArray<float> hi(static_cast<size_t>(n_pad) * k_pad, s), lo(static_cast<size_t>(n_pad) * k_pad, s);
-    split_tf32_kernel<<<grid_for(static_cast<size_t>(n_pad) * k_pad, 256), 256, 0, s>>>(data, n, dim, n_pad, k_pad,
-                                                                                        hi.get(), lo.get(), norms_out);
+    const size_t elems = static_cast<size_t>(n_pad) * k_pad;
+    DevArray<float> ahi(elems, s), alo(elems, s), bhi(elems, s), blo(elems, s);
+    prepare_operands_kernel<<<grid_for(n_pad, 256), 256, 0, s>>>(data, n, dim, n_pad, k_pad, ahi.get(), alo.get(),
+                                                                  bhi.get(), blo.get(), norms_out);
     UMAPB_LAUNCH_CHECK();
-    const CUtensorMap mh = make_map(hi.get(), n_pad, k_pad);
-    const CUtensorMap ml = make_map(lo.get(), n_pad, k_pad);
-    if (kc == 1) {
-        if (kcap == 16) launch_tc<1, 16>(mh, ml, norms_out, n, n_pad, cand_idx, cand_d2, d_err, s);
-        else if (kcap == 24) launch_tc<1, 24>(mh, ml, norms_out, n, n_pad, cand_idx, cand_d2, d_err, s);
-        else launch_tc<1, 32>(mh, ml, norms_out, n, n_pad, cand_idx, cand_d2, d_err, s);
-    } else {
-        if (kcap == 16) launch_tc<2, 16>(mh, ml, norms_out, n, n_pad, cand_idx, cand_d2, d_err, s);
-        else if (kcap == 24) launch_tc<2, 24>(mh, ml, norms_out, n, n_pad, cand_idx, cand_d2, d_err, s);
-        else launch_tc<2, 32>(mh, ml, norms_out, n, n_pad, cand_idx, cand_d2, d_err, s);
-    }
-    // keep hi/lo alive until the kernel has run (stream-ordered free)
+    Maps m;
+    m.ahi = make_map(ahi.get(), n_pad, k_pad);
+    m.alo = make_map(alo.get(), n_pad, k_pad);
+    m.bhi = make_map(bhi.get(), n_pad, k_pad);
+    m.blo = make_map(blo.get(), n_pad, k_pad);
+    if (kc == 1) launch_kcap<1>(kcap, m, norms_out, n, n_pad, cand_idx, cand_d2, d_err, s);
+    else launch_kcap<2>(kcap, m, norms_out, n, n_pad, cand_idx, cand_d2, d_err, s);
+    // the operand arrays are released stream-ordered, after the kernel
 }
 
 }  // namespace umapb
