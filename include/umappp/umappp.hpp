@@ -1,0 +1,18 @@
+#ifndef UMAPPP_UMAPPP_HPP
+#define UMAPPP_UMAPPP_HPP
+
+/**
+ * @file umappp.hpp
+ * @brief Umbrella header of the GPU drop-in for libscran/umappp
+ * (include/umappp/umappp.hpp:9-11): Options, Status, initialize() and the
+ * stage functions, backed by libumappp_b200.so (C ABI in umapb.h).
+ */
+
+#include "Options.hpp"
+#include "Status.hpp"
+#include "initialize.hpp"
+#include "stages.hpp"
+
+namespace umappp {}
+
+#endif

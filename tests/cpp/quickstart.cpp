@@ -1,0 +1,44 @@
+// Drop-in check: the reference's quick-start usage (README "Quick start")
+// written against the GPU headers: 2000 observations x 10 dims of N(0, 1)
+// data, exact neighbours on the device, initialize() then run(), plus a
+// partial run and the NeighborList overload.  Prints one line of results.
+#include <cmath>
+#include <cstdio>
+#include <random>
+#include <vector>
+
+#include "umappp/umappp.hpp"
+
+int main() {
+    const int ndim = 10, nobs = 2000;
+    std::vector<double> data(static_cast<size_t>(ndim) * nobs);
+    std::mt19937_64 rng(1000);
+    std::normal_distribution<double> ndist;
+    for (auto& x : data) x = ndist(rng);
+
+    const size_t out_dim = 2;
+    std::vector<double> embedding(nobs * out_dim);
+    umappp::Options opt;
+    auto status = umappp::initialize(ndim, nobs, data.data(), umappp::DeviceBuilder(), out_dim, embedding.data(), opt);
+    if (status.epoch() != 0 || status.num_epochs() != 500 || status.num_observations() != nobs) return 2;
+    status.run(embedding.data(), 200);
+    if (status.epoch() != 200) return 3;
+    status.run(embedding.data());
+    if (status.epoch() != 500) return 4;
+    for (double v : embedding)
+        if (!std::isfinite(v)) return 5;
+
+    // the NeighborList overload with float data
+    umappp::NeighborList<int, float> nl(nobs);
+    for (int i = 0; i < nobs; ++i)
+        for (int j = 1; j <= 5; ++j) nl[i].emplace_back((i + j) % nobs, 0.1f * j);
+    std::vector<float> emb2(nobs * out_dim);
+    opt.num_epochs = 50;
+    auto st2 = umappp::initialize(nl, out_dim, emb2.data(), opt);
+    st2.run(emb2.data());
+    const auto ep = st2.get_epoch_data();
+    const auto ab = umappp::find_ab<double>(1.0, 0.1);
+    std::printf("quickstart ok: epochs=%d edges=%zu a=%.6f b=%.6f y0=%.4f\n", status.epoch(), ep.edge_targets.size(),
+                ab.first, ab.second, embedding[0]);
+    return 0;
+}

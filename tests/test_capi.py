@@ -73,3 +73,18 @@ def test_no_device_fails_loudly(umap):
     assert e.value.code == 6
     with pytest.raises(umap.UmapbError):
         umap.initialize([[(1, 1.0)], [(0, 1.0)]], 2, np.zeros((2, 2)))
+
+
+def _compile_quickstart(out_path):
+    import subprocess
+    src = os.path.join(ROOT, "tests", "cpp", "quickstart.cpp")
+    cmd = ["g++", "-std=c++17", "-O1", "-I" + os.path.join(ROOT, "include"), src,
+           "-L" + os.path.join(ROOT, "umappp_b200"), "-lumappp_b200",
+           "-Wl,-rpath," + os.path.join(ROOT, "umappp_b200"), "-o", out_path]
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+
+
+def test_cpp_dropin_headers_compile(umap, tmp_path):
+    # user code written for the reference's API compiles and links against the GPU headers
+    _compile_quickstart(str(tmp_path / "quickstart"))
+    assert (tmp_path / "quickstart").exists()

@@ -209,3 +209,13 @@ def test_invalid_arguments(umap):
         umap.initialize([[(5, 1.0)], [(0, 1.0)]], 2, np.zeros((2, 2)))   # out-of-range index
     with pytest.raises(umap.UmapbError):
         umap.initialize([[(1, 1.0)], [(0, 1.0)]], 0, np.zeros((2, 0)))  # num_dim 0
+
+
+def test_cpp_quickstart_runs(umap, tmp_path):
+    import subprocess
+    from test_capi import _compile_quickstart
+    exe = str(tmp_path / "quickstart")
+    _compile_quickstart(exe)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    assert "quickstart ok: epochs=500" in r.stdout
