@@ -269,6 +269,32 @@ int umapb_loss_grad(int dtype, size_t num_dim, const void* embedding, int32_t nu
                     const int32_t* indices, const void* weights, double a, double b, double eps_rep,
                     int with_constant, double* loss, void* grad_embedding, double* grad_ab);
 
+/*
+ * umapb_loss_grad without any device allocation.  It has no counterpart in
+ * the reference.
+ *
+ * For callers that cannot call cudaMalloc: a framework that owns all device
+ * memory through its own pool (where a stray allocation fails or fragments
+ * it), or a serving loop whose per-request path must not block on the
+ * allocator, which also synchronises the device.  Same arguments and results as
+ * umapb_loss_grad, with these differences:
+ *   - embedding, row_ptr, indices, weights and grad_embedding must be device
+ *     memory (host pointers are rejected with UMAPB_ERR_INVALID); loss and
+ *     grad_ab are host memory;
+ *   - the work runs on the calling thread's per-thread default stream;
+ *   - its scratch is a fixed array in the library's device memory (32 MB on
+ *     every device that loads the library, held until exit); for UMAPB_F32 a
+ *     gradient of more than 4,194,304 elements (num_obs * num_dim) is rejected
+ *     with UMAPB_ERR_INVALID;
+ *   - the first call on a device looks up the scratch's device address
+ *     (cudaGetSymbolAddress); make that first call before any stream capture;
+ *   - every call shares the one scratch array, so calls that overlap on the
+ *     GPU (other threads, other streams) race; serialise them.
+ */
+int umapb_loss_grad_noalloc(int dtype, size_t num_dim, const void* embedding, int32_t num_obs, const int64_t* row_ptr,
+                            const int32_t* indices, const void* weights, double a, double b, double eps_rep,
+                            int with_constant, double* loss, void* grad_embedding, double* grad_ab);
+
 #ifdef __cplusplus
 }
 #endif

@@ -77,6 +77,8 @@ SIGNATURES = {
                                        _P(_c_int), _c_dbl, _c_dbl, _c_dbl, _c_dbl, _c_u64, _c_int]),
     "umapb_loss_grad": (_c_int, [_c_int, _c_size, _vp, _c_i32, _vp, _vp, _vp, _c_dbl, _c_dbl, _c_dbl, _c_int,
                                  _P(_c_dbl), _vp, _vp]),
+    "umapb_loss_grad_noalloc": (_c_int, [_c_int, _c_size, _vp, _c_i32, _vp, _vp, _vp, _c_dbl, _c_dbl, _c_dbl, _c_int,
+                                         _P(_c_dbl), _vp, _vp]),
 }
 
 _lib = None

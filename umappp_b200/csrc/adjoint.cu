@@ -18,6 +18,9 @@
 // per block; per-coordinate gradients use FP64 atomics.
 #include <cub/cub.cuh>
 
+#include <mutex>
+#include <type_traits>
+
 #include "stages.cuh"
 
 namespace umapb {
@@ -134,4 +137,124 @@ template void loss_grad<float>(int32_t, int, const float*, const int64_t*, const
 template void loss_grad<double>(int32_t, int, const double*, const int64_t*, const int32_t*, const double*, double,
                                 double, double, bool, double*, double*, double*, cudaStream_t);
 
+// ------------------------------------------------- allocation-free variant --
+//
+// Scratch for umapb_loss_grad_noalloc, resident on every device that loads the
+// library: [0, 3) the loss and dL/da, dL/db accumulators, [4, 4 + max) the FP64
+// accumulation of a float gradient.  Its host-side name is only a stand-in;
+// kernels get the device address from cudaGetSymbolAddress.
+constexpr size_t NOALLOC_GRAD_MAX = size_t(1) << 22;   // gradient elements (n * num_dim) for float data
+constexpr size_t NOALLOC_ACC_OFFSET = 0;
+constexpr size_t NOALLOC_GRAD_OFFSET = 4;
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_GRAD_OFFSET + NOALLOC_GRAD_MAX];
+
+namespace {
+
+constexpr int MAX_DEVICES = 64;
+std::mutex g_noalloc_mutex;
+double* g_noalloc_ptr[MAX_DEVICES] = {nullptr};
+
+// Device address of the scratch on the current device, looked up once per device.
+double* noalloc_scratch(int dev) {
+    require(dev >= 0 && dev < MAX_DEVICES, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        UMAPB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_ptr[dev] = static_cast<double*>(p);
+    }
+    return g_noalloc_ptr[dev];
+}
+
+bool device_pointer(const void* p) {
+    if (!p) return false;
+    cudaPointerAttributes attr;
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+template <typename T>
+void loss_grad_noalloc(int32_t n, int num_dim, const T* Y, const int64_t* ptr, const int32_t* idx, const T* w, double a,
+                       double b, double eps_rep, bool with_constant, double* loss_out, T* grad_Y, double* grad_ab) {
+    require(a > 0 && b > 0, "a and b must be positive");
+    require(n >= 0 && num_dim >= 1, "num_obs must be non-negative and num_dim positive");
+    const size_t total = static_cast<size_t>(n) * num_dim;
+    if (grad_Y && std::is_same<T, float>::value) {
+        require(total <= NOALLOC_GRAD_MAX,
+                "num_obs * num_dim exceeds the allocation-free scratch (4194304 gradient elements for float data)");
+    }
+    require(device_pointer(Y) && device_pointer(ptr) && device_pointer(idx) && device_pointer(w),
+            "the allocation-free entry point takes device pointers for embedding, row_ptr, indices and weights");
+    require(!grad_Y || device_pointer(grad_Y), "grad_embedding must be a device pointer (or NULL)");
+    int dev = 0;
+    UMAPB_CUDA(cudaGetDevice(&dev));
+    double* scratch = noalloc_scratch(dev);
+    double* acc = scratch + NOALLOC_ACC_OFFSET;
+    const cudaStream_t s = cudaStreamPerThread;
+    UMAPB_CUDA(cudaMemsetAsync(acc, 0, 3 * sizeof(double), s));
+    double* gptr = nullptr;
+    if (grad_Y) {
+        if constexpr (std::is_same<T, double>::value) {
+            gptr = grad_Y;
+        } else {
+            gptr = scratch + NOALLOC_GRAD_OFFSET;
+        }
+        UMAPB_CUDA(cudaMemsetAsync(gptr, 0, total * sizeof(double), s));
+    }
+    if (n > 0) {
+        loss_grad_kernel<T><<<(n + ADJ_BLOCK - 1) / ADJ_BLOCK, ADJ_BLOCK, 0, s>>>(
+            n, num_dim, Y, ptr, idx, w, a, b, eps_rep, with_constant ? 1 : 0, gptr, acc);
+        UMAPB_LAUNCH_CHECK();
+    }
+    if (grad_Y && !std::is_same<T, double>::value) {
+        cast_grad_kernel<T><<<grid_for(total, 256), 256, 0, s>>>(total, gptr, grad_Y);
+        UMAPB_LAUNCH_CHECK();
+    }
+    double h[3];
+    UMAPB_CUDA(cudaMemcpyAsync(h, acc, sizeof(h), cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaStreamSynchronize(s));
+    if (loss_out) *loss_out = h[0];
+    if (grad_ab) {
+        grad_ab[0] = h[1];
+        grad_ab[1] = h[2];
+    }
+}
+
+}  // namespace
+
 }  // namespace umapb
+
+extern "C" int umapb_loss_grad_noalloc(int dtype, size_t num_dim, const void* embedding, int32_t num_obs,
+                                       const int64_t* row_ptr, const int32_t* indices, const void* weights, double a,
+                                       double b, double eps_rep, int with_constant, double* loss,
+                                       void* grad_embedding, double* grad_ab) {
+    using namespace umapb;
+    try {
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+            cudaGetLastError();
+            fail(UMAPB_ERR_NO_DEVICE, "no CUDA device is available (libumappp_b200 runs on sm_100 GPUs only)");
+        }
+        require(dtype == UMAPB_F32 || dtype == UMAPB_F64, "dtype must be UMAPB_F32 or UMAPB_F64");
+        if (dtype == UMAPB_F64) {
+            loss_grad_noalloc<double>(num_obs, static_cast<int>(num_dim), static_cast<const double*>(embedding), row_ptr,
+                                      indices, static_cast<const double*>(weights), a, b, eps_rep, with_constant != 0,
+                                      loss, static_cast<double*>(grad_embedding), grad_ab);
+        } else {
+            loss_grad_noalloc<float>(num_obs, static_cast<int>(num_dim), static_cast<const float*>(embedding), row_ptr,
+                                     indices, static_cast<const float*>(weights), a, b, eps_rep, with_constant != 0,
+                                     loss, static_cast<float*>(grad_embedding), grad_ab);
+        }
+        return UMAPB_OK;
+    } catch (const Error& e) {
+        set_last_error(e.what());
+        cudaGetLastError();
+        return e.code;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return UMAPB_ERR_INVALID;
+    }
+}

@@ -55,6 +55,8 @@ void require_device() {
 
 }  // namespace
 
+void set_last_error(const std::string& m) { set_error(m); }
+
 Context& thread_context() {
     thread_local Context ctx;
     int dev = 0;

@@ -187,6 +187,7 @@ struct Context {
 };
 
 Context& thread_context();                 // defined in capi.cu
+void set_last_error(const std::string& m);  // message for umapb_last_error() on this thread
 void check_device_status(Context& ctx);     // reads and clears the status word; throws on error
 
 inline unsigned grid_for(size_t work, unsigned block, unsigned max_blocks = 148u * 64u) {
