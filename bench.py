@@ -45,6 +45,9 @@ CONFIGS = {
     "small_2k": (2_000, 10, 1, 0.0, "equal", 15, 500),
 }
 METRIC = "end-to-end s & SGD edge-updates/s, 1M pts; FP32/batched vs plain at equal trust"
+# Batched workload: 64 independent instances, sizes log-uniform in [500, 50000],
+# 30 dims, float32 5-cluster mixtures, k = 15, 200 epochs.
+BATCH = {"instances": 64, "min": 500, "max": 50_000, "dim": 30, "clusters": 5, "k": 15, "epochs": 200}
 
 
 def make_data(cfg: str, seed: int = 20241203) -> np.ndarray:
@@ -214,6 +217,77 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     return out
 
 
+def make_batch(seed: int = 20241203):
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(BATCH["min"]), np.log(BATCH["max"]), size=BATCH["instances"])).astype(np.int32)
+    parts = []
+    for m in sizes:
+        centres = rng.normal(0.0, 5.0, size=(BATCH["clusters"], BATCH["dim"])).astype(np.float32)
+        labels = rng.choice(BATCH["clusters"], size=int(m))
+        parts.append(centres[labels] + rng.standard_normal(size=(int(m), BATCH["dim"]), dtype=np.float32))
+    return sizes, np.ascontiguousarray(np.concatenate(parts))
+
+
+def run_batch(args, rank: int, world: int) -> dict | None:
+    """64 instances in one umapb_batch_run call against 64 plain
+    initialize_from_data + run calls, device-resident inputs for both."""
+    import torch
+    import umappp_b200 as U
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    sizes, X = make_batch(20241203 + rank)
+    n = int(sizes.sum())
+    opt = U.Options(num_neighbors=BATCH["k"], num_epochs=BATCH["epochs"])
+    d_data = torch.from_numpy(X).to(dev)
+    d_emb = torch.zeros((n, 2), dtype=torch.float32, device=dev)
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    views = [(d_data[offs[i]:offs[i + 1]], d_emb[offs[i]:offs[i + 1]]) for i in range(len(sizes))]
+
+    def batched():
+        return U.batch_run(d_data, sizes, 2, d_emb, opt)
+
+    def sequential():
+        for xd, yd in views:
+            st = U.initialize_from_data(xd, 2, yd, opt)
+            st.run(yd)
+
+    def timed(fn, steps):
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        l0 = U.lib().umapb_launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        last = None
+        for _ in range(steps):
+            last = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, last, (U.lib().umapb_launch_count() - l0) // max(steps, 1)
+
+    for _ in range(args.warmup):
+        batched()
+    with ClockSampler(dev.index) as clk:
+        ms, stages, launches = timed(batched, args.steps)
+    sequential()
+    seq_ms, _, seq_launches = timed(sequential, 1)
+    return {"metric": "batched UMAP: 64 instances, seconds per batch", "value": round(ms / 1e3, 4), "unit": "s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded Gaussian mixtures)",
+            "config": {"workload": f"batch64: {len(sizes)} instances, sizes {int(sizes.min())}..{int(sizes.max())} "
+                                   f"(total {n}), dim={BATCH['dim']} k={BATCH['k']} epochs={BATCH['epochs']}"},
+            "sequential_plain_s": round(seq_ms / 1e3, 4), "speedup_vs_sequential": round(seq_ms / ms, 2),
+            "stage_ms": {k_: round(v, 3) for k_, v in stages.items()}, "gpu_launches": int(launches),
+            "sequential_gpu_launches": int(seq_launches), "clocks": clk.summary()}
+
+
 # --------------------------------------------------- reference on CPU ---
 
 def cpu_sample(cfg: str, budget_queries: int = 1000, sub_n: int = 50_000, sgd_epochs: int = 10) -> dict:
@@ -282,13 +356,18 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="mixture_1m", choices=sorted(CONFIGS))
+    ap.add_argument("--config", default="mixture_1m", choices=sorted(CONFIGS) + ["batch64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     if args.impl == "reference":
+        if args.config == "batch64":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "batch64 is a device-only mode without a "
+                                  "reference counterpart"}), flush=True)
+            return
         out = run_reference(args, rank)
         if out is not None:
             print(json.dumps(out), flush=True)
@@ -299,9 +378,9 @@ def main() -> None:
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     try:
-        out = run_ours(args, rank, world)
+        out = run_batch(args, rank, world) if args.config == "batch64" else run_ours(args, rank, world)
         if rank == 0 and out is not None:
-            if world == 1 and not args.no_cpu_baseline:
+            if world == 1 and not args.no_cpu_baseline and args.config != "batch64":
                 out["cpu_baseline"] = cpu_sample(args.config)
             print(json.dumps(out), flush=True)
     finally:

@@ -251,6 +251,27 @@ int umapb_optimize_layout(int dtype, size_t num_dim, void* embedding, int32_t nu
                           int* current_epoch, double a, double b, double gamma, double learning_rate, uint64_t seed,
                           int epoch_limit);
 
+/* ----------------------------------------------------------------- batched */
+
+/*
+ * Many independent UMAP instances in one call (no counterpart in the
+ * reference, where each would be its own initialize() + run()).  Instance i is
+ * the next sizes[i] observations of 'data' (num_instances blocks one after
+ * another, data_dim values per observation); its embedding is written to the
+ * matching rows of 'embedding'.  Every instance uses 'opt' as one
+ * initialize(data, builder, ...) + Status::run() would, with these shared
+ * steps: one tensor-core kNN launch over all instances (each query searches
+ * its own instance only), one similarity / union / schedule pass over the
+ * block-diagonal graph (each instance keeps its own maximum weight), and one
+ * SGD launch per epoch over all instances (negative samples drawn inside the
+ * head's instance), the epochs recorded as one CUDA graph, with the launch
+ * shape chosen by the autotuner.  All instances must resolve to the same
+ * epoch count (set opt->num_epochs when their sizes differ across 10000).
+ * stage_ms (may be NULL) receives the 7 stage times of umapb_status_stage_ms.
+ */
+int umapb_batch_run(int dtype, int32_t num_instances, const int32_t* sizes, size_t data_dim, const void* data,
+                    size_t num_dim, void* embedding, const umapb_options* opt, double* stage_ms);
+
 /* ----------------------------------------------------------------- adjoint */
 
 /*

@@ -66,30 +66,38 @@ def test_layout_quality_matches_reference(umap, dtype):
     g, ep = _oracle_pipeline(nl, dtype, 500)
     ok, Y0, _ = oracle.spectral_init(g, 2)
     assert ok
-    # device run from the oracle's initial layout
-    Y = np.ascontiguousarray(Y0.copy())
-    st = umap.initialize(csr_tuple(nl), 2, Y, umap.Options(initialize_method=umap.InitializeMethod.NONE))
-    st.run(Y)
-    assert st.epoch() == 500
-    assert np.all(np.isfinite(Y))
-    # reference serial runs from the same layout, over several optimize seeds:
-    # at 2000 points the reference's own seed-to-seed spread (about 0.007 in
-    # trustworthiness and 1% in cross-entropy) is as large as the bars, so the
-    # device is compared with the mean of the reference runs, with the bar
-    # widened to two standard deviations of that spread where it is larger
+    # At 2000 points a single run's trustworthiness varies by about 0.007 and its
+    # cross-entropy by about 1% from seed to seed (in the reference too), as much
+    # as the bars themselves.  So the mean over 4 device runs (different optimize
+    # seeds) is compared with the mean over 6 reference runs (its serial SGD,
+    # same initial layout): within 0.005 / 1%, or within 2.5 standard errors of
+    # the difference of the means where that is larger.
     a, b = oracle.find_ab(1.0, 0.1)
-    t_ref, ce_ref = [], []
+    gw = g.astype(np.float64)
+    t_dev, ce_dev = [], []
     for seed in range(4):
+        Y = np.ascontiguousarray(Y0.copy())
+        st = umap.initialize(csr_tuple(nl), 2, Y, umap.Options(initialize_method=umap.InitializeMethod.NONE,
+                                                                optimize_seed=1234567890 + 101 * seed))
+        st.run(Y)
+        assert st.epoch() == 500
+        assert np.all(np.isfinite(Y))
+        t_dev.append(oracle.trustworthiness(X, Y, 15))
+        ce_dev.append(oracle.cross_entropy(gw, Y, a, b))
+    t_ref, ce_ref = [], []
+    for seed in range(6):
         R = Y0.copy()
         oracle.optimize_layout(2, R, ep.copy(), a, b, 1.0, 1.0, 1234567890 + seed, 500)
         t_ref.append(oracle.trustworthiness(X, R, 15))
-        ce_ref.append(oracle.cross_entropy(g.astype(np.float64), R, a, b))
-    t_dev = oracle.trustworthiness(X, Y, 15)
-    ce_dev = oracle.cross_entropy(g.astype(np.float64), Y, a, b)
-    t_bar = max(0.005, 2 * float(np.std(t_ref)))
-    ce_bar = max(0.01, 2 * float(np.std(ce_ref) / np.mean(ce_ref)))
-    assert abs(t_dev - np.mean(t_ref)) <= t_bar, (t_dev, t_ref)
-    assert abs(ce_dev - np.mean(ce_ref)) <= ce_bar * np.mean(ce_ref), (ce_dev, ce_ref)
+        ce_ref.append(oracle.cross_entropy(gw, R, a, b))
+
+    def se(x, y):
+        return float(np.sqrt(np.var(x, ddof=1) / len(x) + np.var(y, ddof=1) / len(y)))
+
+    t_bar = max(0.005, 2.5 * se(t_dev, t_ref))
+    ce_bar = max(0.01 * np.mean(ce_ref), 2.5 * se(ce_dev, ce_ref))
+    assert abs(np.mean(t_dev) - np.mean(t_ref)) <= t_bar, (t_dev, t_ref)
+    assert abs(np.mean(ce_dev) - np.mean(ce_ref)) <= ce_bar, (ce_dev, ce_ref)
 
 
 def test_spectral_initialize_matches_reference(umap):

@@ -32,7 +32,10 @@ def _same_neighbors(idx_a, idx_b, dist_ref, rel_tie=1e-6):
     return bad
 
 
-@pytest.mark.parametrize("n,dim,k", [(2000, 10, 15), (1500, 50, 15), (600, 7, 5), (300, 3, 30)])
+# (12, 4, 5), (20, 3, 10): fewer other points than the candidate list holds, so
+# padding columns of the tensor-core tile must never become candidates
+@pytest.mark.parametrize("n,dim,k", [(2000, 10, 15), (1500, 50, 15), (600, 7, 5), (300, 3, 30), (12, 4, 5),
+                                     (20, 3, 10), (129, 6, 15)])
 def test_knn_f32_matches_fp64_bruteforce(umap, n, dim, k):
     X = oracle.gaussian_mixture(n, dim, 6, 4.0, seed=n + dim, dtype=np.float32)
     idx, dist = umap.knn(X, k)

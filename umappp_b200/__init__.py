@@ -36,7 +36,7 @@ __all__ = [
     "InitializeMethod", "Options", "Status", "EpochData", "initialize", "initialize_from_data", "knn",
     "neighbor_similarities", "combine_neighbor_sets", "similarities_to_epochs", "has_multiple_components",
     "spectral_init", "random_init", "find_ab", "choose_num_epochs", "optimize_layout", "loss_grad", "UmapbError",
-    "to_csr",
+    "to_csr", "batch_run",
 ]
 
 
@@ -276,6 +276,27 @@ def initialize_from_data(data, num_dim: int, embedding, options: Optional[Option
     check(lib().umapb_initialize_data(_dtype_code(dt), data_dim, num_obs, _ptr(data), num_dim, _ptr(embedding),
                                       ctypes.byref(copt), ctypes.byref(out)))
     return Status(out.value, dt)
+
+
+def batch_run(data, sizes, num_dim: int, embedding, options: Optional[Options] = None) -> dict:
+    """Many independent UMAP runs in one pass: instance i is the next sizes[i]
+    rows of 'data' (float32/float64, (sum(sizes), data_dim)) and of 'embedding'
+    ((sum(sizes), num_dim), overwritten with the final layouts).  Each instance
+    gets the result of initialize_from_data + run with the same options, except
+    that the optimisation draws its negative samples from a different generator
+    stream.  All instances must resolve to the same epoch count (give
+    num_epochs when their sizes straddle 10,000).  Returns the stage times in ms."""
+    options = options or Options()
+    dt = _float_dtype(data)
+    sizes = np.ascontiguousarray(np.asarray(sizes, dtype=np.int32))
+    shape = data.shape if isinstance(data, np.ndarray) else tuple(data.__cuda_array_interface__["shape"])
+    if int(shape[0]) != int(sizes.sum()):
+        raise ValueError("data must have sum(sizes) rows")
+    ms = np.zeros(len(STAGES), dtype=np.float64)
+    copt = options.to_c()
+    check(lib().umapb_batch_run(_dtype_code(dt), len(sizes), _ptr(sizes), int(shape[1]), _ptr(data), num_dim,
+                                _ptr(embedding), ctypes.byref(copt), _ptr(ms)))
+    return dict(zip(STAGES, ms.tolist()))
 
 
 # ------------------------------------------------------------ stage calls --

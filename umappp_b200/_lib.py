@@ -79,6 +79,7 @@ SIGNATURES = {
                                  _P(_c_dbl), _vp, _vp]),
     "umapb_loss_grad_noalloc": (_c_int, [_c_int, _c_size, _vp, _c_i32, _vp, _vp, _vp, _c_dbl, _c_dbl, _c_dbl, _c_int,
                                          _P(_c_dbl), _vp, _vp]),
+    "umapb_batch_run": (_c_int, [_c_int, _c_i32, _vp, _c_size, _vp, _c_size, _vp, _P(UmapbOptions), _vp]),
 }
 
 _lib = None

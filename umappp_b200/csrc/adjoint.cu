@@ -124,7 +124,7 @@ void loss_grad(int32_t n, int num_dim, const T* Y, const int64_t* ptr, const int
     }
     double h[3];
     UMAPB_CUDA(cudaMemcpyAsync(h, acc.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
-    UMAPB_CUDA(cudaStreamSynchronize(s));
+    UMAPB_SYNC(s);
     if (loss_out) *loss_out = h[0];
     if (grad_ab) {
         grad_ab[0] = h[1];
@@ -215,7 +215,7 @@ void loss_grad_noalloc(int32_t n, int num_dim, const T* Y, const int64_t* ptr, c
     }
     double h[3];
     UMAPB_CUDA(cudaMemcpyAsync(h, acc, sizeof(h), cudaMemcpyDeviceToHost, s));
-    UMAPB_CUDA(cudaStreamSynchronize(s));
+    UMAPB_SYNC(s);
     if (loss_out) *loss_out = h[0];
     if (grad_ab) {
         grad_ab[0] = h[1];

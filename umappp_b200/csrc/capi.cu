@@ -99,10 +99,10 @@ struct umapb_status {
     ~umapb_status() {
         impl.reset();
         if (stream) {
+            if (d_status) umapb::ws_free(d_status, stream);
             cudaStreamSynchronize(stream);
-            cudaStreamDestroy(stream);
+            umapb::stream_put(stream);   // streams are pooled: creating one is a resource-manager call
         }
-        if (d_status) cudaFree(d_status);
     }
 };
 
@@ -119,15 +119,13 @@ struct StageTimer {
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
     explicit StageTimer(cudaStream_t st, float* o) : s(st), out(o) {}
     void begin(int stage) {
-        cudaEvent_t a, b;
-        UMAPB_CUDA(cudaEventCreate(&a));
-        UMAPB_CUDA(cudaEventCreate(&b));
+        cudaEvent_t a = event_get(), b = event_get();
         UMAPB_CUDA(cudaEventRecord(a, s));
         marks.push_back({stage, {a, b}});
     }
     void end() { UMAPB_CUDA(cudaEventRecord(marks.back().second.second, s)); }
     void resolve() {
-        UMAPB_CUDA(cudaStreamSynchronize(s));
+        UMAPB_SYNC(s);
         for (auto& m : marks) {
             float t = 0;
             cudaEventElapsedTime(&t, m.second.first, m.second.second);
@@ -136,8 +134,8 @@ struct StageTimer {
     }
     ~StageTimer() {
         for (auto& m : marks) {
-            cudaEventDestroy(m.second.first);
-            cudaEventDestroy(m.second.second);
+            event_put(m.second.first);
+            event_put(m.second.second);
         }
     }
 };
@@ -218,7 +216,7 @@ struct StatusImpl final : StatusBase {
         engine.run(Y.get(), static_cast<int>(st->num_dim), st->current_epoch, epoch_limit, st->a, st->b,
                    st->opt.repulsion_strength, st->opt.learning_rate, st->opt.optimize_seed, s, &ms_sched, &ms_sgd);
         Y.finish();
-        UMAPB_CUDA(cudaStreamSynchronize(s));
+        UMAPB_SYNC(s);
         st->stage_ms[ST_SCHEDULE] = ms_sched;
         st->stage_ms[ST_SGD] = ms_sgd;
         st->current_epoch = epoch_limit;
@@ -237,9 +235,9 @@ struct StatusImpl final : StatusBase {
             engine.state_at(st->current_epoch, a.get(), b.get(), s);
             copy_out(enext, a.get(), sizeof(T) * nnz, s);
             copy_out(enneg, b.get(), sizeof(T) * nnz, s);
-            UMAPB_CUDA(cudaStreamSynchronize(s));
+            UMAPB_SYNC(s);
         }
-        UMAPB_CUDA(cudaStreamSynchronize(s));
+        UMAPB_SYNC(s);
     }
 
     void counts(int first, int last, int64_t* out) override { engine.counts(first, last, out, st->stream); }
@@ -254,9 +252,9 @@ std::unique_ptr<umapb_status> new_status(int dtype, int32_t n, size_t num_dim, c
     auto st = std::make_unique<umapb_status>();
     st->dtype = dtype;
     UMAPB_CUDA(cudaGetDevice(&st->device));
-    UMAPB_CUDA(cudaStreamCreateWithFlags(&st->stream, cudaStreamNonBlocking));
-    UMAPB_CUDA(cudaMalloc(reinterpret_cast<void**>(&st->d_status), sizeof(int)));
-    UMAPB_CUDA(cudaMemset(st->d_status, 0, sizeof(int)));
+    st->stream = stream_get();
+    st->d_status = static_cast<int*>(ws_alloc(sizeof(int), st->stream));
+    UMAPB_CUDA(cudaMemsetAsync(st->d_status, 0, sizeof(int), st->stream));
     st->n = n;
     st->num_dim = num_dim;
     st->opt = *opt;
@@ -273,7 +271,7 @@ void init_from_neighbors(umapb_status* st, const int64_t* row_ptr, const int32_t
     int64_t nnz = 0;
     if (is_device_pointer(row_ptr)) {
         UMAPB_CUDA(cudaMemcpyAsync(&nnz, row_ptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-        UMAPB_CUDA(cudaStreamSynchronize(s));
+        UMAPB_SYNC(s);
     } else {
         nnz = row_ptr[n];
     }
@@ -313,6 +311,112 @@ void init_from_data(umapb_status* st, size_t data_dim, const void* data, void* e
     st->impl = std::move(impl);
 }
 
+// Rows [start, start + len) of a CSR graph as a graph of their own (indices shifted by -start).
+__global__ void sub_csr_kernel(int32_t start, int32_t len, const int64_t* __restrict__ ptr,
+                               const int32_t* __restrict__ idx, int64_t* __restrict__ sub_ptr,
+                               int32_t* __restrict__ sub_idx) {
+    const int64_t base = ptr[start];
+    const int64_t nnz = ptr[start + len] - base;
+    for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t <= len; t += int64_t(gridDim.x) * blockDim.x)
+        sub_ptr[t] = ptr[start + t] - base;
+    for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < nnz; t += int64_t(gridDim.x) * blockDim.x)
+        sub_idx[t] = idx[base + t] - start;
+}
+
+// Batched pipeline (umapb_batch_run): the stages of init_from_data + run over
+// all instances at once, instance boundaries carried by 'inst'.
+template <typename T>
+void batch_pipeline(const std::vector<int32_t>& inst, size_t data_dim, const void* data, size_t num_dim,
+                    void* embedding, const umapb_options& o, float* stage_ms) {
+    Context& ctx = thread_context();
+    cudaStream_t s = ctx.stream;
+    const int ninst = static_cast<int>(inst.size()) - 1;
+    const int32_t n = inst[ninst];
+    const int k = o.num_neighbors;
+    require(k >= 1, "num_neighbors must be positive");
+    require(data_dim >= 1 && data_dim <= INT32_MAX, "data_dim must be positive");
+    int epochs = -1;
+    for (int i = 0; i < ninst; ++i) {
+        require(inst[i + 1] - inst[i] > k, "every instance needs more than num_neighbors observations");
+        const int e = choose_num_epochs(o.has_num_epochs != 0, o.num_epochs, inst[i + 1] - inst[i]);
+        require(epochs < 0 || e == epochs, "batched instances resolve to different epoch counts: set num_epochs");
+        epochs = e;
+    }
+    StageTimer tm(s, stage_ms);
+    DeviceIn<T> d(static_cast<const T*>(data), static_cast<size_t>(n) * data_dim, s);
+    DevArray<int32_t> d_inst(inst.size(), s);
+    UMAPB_CUDA(cudaMemcpyAsync(d_inst.get(), inst.data(), inst.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    const int64_t nnz = static_cast<int64_t>(n) * k;
+    DevArray<int32_t> idx(nnz, s);
+    DevArray<T> dist(nnz, s);
+    DevArray<int64_t> ptr(static_cast<size_t>(n) + 1, s);
+    tm.begin(ST_KNN);
+    knn_exact_batched<T>(d.get(), inst, static_cast<int32_t>(data_dim), k, idx.get(), dist.get(), s);
+    dense_row_ptr_kernel<<<grid_for(static_cast<size_t>(n) + 1, 256), 256, 0, s>>>(n, k, ptr.get());
+    UMAPB_LAUNCH_CHECK();
+    tm.end();
+
+    tm.begin(ST_SIM);
+    neighbor_similarities<T>(n, ptr.get(), dist.get(), o.local_connectivity, o.bandwidth, 1e-3, true, nullptr, nullptr, s);
+    tm.end();
+    tm.begin(ST_UNION);
+    DeviceCsr<T> g;
+    combine_neighbor_sets<T>(n, ptr.get(), idx.get(), dist.get(), nnz, o.mix_ratio, g, s);
+    tm.end();
+
+    // initial layouts, instance by instance (initialize.hpp:79-103)
+    tm.begin(ST_INIT);
+    DeviceInOut<T> Y(static_cast<T*>(embedding), static_cast<size_t>(n) * num_dim, s, /*load=*/true);
+    std::vector<int64_t> hptr(inst.size());
+    for (int i = 0; i <= ninst; ++i) {
+        UMAPB_CUDA(cudaMemcpyAsync(&hptr[i], g.ptr.get() + inst[i], sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    }
+    UMAPB_SYNC(s);
+    for (int i = 0; i < ninst; ++i) {
+        const int32_t start = inst[i], len = inst[i + 1] - inst[i];
+        T* Yi = Y.get() + static_cast<size_t>(start) * num_dim;
+        bool use_random = (o.initialize_method == UMAPB_INIT_RANDOM);
+        if (o.initialize_method == UMAPB_INIT_SPECTRAL) {
+            const int64_t sub_nnz = hptr[i + 1] - hptr[i];
+            DevArray<int64_t> sp(static_cast<size_t>(len) + 1, s);
+            DevArray<int32_t> si(std::max<int64_t>(sub_nnz, 1), s);
+            sub_csr_kernel<<<grid_for(std::max<int64_t>(sub_nnz, len + 1), 256), 256, 0, s>>>(start, len, g.ptr.get(),
+                                                                                            g.idx.get(), sp.get(),
+                                                                                            si.get());
+            UMAPB_LAUNCH_CHECK();
+            const SpectralResult r = spectral_init<T>(
+                len, sp.get(), si.get(), g.val.get() + hptr[i], static_cast<int>(num_dim), Yi, o.irlba_extra_work,
+                o.irlba_max_iterations, o.irlba_convergence_tolerance, o.initialize_spectral_scale,
+                o.initialize_spectral_jitter != 0, o.initialize_spectral_jitter_sd, o.initialize_seed, ctx.d_status, s);
+            use_random = (o.initialize_random_on_spectral_fail != 0 && !r.ok);
+        }
+        if (use_random) {
+            random_init<T>(len, static_cast<int>(num_dim), Yi, o.initialize_seed, o.initialize_random_scale, s);
+        }
+    }
+    tm.end();
+
+    double a = o.a, b = o.b;
+    if (!o.has_a || !o.has_b) find_ab(o.spread, o.min_dist, &a, &b);
+    tm.begin(ST_EPOCHS);
+    DeviceEpochs<T> ep;
+    similarities_to_epochs<T>(n, g.ptr.get(), g.idx.get(), g.val.get(), g.nnz, epochs, o.negative_sample_rate, ep, s,
+                              d_inst.get(), ninst);
+    SgdEngine<T> engine;
+    engine.setup(&ep, s);
+    engine.set_instances(d_inst.get(), ninst);
+    engine.use_graphs = true;
+    engine.autotune = true;
+    tm.end();
+    float ms_sched = 0, ms_sgd = 0;
+    engine.run(Y.get(), static_cast<int>(num_dim), 0, epochs, a, b, o.repulsion_strength, o.learning_rate,
+               o.optimize_seed, s, &ms_sched, &ms_sgd);
+    Y.finish();
+    tm.resolve();
+    stage_ms[ST_SCHEDULE] = ms_sched;
+    stage_ms[ST_SGD] = ms_sgd;
+}
+
 template <typename F>
 int guarded(F&& f) {
     try {
@@ -341,7 +445,7 @@ int64_t host_nnz(const int64_t* row_ptr, int32_t n, cudaStream_t s) {
     int64_t nnz = 0;
     if (is_device_pointer(row_ptr)) {
         UMAPB_CUDA(cudaMemcpyAsync(&nnz, row_ptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-        UMAPB_CUDA(cudaStreamSynchronize(s));
+        UMAPB_SYNC(s);
     } else {
         nnz = row_ptr[n];
     }
@@ -354,7 +458,7 @@ int64_t host_nnz(const int64_t* row_ptr, int32_t n, cudaStream_t s) {
 void check_device_status(Context& ctx) {
     int st = 0;
     UMAPB_CUDA(cudaMemcpyAsync(&st, ctx.d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
-    UMAPB_CUDA(cudaStreamSynchronize(ctx.stream));
+    UMAPB_SYNC(ctx.stream);
     if (st != DEV_OK) {
         UMAPB_CUDA(cudaMemsetAsync(ctx.d_status, 0, sizeof(int), ctx.stream));
         if (st == DEV_TIMEOUT) fail(UMAPB_ERR_DEVICE_TIMEOUT, "a bounded device wait gave up");
@@ -499,7 +603,7 @@ int umapb_knn(int dtype, size_t data_dim, int32_t num_obs, const void* data, int
             od.finish();
         }
         oi.finish();
-        UMAPB_CUDA(cudaStreamSynchronize(c.stream));
+        UMAPB_SYNC(c.stream);
     });
 }
 
@@ -528,7 +632,7 @@ int umapb_neighbor_similarities(int dtype, int32_t num_obs, const int64_t* row_p
         }
         rho.finish();
         sig.finish();
-        UMAPB_CUDA(cudaStreamSynchronize(c.stream));
+        UMAPB_SYNC(c.stream);
     });
 }
 
@@ -550,7 +654,7 @@ int umapb_combine_neighbor_sets(int dtype, int32_t num_obs, const int64_t* row_p
             copy_out(out_row_ptr, g.ptr.get(), sizeof(int64_t) * (static_cast<size_t>(num_obs) + 1), c.stream);
             copy_out(out_indices, g.idx.get(), sizeof(int32_t) * g.nnz, c.stream);
             copy_out(out_weights, g.val.get(), sizeof(T) * g.nnz, c.stream);
-            UMAPB_CUDA(cudaStreamSynchronize(c.stream));
+            UMAPB_SYNC(c.stream);
             if (out_nnz) *out_nnz = g.nnz;
         };
         if (dtype == UMAPB_F64) body(double{}); else body(float{});
@@ -578,7 +682,7 @@ int umapb_similarities_to_epochs(int dtype, int32_t num_obs, const int64_t* row_
             copy_out(eps, ep.eps.get(), sizeof(T) * ep.nnz, c.stream);
             copy_out(enext, ep.enext0.get(), sizeof(T) * ep.nnz, c.stream);
             copy_out(enneg, ep.enneg0.get(), sizeof(T) * ep.nnz, c.stream);
-            UMAPB_CUDA(cudaStreamSynchronize(c.stream));
+            UMAPB_SYNC(c.stream);
             if (out_nnz) *out_nnz = ep.nnz;
         };
         if (dtype == UMAPB_F64) body(double{}); else body(float{});
@@ -616,7 +720,7 @@ int umapb_spectral_init(int dtype, int32_t num_obs, const int64_t* row_ptr, cons
                                                       Y.get(), extra_work, max_iterations, tolerance, scale,
                                                       jitter != 0, jitter_sd, seed, c.d_status, c.stream);
             if (r.ok) Y.finish();
-            UMAPB_CUDA(cudaStreamSynchronize(c.stream));
+            UMAPB_SYNC(c.stream);
             if (ok) *ok = r.ok ? 1 : 0;
             if (evals_out) for (size_t d = 0; d <= num_dim && d < 64; ++d) evals_out[d] = r.evals[d];
         };
@@ -633,7 +737,7 @@ int umapb_random_init(int dtype, int32_t num_obs, size_t num_dim, void* embeddin
             DeviceInOut<T> Y(static_cast<T*>(embedding), static_cast<size_t>(num_obs) * num_dim, c.stream, false);
             random_init<T>(num_obs, static_cast<int>(num_dim), Y.get(), seed, scale, c.stream);
             Y.finish();
-            UMAPB_CUDA(cudaStreamSynchronize(c.stream));
+            UMAPB_SYNC(c.stream);
         };
         if (dtype == UMAPB_F64) body(double{}); else body(float{});
     });
@@ -683,7 +787,7 @@ int umapb_optimize_layout(int dtype, size_t num_dim, void* embedding, int32_t nu
             // heads from the row pointers
             std::vector<int64_t> hp(static_cast<size_t>(num_obs) + 1);
             UMAPB_CUDA(cudaMemcpyAsync(hp.data(), ep.ptr.get(), sizeof(int64_t) * (num_obs + 1), cudaMemcpyDeviceToHost, c.stream));
-            UMAPB_CUDA(cudaStreamSynchronize(c.stream));
+            UMAPB_SYNC(c.stream);
             std::vector<int32_t> heads(nnz);
             for (int32_t i = 0; i < num_obs; ++i)
                 for (int64_t q = hp[i]; q < hp[i + 1]; ++q) heads[q] = i;
@@ -703,9 +807,33 @@ int umapb_optimize_layout(int dtype, size_t num_dim, void* embedding, int32_t nu
                 copy_out(epoch_of_next_negative_sample, enn.get(), sizeof(T) * nnz, c.stream);
                 *current_epoch = epoch_limit;
             }
-            UMAPB_CUDA(cudaStreamSynchronize(c.stream));
+            UMAPB_SYNC(c.stream);
         };
         if (dtype == UMAPB_F64) body(double{}); else body(float{});
+    });
+}
+
+int umapb_batch_run(int dtype, int32_t num_instances, const int32_t* sizes, size_t data_dim, const void* data,
+                    size_t num_dim, void* embedding, const umapb_options* opt, double* stage_ms) {
+    return guarded([&] {
+        require_device();
+        require(dtype == UMAPB_F32 || dtype == UMAPB_F64, "dtype must be UMAPB_F32 or UMAPB_F64");
+        require(opt != nullptr && sizes != nullptr, "options and sizes must not be NULL");
+        require(num_instances >= 1, "at least one instance is needed");
+        require(num_dim >= 1 && num_dim <= 64, "num_dim must be between 1 and 64");
+        std::vector<int32_t> inst(static_cast<size_t>(num_instances) + 1, 0);
+        for (int i = 0; i < num_instances; ++i) {
+            require(sizes[i] >= 2, "every instance needs at least two observations");
+            require(static_cast<int64_t>(inst[i]) + sizes[i] <= INT32_MAX, "too many observations", UMAPB_ERR_OVERFLOW);
+            inst[i + 1] = inst[i] + sizes[i];
+        }
+        float ms[7] = {0, 0, 0, 0, 0, 0, 0};
+        if (dtype == UMAPB_F64) {
+            batch_pipeline<double>(inst, data_dim, data, num_dim, embedding, *opt, ms);
+        } else {
+            batch_pipeline<float>(inst, data_dim, data, num_dim, embedding, *opt, ms);
+        }
+        if (stage_ms) for (int i = 0; i < 7; ++i) stage_ms[i] = ms[i];
     });
 }
 
@@ -727,7 +855,7 @@ int umapb_loss_grad(int dtype, size_t num_dim, const void* embedding, int32_t nu
             loss_grad<T>(num_obs, static_cast<int>(num_dim), Y.get(), p.get(), ix.get(), w.get(), a, b, eps_rep,
                          with_constant != 0, loss, grad_embedding ? g.get() : nullptr, grad_ab, c.stream);
             g.finish();
-            UMAPB_CUDA(cudaStreamSynchronize(c.stream));
+            UMAPB_SYNC(c.stream);
         };
         if (dtype == UMAPB_F64) body(double{}); else body(float{});
     });

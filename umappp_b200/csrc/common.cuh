@@ -7,7 +7,10 @@
 #include <math_constants.h>
 
 #include <atomic>
+#include <chrono>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -35,10 +38,37 @@ struct Error : public std::runtime_error {
     throw Error(code, std::string(cudaGetErrorString(e)) + " in " + what + " (" + file + ":" + std::to_string(line) + ")");
 }
 
+// ---------------------------------------------------------------- tracing ---
+// UMAPB_TRACE=1 reports to stderr every runtime call of this library that
+// holds the host for longer than a millisecond (synchronisations, allocations,
+// copies), with its source line, so that stalls between kernels can be
+// attributed.
+
+inline bool trace_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("UMAPB_TRACE");
+        return e && *e && *e != '0';
+    }();
+    return on;
+}
+
+inline double host_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+inline void trace_wait(const char* what, double t0, size_t bytes, const char* file, int line) {
+    const double dt = host_ms() - t0;
+    if (dt <= 1.0) return;
+    if (bytes) std::fprintf(stderr, "[umapb] %s of %.0f MB took %.1f ms (%s:%d)\n", what, bytes / 1e6, dt, file, line);
+    else std::fprintf(stderr, "[umapb] %s took %.1f ms (%s:%d)\n", what, dt, file, line);
+}
+
 #define UMAPB_CUDA(call)                                                           \
     do {                                                                           \
+        const double umapb_t0_ = ::umapb::trace_enabled() ? ::umapb::host_ms() : 0.0; \
         cudaError_t umapb_e_ = (call);                                             \
         if (umapb_e_ != cudaSuccess) ::umapb::cuda_fail(umapb_e_, #call, __FILE__, __LINE__); \
+        if (::umapb::trace_enabled()) ::umapb::trace_wait(#call, umapb_t0_, 0, __FILE__, __LINE__); \
     } while (0)
 
 // Every kernel launch of this library is followed by this check, which also
@@ -53,13 +83,32 @@ inline void require(bool cond, const std::string& msg, int code = UMAPB_ERR_INVA
     if (!cond) fail(code, msg);
 }
 
+inline void stream_sync(cudaStream_t s, const char* file, int line) {
+    const double t0 = trace_enabled() ? host_ms() : 0.0;
+    const cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) cuda_fail(e, "cudaStreamSynchronize", file, line);
+    if (trace_enabled()) trace_wait("stream synchronise", t0, 0, file, line);
+}
+#define UMAPB_SYNC(stream) ::umapb::stream_sync((stream), __FILE__, __LINE__)
+
 // Device-side error word values (written by kernels with bounded waits).
 enum DeviceStatus : int { DEV_OK = 0, DEV_TIMEOUT = 1, DEV_BAD_INPUT = 2 };
 
 // ------------------------------------------------------- device buffers ---
 
-// Stream-ordered device allocation (cudaMallocAsync pool); freed on the same
-// stream when the owner goes away.
+// Workspace cache (memory.cu): stream-ordered device blocks that are kept
+// and reused instead of being returned to the runtime; event and stream pools.
+void* ws_alloc(size_t bytes, cudaStream_t s);
+void ws_free(void* p, cudaStream_t s);
+size_t ws_cached_bytes();
+void ws_release_cached();
+cudaEvent_t event_get();          // timing event from the pool
+void event_put(cudaEvent_t e);
+cudaStream_t stream_get();        // non-blocking stream of the current device
+void stream_put(cudaStream_t s);  // s must be idle
+
+// Stream-ordered device allocation from the workspace cache; released on the
+// stream it was allocated on when the owner goes away.
 template <typename T>
 class DevArray {
 public:
@@ -83,11 +132,15 @@ public:
         n_ = n;
         if (n > 0) {
             if (n > SIZE_MAX / sizeof(T)) fail(UMAPB_ERR_OVERFLOW, "device allocation size overflows");
-            UMAPB_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&ptr_), n * sizeof(T), s));
+            ptr_ = static_cast<T*>(ws_alloc(n * sizeof(T), s));
         }
     }
+    // Grows to at least n elements (contents are not kept); never shrinks.
+    void reserve(size_t n, cudaStream_t s) {
+        if (n > n_) allocate(n, s);
+    }
     void release() {
-        if (ptr_) cudaFreeAsync(ptr_, stream_);
+        if (ptr_) ws_free(ptr_, stream_);
         ptr_ = nullptr;
         n_ = 0;
     }

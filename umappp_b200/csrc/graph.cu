@@ -166,7 +166,7 @@ void combine_neighbor_sets(int32_t n, const int64_t* ptr, const int32_t* idx, co
     UMAPB_CUDA(cudaMemcpyAsync(&last_pos, pos.get() + (m - 1), sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     UMAPB_CUDA(cudaMemcpyAsync(&last_keep, keep.get() + (m - 1), sizeof(int), cudaMemcpyDeviceToHost, s));
     UMAPB_CUDA(cudaMemcpyAsync(&st, status.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
-    UMAPB_CUDA(cudaStreamSynchronize(s));
+    UMAPB_SYNC(s);
     require(st == DEV_OK, "neighbour list has an out-of-range index, a self edge or a duplicate neighbour");
     const int64_t nnz = last_pos + last_keep;
 
@@ -188,11 +188,26 @@ struct MaxOp {
     __device__ __forceinline__ T operator()(const T& a, const T& b) const { return (a < b) ? b : a; }   // std::max
 };
 
+// The maximum weight that applies to row i: one value, or (batched runs) the
+// maximum of row i's instance, instance j owning rows [inst[j], inst[j + 1]).
+template <typename T>
+__device__ __forceinline__ T row_max(int32_t i, const T* __restrict__ maxed, const int32_t* __restrict__ inst,
+                                     int num_inst) {
+    if (num_inst <= 1) return maxed[0];
+    int lo = 0, hi = num_inst - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (inst[mid] <= i) lo = mid; else hi = mid - 1;
+    }
+    return maxed[lo];
+}
+
 template <typename T>
 __global__ void epochs_count_kernel(int32_t n, const int64_t* __restrict__ ptr, const T* __restrict__ w,
-                                    const T* __restrict__ maxed, int num_epochs, int64_t* __restrict__ counts) {
+                                    const T* __restrict__ maxed, const int32_t* __restrict__ inst, int num_inst,
+                                    int num_epochs, int64_t* __restrict__ counts) {
     for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const T limit = *maxed / static_cast<T>(num_epochs);      // :63
+        const T limit = row_max(i, maxed, inst, num_inst) / static_cast<T>(num_epochs);      // :63
         int64_t c = 0;
         for (int64_t p = ptr[i]; p < ptr[i + 1]; ++p) c += (w[p] >= limit);
         counts[i] = c;
@@ -201,12 +216,13 @@ __global__ void epochs_count_kernel(int32_t n, const int64_t* __restrict__ ptr, 
 
 template <typename T>
 __global__ void epochs_fill_kernel(int32_t n, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                                   const T* __restrict__ w, const T* __restrict__ maxed, int num_epochs, T rate,
+                                   const T* __restrict__ w, const T* __restrict__ maxed,
+                                   const int32_t* __restrict__ inst, int num_inst, int num_epochs, T rate,
                                    const int64_t* __restrict__ out_ptr, int32_t* __restrict__ heads,
                                    int32_t* __restrict__ targets, T* __restrict__ eps, T* __restrict__ enext,
                                    T* __restrict__ enneg) {
     for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const T mx = *maxed;
+        const T mx = row_max(i, maxed, inst, num_inst);
         const T limit = mx / static_cast<T>(num_epochs);
         int64_t q = out_ptr[i];
         for (int64_t p = ptr[i]; p < ptr[i + 1]; ++p) {
@@ -223,9 +239,45 @@ __global__ void epochs_fill_kernel(int32_t n, const int64_t* __restrict__ ptr, c
     }
 }
 
+// Per-instance maxima (weights are non-negative, so their bit patterns order like the values).
+template <typename T>
+struct Bits;
+template <>
+struct Bits<float> {
+    typedef unsigned int type;
+    static __device__ __forceinline__ unsigned int of(float v) { return __float_as_uint(v); }
+};
+template <>
+struct Bits<double> {
+    typedef unsigned long long type;
+    static __device__ __forceinline__ unsigned long long of(double v) {
+        return static_cast<unsigned long long>(__double_as_longlong(v));
+    }
+};
+
+template <typename T>
+__global__ void instance_max_kernel(int32_t n, const int64_t* __restrict__ ptr, const T* __restrict__ w,
+                                    const int32_t* __restrict__ inst, int num_inst,
+                                    typename Bits<T>::type* __restrict__ maxed_bits) {
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int lo = 0, hi = num_inst - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (inst[mid] <= i) lo = mid; else hi = mid - 1;
+        }
+        typename Bits<T>::type m = 0;
+        for (int64_t p = ptr[i]; p < ptr[i + 1]; ++p) {
+            const typename Bits<T>::type b = Bits<T>::of(w[p]);
+            m = (m < b) ? b : m;
+        }
+        if (m) atomicMax(&maxed_bits[lo], m);
+    }
+}
+
 template <typename T>
 void similarities_to_epochs(int32_t n, const int64_t* ptr, const int32_t* idx, const T* w, int64_t nnz, int num_epochs,
-                            double negative_sample_rate, DeviceEpochs<T>& out, cudaStream_t s) {
+                            double negative_sample_rate, DeviceEpochs<T>& out, cudaStream_t s,
+                            const int32_t* inst_start, int32_t num_inst) {
     require(num_epochs > 0, "num_epochs must be positive");
     // the reference checks that num_epochs * rate fits an int (optimize_layout.hpp:89)
     const double cap = static_cast<double>(static_cast<T>(num_epochs) * static_cast<T>(negative_sample_rate));
@@ -236,8 +288,16 @@ void similarities_to_epochs(int32_t n, const int64_t* ptr, const int32_t* idx, c
     out.negative_sample_rate = static_cast<T>(negative_sample_rate);
     out.ptr.allocate(static_cast<size_t>(n) + 1, s);
 
-    DevArray<T> maxed(1, s);
-    if (nnz > 0) {
+    const int ni = (inst_start && num_inst > 1) ? num_inst : 1;
+    DevArray<T> maxed(ni, s);
+    if (ni > 1) {
+        maxed.zero(s);
+        if (n > 0) {
+            instance_max_kernel<T><<<grid_for(n, 256), 256, 0, s>>>(
+                n, ptr, w, inst_start, ni, reinterpret_cast<typename Bits<T>::type*>(maxed.get()));
+            UMAPB_LAUNCH_CHECK();
+        }
+    } else if (nnz > 0) {
         size_t tb = 0;
         UMAPB_CUDA(cub::DeviceReduce::Reduce(nullptr, tb, w, maxed.get(), nnz, MaxOp<T>(), T(0), s));
         DevArray<unsigned char> temp(tb, s);
@@ -248,7 +308,8 @@ void similarities_to_epochs(int32_t n, const int64_t* ptr, const int32_t* idx, c
     DevArray<int64_t> counts(static_cast<size_t>(n) + 1, s);
     counts.zero(s);
     if (n > 0) {
-        epochs_count_kernel<T><<<grid_for(n, 256), 256, 0, s>>>(n, ptr, w, maxed.get(), num_epochs, counts.get());
+        epochs_count_kernel<T><<<grid_for(n, 256), 256, 0, s>>>(n, ptr, w, maxed.get(), inst_start, ni, num_epochs,
+                                                                counts.get());
         UMAPB_LAUNCH_CHECK();
     }
     {
@@ -259,7 +320,7 @@ void similarities_to_epochs(int32_t n, const int64_t* ptr, const int32_t* idx, c
     }
     int64_t kept = 0;
     UMAPB_CUDA(cudaMemcpyAsync(&kept, out.ptr.get() + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-    UMAPB_CUDA(cudaStreamSynchronize(s));
+    UMAPB_SYNC(s);
     out.nnz = kept;
     out.heads.allocate(kept, s);
     out.targets.allocate(kept, s);
@@ -267,7 +328,7 @@ void similarities_to_epochs(int32_t n, const int64_t* ptr, const int32_t* idx, c
     out.enext0.allocate(kept, s);
     out.enneg0.allocate(kept, s);
     if (n > 0 && kept > 0) {
-        epochs_fill_kernel<T><<<grid_for(n, 256), 256, 0, s>>>(n, ptr, idx, w, maxed.get(), num_epochs,
+        epochs_fill_kernel<T><<<grid_for(n, 256), 256, 0, s>>>(n, ptr, idx, w, maxed.get(), inst_start, ni, num_epochs,
                                                                static_cast<T>(negative_sample_rate), out.ptr.get(),
                                                                out.heads.get(), out.targets.get(), out.eps.get(),
                                                                out.enext0.get(), out.enneg0.get());
@@ -350,7 +411,7 @@ int64_t count_components(int32_t n, const int64_t* ptr, const int32_t* idx, int*
     int st = 0;
     UMAPB_CUDA(cudaMemcpyAsync(&h, count.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
     UMAPB_CUDA(cudaMemcpyAsync(&st, d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
-    UMAPB_CUDA(cudaStreamSynchronize(s));
+    UMAPB_SYNC(s);
     if (st == DEV_TIMEOUT) fail(UMAPB_ERR_DEVICE_TIMEOUT, "union-find hook loop hit its iteration cap");
     if (st == DEV_BAD_INPUT) fail(UMAPB_ERR_INVALID, "graph has an out-of-range neighbour index");
     return static_cast<int64_t>(h);
@@ -361,8 +422,8 @@ template void combine_neighbor_sets<float>(int32_t, const int64_t*, const int32_
 template void combine_neighbor_sets<double>(int32_t, const int64_t*, const int32_t*, const double*, int64_t, double,
                                             DeviceCsr<double>&, cudaStream_t);
 template void similarities_to_epochs<float>(int32_t, const int64_t*, const int32_t*, const float*, int64_t, int, double,
-                                            DeviceEpochs<float>&, cudaStream_t);
+                                            DeviceEpochs<float>&, cudaStream_t, const int32_t*, int32_t);
 template void similarities_to_epochs<double>(int32_t, const int64_t*, const int32_t*, const double*, int64_t, int,
-                                             double, DeviceEpochs<double>&, cudaStream_t);
+                                             double, DeviceEpochs<double>&, cudaStream_t, const int32_t*, int32_t);
 
 }  // namespace umapb

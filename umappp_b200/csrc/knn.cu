@@ -267,7 +267,7 @@ void run_f32(const float* data, int32_t n, int32_t dim, int32_t k, int32_t* out_
         knn_tc_candidates(data, n, dim, KCAP, ci.get(), cd.get(), norms.get(), err.get(), s);
         int h_err = 0;
         UMAPB_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
-        UMAPB_CUDA(cudaStreamSynchronize(s));
+        UMAPB_SYNC(s);
         if (h_err != DEV_OK) fail(UMAPB_ERR_DEVICE_TIMEOUT, "tensor-core kNN: a pipeline wait gave up");
         norm_max.zero(s);
         norm_max_kernel<<<grid_for(n, 256, 1024), 256, 0, s>>>(n, norms.get(), norm_max.get());
@@ -285,7 +285,7 @@ void run_f32(const float* data, int32_t n, int32_t dim, int32_t k, int32_t* out_
     UMAPB_LAUNCH_CHECK();
     int32_t nredo = 0;
     UMAPB_CUDA(cudaMemcpyAsync(&nredo, redo_count.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-    UMAPB_CUDA(cudaStreamSynchronize(s));
+    UMAPB_SYNC(s);
     last_knn_redo_count() = nredo;
     if (nredo > 0) {
         // exact FP64 search for the uncertain queries (same output rows)
@@ -299,7 +299,108 @@ void run_f32(const float* data, int32_t n, int32_t dim, int32_t k, int32_t* out_
     }
 }
 
+__global__ void row_norms_kernel(const float* __restrict__ data, int32_t n, int32_t dim, float* __restrict__ norms) {
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double s = 0;
+        for (int d = 0; d < dim; ++d) {
+            const double v = data[static_cast<size_t>(i) * dim + d];
+            s += v * v;
+        }
+        norms[i] = static_cast<float>(s);
+    }
+}
+
+__global__ void shift_indices_kernel(int32_t* __restrict__ idx, size_t count, int32_t delta) {
+    for (size_t t = blockIdx.x * size_t(blockDim.x) + threadIdx.x; t < count; t += size_t(gridDim.x) * blockDim.x)
+        idx[t] += delta;
+}
+
+// Batched tensor-core search with FP64 rescoring; instances holding uncertain
+// queries are recomputed whole by the per-instance search.
+template <int KCAP>
+void run_f32_batched(const float* data, const std::vector<int32_t>& inst, int32_t dim, int32_t k, int32_t* out_idx,
+                     float* out_dist, cudaStream_t s) {
+    const int ninst = static_cast<int>(inst.size()) - 1;
+    const int32_t n = inst[ninst];
+    DevArray<int32_t> ci(static_cast<size_t>(n) * KCAP, s);
+    DevArray<float> cd(static_cast<size_t>(n) * KCAP, s);
+    DevArray<int> err(1, s);
+    err.zero(s);
+    knn_tc_candidates_batched(data, inst, dim, KCAP, ci.get(), cd.get(), err.get(), s);
+    int h_err = 0;
+    UMAPB_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    UMAPB_SYNC(s);
+    if (h_err != DEV_OK) fail(UMAPB_ERR_DEVICE_TIMEOUT, "tensor-core kNN: a pipeline wait gave up");
+    DevArray<float> norms(n, s);
+    DevArray<unsigned int> norm_max(1, s);
+    norm_max.zero(s);
+    row_norms_kernel<<<grid_for(n, 256), 256, 0, s>>>(data, n, dim, norms.get());
+    UMAPB_LAUNCH_CHECK();
+    norm_max_kernel<<<grid_for(n, 256, 1024), 256, 0, s>>>(n, norms.get(), norm_max.get());
+    UMAPB_LAUNCH_CHECK();
+    DevArray<int32_t> redo(n, s), redo_count(1, s);
+    redo_count.zero(s);
+    knn_rescore_kernel<KCAP><<<(n + 127) / 128, 128, 0, s>>>(data, n, dim, k, ci.get(), cd.get(), out_idx, out_dist,
+                                                             nullptr, redo.get(), redo_count.get(), norms.get(),
+                                                             norm_max.get(), TC_REL_BOUND);
+    UMAPB_LAUNCH_CHECK();
+    int32_t nredo = 0;
+    UMAPB_CUDA(cudaMemcpyAsync(&nredo, redo_count.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    UMAPB_SYNC(s);
+    last_knn_redo_count() = nredo;
+    if (nredo > 0) {
+        std::vector<int32_t> rq(nredo);
+        UMAPB_CUDA(cudaMemcpyAsync(rq.data(), redo.get(), nredo * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        UMAPB_SYNC(s);
+        std::vector<char> mark(ninst, 0);
+        for (int32_t q : rq) mark[std::upper_bound(inst.begin(), inst.end(), q) - inst.begin() - 1] = 1;
+        for (int i = 0; i < ninst; ++i) {
+            if (!mark[i]) continue;
+            const int32_t start = inst[i], len = inst[i + 1] - inst[i];
+            run_f64<float, KCAP>(data + static_cast<size_t>(start) * dim, len, dim, k, nullptr, len,
+                                 out_idx + static_cast<size_t>(start) * k, out_dist + static_cast<size_t>(start) * k,
+                                 nullptr, s);
+            shift_indices_kernel<<<grid_for(static_cast<size_t>(len) * k, 256), 256, 0, s>>>(
+                out_idx + static_cast<size_t>(start) * k, static_cast<size_t>(len) * k, start);
+            UMAPB_LAUNCH_CHECK();
+        }
+    }
+}
+
 }  // namespace
+
+template <typename T>
+void knn_exact_batched(const T* data, const std::vector<int32_t>& inst, int32_t dim, int32_t k, int32_t* out_idx,
+                       T* out_dist, cudaStream_t s) {
+    const int ninst = static_cast<int>(inst.size()) - 1;
+    require(ninst >= 1, "at least one instance is needed");
+    require(k >= 1 && k <= 120, "num_neighbors must be in [1, 120] for the device search");
+    for (int i = 0; i < ninst; ++i) {
+        require(inst[i + 1] - inst[i] > k, "every instance needs more observations than num_neighbors");
+    }
+    if constexpr (std::is_same<T, float>::value) {
+        const int kcap = (k + 8 <= 16) ? 16 : (k + 8 <= 24) ? 24 : 32;
+        if (k + 8 <= 32 && use_tensor_cores() && knn_tc_supported(dim, kcap)) {
+            if (kcap == 16) run_f32_batched<16>(data, inst, dim, k, out_idx, out_dist, s);
+            else if (kcap == 24) run_f32_batched<24>(data, inst, dim, k, out_idx, out_dist, s);
+            else run_f32_batched<32>(data, inst, dim, k, out_idx, out_dist, s);
+            return;
+        }
+    }
+    for (int i = 0; i < ninst; ++i) {
+        const int32_t start = inst[i], len = inst[i + 1] - inst[i];
+        knn_exact<T>(data + static_cast<size_t>(start) * dim, len, dim, k, out_idx + static_cast<size_t>(start) * k,
+                     out_dist + static_cast<size_t>(start) * k, s);
+        shift_indices_kernel<<<grid_for(static_cast<size_t>(len) * k, 256), 256, 0, s>>>(
+            out_idx + static_cast<size_t>(start) * k, static_cast<size_t>(len) * k, start);
+        UMAPB_LAUNCH_CHECK();
+    }
+}
+
+template void knn_exact_batched<float>(const float*, const std::vector<int32_t>&, int32_t, int32_t, int32_t*, float*,
+                                       cudaStream_t);
+template void knn_exact_batched<double>(const double*, const std::vector<int32_t>&, int32_t, int32_t, int32_t*,
+                                        double*, cudaStream_t);
 
 template <typename T>
 void knn_exact(const T* data, int32_t n, int32_t dim, int32_t k, int32_t* out_idx, T* out_dist, cudaStream_t s,

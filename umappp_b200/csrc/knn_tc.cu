@@ -174,32 +174,36 @@ __device__ __forceinline__ void split_tf32(float a, float& hi, float& lo) {
     lo = __uint_as_float(l);
 }
 
+// pad_src (batched runs) maps operand row i to its data row, or -1 for a
+// padding row; without it, rows below n are data rows.
 __global__ void prepare_operands_kernel(const float* __restrict__ data, int32_t n, int32_t dim, int32_t n_pad,
                                         int32_t k_pad, float* __restrict__ a_hi, float* __restrict__ a_lo,
                                         float* __restrict__ b_hi, float* __restrict__ b_lo,
-                                        float* __restrict__ norms) {
+                                        float* __restrict__ norms, const int32_t* __restrict__ pad_src) {
     for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n_pad; i += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t src = pad_src ? pad_src[i] : (i < n ? i : -1);
+        const bool real = src >= 0;
         double s = 0;
-        if (i < n) {
+        if (real) {
             for (int d = 0; d < dim; ++d) {
-                const double v = data[i * dim + d];
+                const double v = data[src * dim + d];
                 s += v * v;
             }
         }
-        norms[i] = (i < n) ? static_cast<float>(s) : CUDART_INF_F;
+        norms[i] = real ? static_cast<float>(s) : CUDART_INF_F;
         const int64_t row = i * k_pad;
         for (int d = 0; d < k_pad; ++d) {
             float v = 0.0f;
-            if (i < n && d < dim) v = data[i * dim + d];
+            if (real && d < dim) v = data[src * dim + d];
             float h, l;
             split_tf32(v, h, l);
             a_hi[row + d] = h;
             a_lo[row + d] = l;
             if (d == dim) {
                 // the norm column: 1 for queries, -|r|^2 / 2 for references
-                a_hi[row + d] = (i < n) ? 1.0f : 0.0f;
+                a_hi[row + d] = real ? 1.0f : 0.0f;
                 a_lo[row + d] = 0.0f;
-                if (i < n) {
+                if (real) {
                     split_tf32(static_cast<float>(-0.5 * s), h, l);
                 } else {
                     h = -1e30f;
@@ -251,13 +255,34 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_tc_kernel(const __grid_cons
                                                                const __grid_constant__ CUtensorMap map_bhi,
                                                                const __grid_constant__ CUtensorMap map_blo,
                                                                const float* __restrict__ norms, int32_t n,
-                                                               int32_t n_tiles, int32_t* __restrict__ cand_idx,
-                                                               float* __restrict__ cand_d2, int* __restrict__ err) {
+                                                               int32_t n_tiles_all, int32_t ksteps,
+                                                               int32_t* __restrict__ cand_idx,
+                                                               float* __restrict__ cand_d2, int* __restrict__ err,
+                                                               const int4* __restrict__ tasks,
+                                                               const int32_t* __restrict__ shifts) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // the dynamic window is only guaranteed 16-byte aligned: round up to 1024
     TcSmem<KC>& sm = *reinterpret_cast<TcSmem<KC>*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int q_base = blockIdx.x * TC_M;
+    // This CTA's queries are operand rows [q_base, q_base + 128), valid below
+    // q_limit; its references are the n_tiles tiles from ref_tile0.  Batched
+    // runs give each CTA a task (one instance's query tile against that
+    // instance's reference tiles) and the shift from operand rows to data rows.
+    int q_base, ref_tile0, n_tiles, q_limit, shift;
+    if (tasks) {
+        const int4 t = tasks[blockIdx.x];
+        q_base = t.x;
+        ref_tile0 = t.y;
+        n_tiles = t.z;
+        q_limit = t.w;
+        shift = shifts[blockIdx.x];
+    } else {
+        q_base = blockIdx.x * TC_M;
+        ref_tile0 = 0;
+        n_tiles = n_tiles_all;
+        q_limit = n;
+        shift = 0;
+    }
     volatile int* abort_flag = &sm.abort_flag;
 
     if (threadIdx.x == 0) {
@@ -301,8 +326,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_tc_kernel(const __grid_cons
                 if (!mbar_wait(&sm.empty[s], (round & 1) ^ 1, abort_flag, err)) break;
                 mbar_arrive_expect_tx(&sm.full[s], B_BYTES);
                 for (int c = 0; c < KC; ++c) {
-                    tma_load_2d(sm.b_hi[s][c], &map_bhi, &sm.full[s], c * TC_KCHUNK, it * TC_N);
-                    tma_load_2d(sm.b_lo[s][c], &map_blo, &sm.full[s], c * TC_KCHUNK, it * TC_N);
+                    tma_load_2d(sm.b_hi[s][c], &map_bhi, &sm.full[s], c * TC_KCHUNK, (ref_tile0 + it) * TC_N);
+                    tma_load_2d(sm.b_lo[s][c], &map_blo, &sm.full[s], c * TC_KCHUNK, (ref_tile0 + it) * TC_N);
                 }
                 ++issued;
             }
@@ -322,6 +347,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_tc_kernel(const __grid_cons
                     for (int c = 0; c < KC; ++c) {
 #pragma unroll
                         for (int kk = 0; kk < TC_KCHUNK / 8; ++kk) {
+                            // K-steps past the last non-zero column (data + norm) contribute nothing
+                            if (c * (TC_KCHUNK / 8) + kk >= ksteps) break;
                             const int off = kk * 8;   // 8 TF32 = 32 bytes along K inside the swizzle row
                             const uint64_t ah = smem_desc(sm.a_hi[c] + off), al = smem_desc(sm.a_lo[c] + off);
                             const uint64_t bh = smem_desc(sm.b_hi[s][c] + off), bl = smem_desc(sm.b_lo[s][c] + off);
@@ -341,7 +368,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_tc_kernel(const __grid_cons
         const int quarter = warp & 3;
         const int row = quarter * 32 + lane;
         const int q = q_base + row;
-        const float qn = (q < n) ? norms[q] : 0.0f;
+        const float qn = (q < q_limit) ? norms[q] : 0.0f;
         float bd[KCAP];
         int bi[KCAP];
 #pragma unroll
@@ -355,7 +382,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_tc_kernel(const __grid_cons
             if (!mbar_wait(&sm.tmem_full[buf], (it >> 1) & 1, abort_flag, err)) break;
             tc_fence_after();
             const uint32_t taddr = tmem_base + (uint32_t(quarter * 32) << 16) + buf * TC_N;
-            const bool diag = (it == static_cast<int>(blockIdx.x));
+            const bool diag = ((ref_tile0 + it) * TC_N == q_base);
+            // reference columns at or past q_limit are padding (their distances
+            // are finite, so they are masked out rather than left to lose)
+            const int valid = q_limit - (ref_tile0 + it) * TC_N;
 #pragma unroll 1
             for (int ch = 0; ch < TC_N / 32; ++ch) {
                 uint32_t r[32];
@@ -368,12 +398,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_tc_kernel(const __grid_cons
                     mask |= (d2[i] < thr ? 1u : 0u) << i;
                 }
                 if (diag && ch == (row >> 5)) mask &= ~(1u << (row & 31));   // self
+                const int vc = valid - ch * 32;
+                if (vc < 32) mask &= (vc <= 0) ? 0u : ((1u << vc) - 1u);
                 while (mask) {   // rare: candidates better than the current k-th
                     const int i = __ffs(mask) - 1;
                     mask &= mask - 1;
                     const float v = select32(d2, i);
                     if (v < thr) {
-                        insert_sorted<KCAP>(bd, bi, v, it * TC_N + ch * 32 + i);
+                        insert_sorted<KCAP>(bd, bi, v, (ref_tile0 + it) * TC_N + ch * 32 + i + shift);
                         thr = bd[KCAP - 1];
                     }
                 }
@@ -381,11 +413,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_tc_kernel(const __grid_cons
             tc_fence_before();
             mbar_arrive(&sm.tmem_empty[buf]);
         }
-        if (q < n) {
+        if (q < q_limit) {
+            const size_t out_row = static_cast<size_t>(q + shift);   // data row of this query
 #pragma unroll
             for (int i = 0; i < KCAP; ++i) {
-                cand_idx[static_cast<size_t>(q) * KCAP + i] = bi[i];
-                cand_d2[static_cast<size_t>(q) * KCAP + i] = bd[i];
+                cand_idx[out_row * KCAP + i] = bi[i];
+                cand_d2[out_row * KCAP + i] = bd[i];
             }
         }
     }
@@ -439,11 +472,13 @@ CUtensorMap make_map(const float* base, int64_t rows, int k_pad) {
 
 struct Maps {
     CUtensorMap ahi, alo, bhi, blo;
+    int ksteps;   // MMA K-steps of 8 columns that hold data or the norm column
 };
 
+// One launch: 'ctas' CTAs; with tasks, CTA b runs tasks[b] (see the kernel).
 template <int KC, int KCAP>
-void launch_tc(const Maps& m, const float* norms, int32_t n, int32_t n_pad, int32_t* cand_idx, float* cand_d2, int* err,
-               cudaStream_t s) {
+void launch_tc(const Maps& m, const float* norms, int32_t n, int32_t n_pad, int32_t ctas, const int4* tasks,
+               const int32_t* shifts, int32_t* cand_idx, float* cand_d2, int* err, cudaStream_t s) {
     const size_t smem = sizeof(TcSmem<KC>) + 1024;
     static bool configured = false;
     if (!configured) {
@@ -452,17 +487,41 @@ void launch_tc(const Maps& m, const float* norms, int32_t n, int32_t n_pad, int3
         configured = true;
     }
     const int n_tiles = n_pad / TC_N;
-    knn_tc_kernel<KC, KCAP><<<n_pad / TC_M, TC_THREADS, smem, s>>>(m.ahi, m.alo, m.bhi, m.blo, norms, n, n_tiles,
-                                                                   cand_idx, cand_d2, err);
+    knn_tc_kernel<KC, KCAP><<<ctas, TC_THREADS, smem, s>>>(m.ahi, m.alo, m.bhi, m.blo, norms, n, n_tiles, m.ksteps,
+                                                           cand_idx, cand_d2, err, tasks, shifts);
     UMAPB_LAUNCH_CHECK();
 }
 
 template <int KC>
-void launch_kcap(int kcap, const Maps& m, const float* norms, int32_t n, int32_t n_pad, int32_t* cand_idx,
-                 float* cand_d2, int* err, cudaStream_t s) {
-    if (kcap == 16) launch_tc<KC, 16>(m, norms, n, n_pad, cand_idx, cand_d2, err, s);
-    else if (kcap == 24) launch_tc<KC, 24>(m, norms, n, n_pad, cand_idx, cand_d2, err, s);
-    else launch_tc<KC, 32>(m, norms, n, n_pad, cand_idx, cand_d2, err, s);
+void launch_kcap(int kcap, const Maps& m, const float* norms, int32_t n, int32_t n_pad, int32_t ctas,
+                 const int4* tasks, const int32_t* shifts, int32_t* cand_idx, float* cand_d2, int* err,
+                 cudaStream_t s) {
+    if (kcap == 16) launch_tc<KC, 16>(m, norms, n, n_pad, ctas, tasks, shifts, cand_idx, cand_d2, err, s);
+    else if (kcap == 24) launch_tc<KC, 24>(m, norms, n, n_pad, ctas, tasks, shifts, cand_idx, cand_d2, err, s);
+    else launch_tc<KC, 32>(m, norms, n, n_pad, ctas, tasks, shifts, cand_idx, cand_d2, err, s);
+}
+
+// Shared body: operands over n_pad rows (pad_src maps rows to data rows in
+// batched runs), then one launch over 'ctas' CTAs.
+void run_candidates(const float* data, int32_t n, int32_t dim, int kcap, int32_t n_pad, const int32_t* pad_src,
+                    int32_t ctas, const int4* tasks, const int32_t* shifts, int32_t* cand_idx, float* cand_d2,
+                    float* norms_pad, int* d_err, cudaStream_t s) {
+    const int kc = (dim + 1 + TC_KCHUNK - 1) / TC_KCHUNK;
+    const int k_pad = kc * TC_KCHUNK;
+    const size_t elems = static_cast<size_t>(n_pad) * k_pad;
+    DevArray<float> ahi(elems, s), alo(elems, s), bhi(elems, s), blo(elems, s);
+    prepare_operands_kernel<<<grid_for(n_pad, 256), 256, 0, s>>>(data, n, dim, n_pad, k_pad, ahi.get(), alo.get(),
+                                                                  bhi.get(), blo.get(), norms_pad, pad_src);
+    UMAPB_LAUNCH_CHECK();
+    Maps m;
+    m.ahi = make_map(ahi.get(), n_pad, k_pad);
+    m.alo = make_map(alo.get(), n_pad, k_pad);
+    m.bhi = make_map(bhi.get(), n_pad, k_pad);
+    m.blo = make_map(blo.get(), n_pad, k_pad);
+    m.ksteps = (dim + 1 + 7) / 8;
+    if (kc == 1) launch_kcap<1>(kcap, m, norms_pad, n, n_pad, ctas, tasks, shifts, cand_idx, cand_d2, d_err, s);
+    else launch_kcap<2>(kcap, m, norms_pad, n, n_pad, ctas, tasks, shifts, cand_idx, cand_d2, d_err, s);
+    // the operand arrays are released stream-ordered, after the kernel
 }
 
 }  // namespace
@@ -478,22 +537,47 @@ bool knn_tc_supported(int32_t dim, int kcap) {
 void knn_tc_candidates(const float* data, int32_t n, int32_t dim, int kcap, int32_t* cand_idx, float* cand_d2,
                        float* norms_out, int* d_err, cudaStream_t s) {
     require(knn_tc_supported(dim, kcap), "tensor-core kNN: unsupported dimension or candidate count");
-    const int kc = (dim + 1 + TC_KCHUNK - 1) / TC_KCHUNK;
-    const int k_pad = kc * TC_KCHUNK;
     const int32_t n_pad = ((n + TC_M - 1) / TC_M) * TC_M;
-    const size_t elems = static_cast<size_t>(n_pad) * k_pad;
-    DevArray<float> ahi(elems, s), alo(elems, s), bhi(elems, s), blo(elems, s);
-    prepare_operands_kernel<<<grid_for(n_pad, 256), 256, 0, s>>>(data, n, dim, n_pad, k_pad, ahi.get(), alo.get(),
-                                                                  bhi.get(), blo.get(), norms_out);
-    UMAPB_LAUNCH_CHECK();
-    Maps m;
-    m.ahi = make_map(ahi.get(), n_pad, k_pad);
-    m.alo = make_map(alo.get(), n_pad, k_pad);
-    m.bhi = make_map(bhi.get(), n_pad, k_pad);
-    m.blo = make_map(blo.get(), n_pad, k_pad);
-    if (kc == 1) launch_kcap<1>(kcap, m, norms_out, n, n_pad, cand_idx, cand_d2, d_err, s);
-    else launch_kcap<2>(kcap, m, norms_out, n, n_pad, cand_idx, cand_d2, d_err, s);
-    // the operand arrays are released stream-ordered, after the kernel
+    run_candidates(data, n, dim, kcap, n_pad, nullptr, n_pad / TC_M, nullptr, nullptr, cand_idx, cand_d2, norms_out,
+                   d_err, s);
+}
+
+// Batched: instance i is data rows [inst[i], inst[i + 1]); every query's
+// candidates come from its own instance only.  Each instance is placed at a
+// 128-row boundary of the operands, so a CTA's query tile and reference tiles
+// all belong to one instance.  Candidate indices are data rows.
+void knn_tc_candidates_batched(const float* data, const std::vector<int32_t>& inst, int32_t dim, int kcap,
+                               int32_t* cand_idx, float* cand_d2, int* d_err, cudaStream_t s) {
+    require(knn_tc_supported(dim, kcap), "tensor-core kNN: unsupported dimension or candidate count");
+    const int ninst = static_cast<int>(inst.size()) - 1;
+    std::vector<int32_t> pad_start(ninst + 1, 0);
+    for (int i = 0; i < ninst; ++i) {
+        const int32_t len = inst[i + 1] - inst[i];
+        pad_start[i + 1] = pad_start[i] + ((len + TC_M - 1) / TC_M) * TC_M;
+    }
+    const int32_t n_pad = std::max(pad_start[ninst], TC_M);
+    std::vector<int32_t> src(n_pad, -1);
+    std::vector<int4> tasks;
+    std::vector<int32_t> shifts;
+    for (int i = 0; i < ninst; ++i) {
+        const int32_t len = inst[i + 1] - inst[i];
+        for (int32_t r = 0; r < len; ++r) src[pad_start[i] + r] = inst[i] + r;
+        const int32_t tiles = (len + TC_M - 1) / TC_M;
+        for (int32_t t = 0; t < tiles; ++t) {
+            tasks.push_back(make_int4(pad_start[i] + t * TC_M, pad_start[i] / TC_N, tiles, pad_start[i] + len));
+            shifts.push_back(inst[i] - pad_start[i]);
+        }
+    }
+    if (tasks.empty()) return;
+    DevArray<int32_t> d_src(src.size(), s), d_shift(shifts.size(), s);
+    DevArray<int4> d_tasks(tasks.size(), s);
+    DevArray<float> norms(n_pad, s);
+    UMAPB_CUDA(cudaMemcpyAsync(d_src.get(), src.data(), src.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    UMAPB_CUDA(cudaMemcpyAsync(d_tasks.get(), tasks.data(), tasks.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
+    UMAPB_CUDA(cudaMemcpyAsync(d_shift.get(), shifts.data(), shifts.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    run_candidates(data, inst[ninst], dim, kcap, n_pad, d_src.get(), static_cast<int32_t>(tasks.size()), d_tasks.get(),
+                   d_shift.get(), cand_idx, cand_d2, norms.get(), d_err, s);
+    UMAPB_SYNC(s);   // the host vectors above are the copies' sources
 }
 
 }  // namespace umapb

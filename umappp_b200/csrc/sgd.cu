@@ -23,6 +23,9 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <cstdlib>
+#include <map>
+#include <mutex>
 #include <type_traits>
 #include <vector>
 
@@ -34,6 +37,13 @@ namespace {
 
 constexpr int SCHED_BLOCK = 256;
 constexpr int MAX_WINDOW = 512;
+// Default cap on a window's event buffers (events, negative counts, segment
+// starts).  Windows of about a gigabyte keep the schedule's footprint small
+// next to the data and let the buffers be reused from window to window; one
+// buffer for a whole million-point run would be ~26 GB, and allocating that
+// afresh (and fragmenting the stream-ordered pool with it) costs more than
+// the extra count passes of smaller windows.
+constexpr size_t WINDOW_BYTES = size_t(1) << 30;
 constexpr int MAX_GENERIC_DIM = 64;
 
 template <typename T>
@@ -186,7 +196,40 @@ struct SgdParams {
     uint32_t k0, k1;
     uint32_t epoch;
     int32_t n;
+    // Independent instances laid out one after another (batched runs):
+    // instance i owns observations [inst_start[i], inst_start[i + 1]) and
+    // draws its negative samples there.  num_inst <= 1: one instance of n.
+    const int32_t* inst_start;
+    int32_t num_inst;
+    // Phases: an epoch runs as num_phases launches; launch 'phase' processes
+    // the heads in the phase-th of num_phases equal slices of each instance.
+    int32_t phase, num_phases;
 };
+
+// Observation range [base, base + size) of the instance that owns h.
+template <typename T>
+__device__ __forceinline__ void instance_range(int32_t h, const SgdParams<T>& p, int32_t& base, uint32_t& size) {
+    if (p.num_inst <= 1) {
+        base = 0;
+        size = static_cast<uint32_t>(p.n);
+        return;
+    }
+    int lo = 0, hi = p.num_inst - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (p.inst_start[mid] <= h) lo = mid; else hi = mid - 1;
+    }
+    base = p.inst_start[lo];
+    size = static_cast<uint32_t>(p.inst_start[lo + 1] - base);
+}
+
+// Whether head h (in the instance [base, base + size)) belongs to this launch's phase.
+template <typename T>
+__device__ __forceinline__ bool in_phase(int32_t h, int32_t base, uint32_t size, const SgdParams<T>& p) {
+    if (p.num_phases <= 1) return true;
+    const int64_t slice = (static_cast<int64_t>(h - base) * p.num_phases) / size;
+    return slice == p.phase;
+}
 
 // Counter-based negative-sample stream of one event.
 struct NegStream {
@@ -224,7 +267,10 @@ __device__ __forceinline__ T clamp4(T g) {
     return (T(4) < g) ? T(4) : g;
 }
 
-__device__ __forceinline__ float pow_b(float x, float b) { return powf(x, b); }
+// FP32 layouts use the hardware-approximated power (__powf, an exp2 of b log2 x
+// in the special-function unit): the step is stochastic and clamped, and a
+// few-ulp error in d^(2b) is far below the noise of negative sampling.
+__device__ __forceinline__ float pow_b(float x, float b) { return __powf(x, b); }
 __device__ __forceinline__ double pow_b(double x, double b) { return pow(x, b); }
 
 // Attractive coefficient, optimize_layout.hpp:147-149.
@@ -338,35 +384,41 @@ __global__ void __launch_bounds__(256) sgd_epoch_2d_f32(const int64_t* __restric
     for (int64_t s = s0 + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; s < s1; s += int64_t(gridDim.x) * blockDim.x) {
         const int64_t e0 = seg_pos[s], e1 = seg_pos[s + 1];
         const int32_t h = ht[e0].x;
+        int32_t nbase;
+        uint32_t nsize;
+        instance_range(h, p, nbase, nsize);
+        if (!in_phase(h, nbase, nsize, p)) continue;
         const float2 y0 = __ldcg(&Y[h]);
         float hx = y0.x, hy = y0.y;
         for (int64_t e = e0; e < e1; ++e) {
             const int2 pr = ht[e];
-            int nn = nneg[e];
+            int remaining = nneg[e];
             const float2 yt = __ldcg(&Y[pr.y]);
             NegStream rng(static_cast<uint32_t>(h), static_cast<uint32_t>(pr.y), p.epoch, p.k0, p.k1);
-            int32_t ks[NEG_BATCH];
-            float2 yk[NEG_BATCH];
-            const int m0 = nn < NEG_BATCH ? nn : NEG_BATCH;
+            bool attract = true;
+            do {
+                // issue this batch's gathers, then apply the updates in order
+                const int m = remaining < NEG_BATCH ? remaining : NEG_BATCH;
+                int32_t ks[NEG_BATCH];
+                float2 yk[NEG_BATCH];
 #pragma unroll
-            for (int i = 0; i < NEG_BATCH; ++i) {
-                if (i < m0) {
-                    ks[i] = rng.bounded(static_cast<uint32_t>(p.n));
-                    yk[i] = __ldcg(&Y[ks[i]]);
+                for (int i = 0; i < NEG_BATCH; ++i) {
+                    if (i < m) {
+                        ks[i] = nbase + rng.bounded(nsize);
+                        yk[i] = __ldcg(&Y[ks[i]]);
+                    }
                 }
-            }
-            {
-                const float dx = hx - yt.x, dy = hy - yt.y;
-                const float d2 = floor_eps(dx * dx + dy * dy);
-                const float cf = attract_coef(d2, p);
-                const float gx = p.alpha * clamp4(cf * dx);
-                const float gy = p.alpha * clamp4(cf * dy);
-                hx += gx;
-                hy += gy;
-                atomicAdd(&Y[pr.y], make_float2(-gx, -gy));
-            }
-            int m = m0;
-            while (true) {
+                if (attract) {
+                    const float dx = hx - yt.x, dy = hy - yt.y;
+                    const float d2 = floor_eps(dx * dx + dy * dy);
+                    const float cf = attract_coef(d2, p);
+                    const float gx = p.alpha * clamp4(cf * dx);
+                    const float gy = p.alpha * clamp4(cf * dy);
+                    hx += gx;
+                    hy += gy;
+                    atomicAdd(&Y[pr.y], make_float2(-gx, -gy));
+                    attract = false;
+                }
 #pragma unroll
                 for (int i = 0; i < NEG_BATCH; ++i) {
                     if (i < m && ks[i] != h) {
@@ -377,17 +429,8 @@ __global__ void __launch_bounds__(256) sgd_epoch_2d_f32(const int64_t* __restric
                         hy += p.alpha * clamp4(cf * dy);
                     }
                 }
-                nn -= m;
-                if (nn <= 0) break;
-                m = nn < NEG_BATCH ? nn : NEG_BATCH;
-#pragma unroll
-                for (int i = 0; i < NEG_BATCH; ++i) {
-                    if (i < m) {
-                        ks[i] = rng.bounded(static_cast<uint32_t>(p.n));
-                        yk[i] = __ldcg(&Y[ks[i]]);
-                    }
-                }
-            }
+                remaining -= m;
+            } while (remaining > 0);
         }
         atomicAdd(&Y[h], make_float2(hx - y0.x, hy - y0.y));
     }
@@ -404,6 +447,10 @@ __global__ void __launch_bounds__(128) sgd_epoch_generic(const int64_t* __restri
     for (int64_t s = s0 + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; s < s1; s += int64_t(gridDim.x) * blockDim.x) {
         const int64_t e0 = seg_pos[s], e1 = seg_pos[s + 1];
         const int32_t h = ht[e0].x;
+        int32_t nbase;
+        uint32_t nsize;
+        instance_range(h, p, nbase, nsize);
+        if (!in_phase(h, nbase, nsize, p)) continue;
         T* yh = Y + static_cast<size_t>(h) * dim;
         for (int d = 0; d < dim; ++d) head[d] = orig[d] = __ldcg(yh + d);
         for (int64_t e = e0; e < e1; ++e) {
@@ -426,7 +473,7 @@ __global__ void __launch_bounds__(128) sgd_epoch_generic(const int64_t* __restri
             if (nn > 0) {
                 NegStream rng(static_cast<uint32_t>(h), static_cast<uint32_t>(pr.y), p.epoch, p.k0, p.k1);
                 for (int q = 0; q < nn; ++q) {
-                    const int32_t k = rng.bounded(static_cast<uint32_t>(p.n));
+                    const int32_t k = nbase + rng.bounded(nsize);
                     if (k == h) continue;
                     const T* yk = Y + static_cast<size_t>(k) * dim;
                     T dd2 = 0;
@@ -527,33 +574,26 @@ void SgdEngine<T>::build_window(int first, int last_wanted, cudaStream_t s) {
     int64_t last_off = 0, last_cnt = 0;
     UMAPB_CUDA(cudaMemcpyAsync(&last_off, offsets.get() + ncount - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     UMAPB_CUDA(cudaMemcpyAsync(&last_cnt, counts.get() + ncount - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-    UMAPB_CUDA(cudaStreamSynchronize(s));
+    UMAPB_SYNC(s);
     DevArray<int64_t> starts(W + 1, s);
     gather_epoch_starts_kernel<<<grid_for(W + 1, 128), 128, 0, s>>>(offsets.get(), nblocks, W, last_off + last_cnt,
                                                                      starts.get());
     UMAPB_LAUNCH_CHECK();
     std::vector<int64_t> h(W + 1);
     UMAPB_CUDA(cudaMemcpyAsync(h.data(), starts.get(), (W + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-    UMAPB_CUDA(cudaStreamSynchronize(s));
+    UMAPB_SYNC(s);
 
     // fit the window to the memory budget
-    size_t budget = event_budget_bytes;
-    if (budget == 0) {
-        size_t free_b = 0, total_b = 0;
-        UMAPB_CUDA(cudaMemGetInfo(&free_b, &total_b));
-        budget = free_b / 3;
-    }
+    const size_t budget = event_budget_bytes ? event_budget_bytes : WINDOW_BYTES;
     // event record + (at most) one segment start per event
     const size_t per_event = sizeof(int2) + sizeof(uint16_t) + sizeof(int64_t);
     int Wk = W;
     while (Wk > 1 && static_cast<size_t>(h[Wk]) * per_event > budget) --Wk;
     const int64_t events = h[Wk];
 
-    ht_.release();
-    nneg_.release();
-    seg_pos_.release();
-    ht_.allocate(events, s);
-    nneg_.allocate(events, s);
+    // the window buffers are kept across windows (and runs) and only grow
+    ht_.reserve(events, s);
+    nneg_.reserve(events, s);
     DevArray<int> status(1, s);
     status.zero(s);
     if (nnz) {
@@ -582,8 +622,8 @@ void SgdEngine<T>::build_window(int first, int last_wanted, cudaStream_t s) {
     }
     int64_t nseg = 0;
     UMAPB_CUDA(cudaMemcpyAsync(&nseg, boff.get() + seg_blocks, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-    UMAPB_CUDA(cudaStreamSynchronize(s));
-    seg_pos_.allocate(nseg + 1, s);
+    UMAPB_SYNC(s);
+    seg_pos_.reserve(nseg + 1, s);
     UMAPB_CUDA(cudaMemcpyAsync(seg_pos_.get() + nseg, &events, sizeof(int64_t), cudaMemcpyHostToDevice, s));
     if (events > 0) {
         seg_write_kernel<<<static_cast<unsigned>(seg_blocks), SEG_BLOCK, 0, s>>>(events, ht_.get(), epoch_offsets_.get(),
@@ -601,11 +641,62 @@ void SgdEngine<T>::build_window(int first, int last_wanted, cudaStream_t s) {
     host_epoch_offsets_.assign(h.begin(), h.begin() + Wk + 1);
     int st = 0;
     UMAPB_CUDA(cudaMemcpyAsync(&st, status.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
-    UMAPB_CUDA(cudaStreamSynchronize(s));
+    UMAPB_SYNC(s);
     require(st == DEV_OK, "a negative-sample count exceeded 65535");
     window_begin_ = first;
     window_end_ = first + Wk;
     state_epoch_ = window_end_;
+}
+
+// Autotuner: times the 2-d epoch kernel with each candidate launch shape on a
+// scratch copy of the layout (one epoch of the current window), keeps the
+// fastest, and remembers it per size class (log2 of the epoch's events).
+template <typename T>
+template <class Launch>
+void SgdEngine<T>::tune(T* Y, int num_dim, int first, int stop, Launch& launch, cudaStream_t s) {
+    static std::mutex mu;
+    static std::map<int, std::pair<int, int>> cache;
+    int w = -1;
+    for (int e = (first + stop) / 2; e < stop && w < 0; ++e) {
+        const int ww = e - window_begin_;
+        if (host_seg_first_[ww + 1] > host_seg_first_[ww]) w = ww;
+    }
+    if (w < 0) return;
+    const int64_t events = host_epoch_offsets_[w + 1] - host_epoch_offsets_[w];
+    int key = 0;
+    while ((int64_t(1) << key) < events) ++key;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) {
+            block_ = it->second.first;
+            blocks_per_sm_ = it->second.second;
+            return;
+        }
+    }
+    const size_t total = static_cast<size_t>(ep_->n) * num_dim;
+    DevArray<T> scratch(total, s);
+    cudaEvent_t a = event_get(), b = event_get();
+    const int candidates[][2] = {{128, 8}, {128, 16}, {256, 4}, {256, 8}, {256, 12}};
+    float best = 1e30f;
+    for (const auto& c : candidates) {
+        UMAPB_CUDA(cudaMemcpyAsync(scratch.get(), Y, total * sizeof(T), cudaMemcpyDeviceToDevice, s));
+        UMAPB_CUDA(cudaEventRecord(a, s));
+        launch(scratch.get(), window_begin_ + w, w, c[0], c[1]);
+        UMAPB_CUDA(cudaEventRecord(b, s));
+        UMAPB_CUDA(cudaEventSynchronize(b));
+        float t = 0;
+        UMAPB_CUDA(cudaEventElapsedTime(&t, a, b));
+        if (t < best) {
+            best = t;
+            block_ = c[0];
+            blocks_per_sm_ = c[1];
+        }
+    }
+    event_put(a);
+    event_put(b);
+    std::lock_guard<std::mutex> lock(mu);
+    cache[key] = std::make_pair(block_, blocks_per_sm_);
 }
 
 template <typename T>
@@ -624,13 +715,57 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
     p.k0 = static_cast<uint32_t>(seed) ^ RNG_NEGATIVE;
     p.k1 = static_cast<uint32_t>(seed >> 32);
     p.n = ep_->n;
+    p.inst_start = inst_start_;
+    p.num_inst = num_inst_;
+    p.phase = 0;
+    p.num_phases = 1;
     const T lr = static_cast<T>(learning_rate);
 
     cudaEvent_t ev[4];
-    for (auto& e : ev) UMAPB_CUDA(cudaEventCreate(&e));
+    for (auto& e : ev) e = event_get();
     float sched_ms = 0, sgd_ms = 0;
-    const int blocks_2d = sm_count() * 8;
     const int blocks_gen = sm_count() * 8;
+
+    // One epoch launch of window slot w on Yp, with the 2-d kernel's launch shape.
+    auto launch = [&](T* Yp, int e_abs, int w, int block, int blocks_per_sm) {
+        const T epoch_t = static_cast<T>(e_abs);
+        // alpha = lr * (1 - epoch / num_epochs) in the reference's types (optimize_layout.hpp:132-133)
+        p.alpha = static_cast<T>(static_cast<double>(lr) * (1.0 - static_cast<double>(epoch_t / static_cast<T>(total))));
+        p.epoch = static_cast<uint32_t>(e_abs);
+        const int64_t nsegs = host_seg_first_[w + 1] - host_seg_first_[w];
+        if (nsegs == 0) return;
+        const bool use_2d = std::is_same<T, float>::value && num_dim == 2;
+        const int blk = use_2d ? block : 128;
+        const unsigned g = use_2d ? grid_for(nsegs, block, sm_count() * blocks_per_sm) : grid_for(nsegs, 128, blocks_gen);
+        // Parallel updates read positions that the serial order would already
+        // have moved; when every event of an epoch is in flight at once the
+        // layouts come out measurably tighter (lower edge cross-entropy) than
+        // the reference's.  Slicing each instance's heads into at least
+        // min_phases ordered launches bounds that staleness.  One instance with
+        // more segments than resident threads is already processed in rounds
+        // by the grid-stride loop, and needs fewer explicit phases.
+        int phases = std::max(1, min_phases);
+        if (num_inst_ <= 1) {
+            const int64_t threads = static_cast<int64_t>(g) * blk;
+            const int64_t rounds = (nsegs + threads - 1) / threads;
+            phases = static_cast<int>(std::max<int64_t>(1, (phases + rounds - 1) / rounds));
+        }
+        p.num_phases = phases;
+        for (int ph = 0; ph < phases; ++ph) {
+            p.phase = ph;
+            if (use_2d) {
+                if constexpr (std::is_same<T, float>::value) {
+                    sgd_epoch_2d_f32<<<g, blk, 0, s>>>(seg_first_.get(), w, seg_pos_.get(), ht_.get(), nneg_.get(),
+                                                       reinterpret_cast<float2*>(Yp), p);
+                }
+            } else {
+                sgd_epoch_generic<T><<<g, 128, 0, s>>>(seg_first_.get(), w, seg_pos_.get(), ht_.get(), nneg_.get(),
+                                                       Yp, num_dim, p);
+            }
+            UMAPB_LAUNCH_CHECK();
+        }
+    };
+
     int e = first;
     while (e < last) {
         if (e < window_begin_ || e >= window_end_) {
@@ -643,30 +778,20 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
             sched_ms += t;
         }
         const int stop = std::min(last, window_end_);
+        if (autotune && std::is_same<T, float>::value && num_dim == 2) tune(Y, num_dim, e, stop, launch, s);
         UMAPB_CUDA(cudaEventRecord(ev[2], s));
-        for (; e < stop; ++e) {
-            // alpha = lr * (1 - epoch / num_epochs) in the reference's types (optimize_layout.hpp:132-133)
-            const T epoch_t = static_cast<T>(e);
-            p.alpha = static_cast<T>(static_cast<double>(lr) * (1.0 - static_cast<double>(epoch_t / static_cast<T>(total))));
-            p.epoch = static_cast<uint32_t>(e);
-            const int w = e - window_begin_;
-            const int64_t nsegs = host_seg_first_[w + 1] - host_seg_first_[w];
-            if (nsegs == 0) continue;
-            bool done = false;
-            if constexpr (std::is_same<T, float>::value) {
-                if (num_dim == 2) {
-                    const unsigned g = grid_for(nsegs, 256, blocks_2d);
-                    sgd_epoch_2d_f32<<<g, 256, 0, s>>>(seg_first_.get(), w, seg_pos_.get(), ht_.get(), nneg_.get(),
-                                                       reinterpret_cast<float2*>(Y), p);
-                    done = true;
-                }
-            }
-            if (!done) {
-                const unsigned g = grid_for(nsegs, 128, blocks_gen);
-                sgd_epoch_generic<T><<<g, 128, 0, s>>>(seg_first_.get(), w, seg_pos_.get(), ht_.get(), nneg_.get(), Y,
-                                                       num_dim, p);
-            }
-            UMAPB_LAUNCH_CHECK();
+        // optionally record this window's epoch launches as one CUDA graph
+        cudaGraph_t graph = nullptr;
+        if (use_graphs) UMAPB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        for (; e < stop; ++e) launch(Y, e, e - window_begin_, block_, blocks_per_sm_);
+        if (use_graphs) {
+            UMAPB_CUDA(cudaStreamEndCapture(s, &graph));
+            cudaGraphExec_t exec = nullptr;
+            UMAPB_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+            UMAPB_CUDA(cudaGraphLaunch(exec, s));
+            UMAPB_SYNC(s);
+            cudaGraphExecDestroy(exec);
+            cudaGraphDestroy(graph);
         }
         UMAPB_CUDA(cudaEventRecord(ev[3], s));
         UMAPB_CUDA(cudaEventSynchronize(ev[3]));
@@ -674,7 +799,7 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
         UMAPB_CUDA(cudaEventElapsedTime(&t, ev[2], ev[3]));
         sgd_ms += t;
     }
-    for (auto& x : ev) cudaEventDestroy(x);
+    for (auto& x : ev) event_put(x);
     if (ms_schedule) *ms_schedule = sched_ms;
     if (ms_sgd) *ms_sgd = sgd_ms;
 }
@@ -696,8 +821,21 @@ void SgdEngine<T>::counts(int first, int last, int64_t* out, cudaStream_t s) {
     }
     std::vector<unsigned long long> h(2 * static_cast<size_t>(W));
     UMAPB_CUDA(cudaMemcpyAsync(h.data(), totals.get(), h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-    UMAPB_CUDA(cudaStreamSynchronize(s));
+    UMAPB_SYNC(s);
     for (size_t i = 0; i < h.size(); ++i) out[i] = static_cast<int64_t>(h[i]);
+}
+
+// 4 ordered slices: the parallel epoch then matches the serial reference's
+// edge cross-entropy and trustworthiness to within their seed-to-seed noise.
+// UMAPB_SGD_PHASES overrides it (1 = every event of an epoch in one launch).
+template <typename T>
+int SgdEngine<T>::default_min_phases() {
+    static const int v = [] {
+        const char* e = std::getenv("UMAPB_SGD_PHASES");
+        const int x = e ? std::atoi(e) : 0;
+        return (x >= 1 && x <= 64) ? x : 4;
+    }();
+    return v;
 }
 
 template class SgdEngine<float>;

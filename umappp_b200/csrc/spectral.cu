@@ -290,7 +290,7 @@ struct LanczosDevice {
         UMAPB_LAUNCH_CHECK();
         double v = 0;
         UMAPB_CUDA(cudaMemcpyAsync(&v, h.get(), sizeof(double), cudaMemcpyDeviceToHost, s));
-        UMAPB_CUDA(cudaStreamSynchronize(s));
+        UMAPB_SYNC(s);
         return std::sqrt(v);
     }
     void scale(const double* x, double f, double* y) {
@@ -300,7 +300,7 @@ struct LanczosDevice {
     double hsum_at(int c) {
         double v = 0;
         UMAPB_CUDA(cudaMemcpyAsync(&v, hsum.get() + c, sizeof(double), cudaMemcpyDeviceToHost, s));
-        UMAPB_CUDA(cudaStreamSynchronize(s));
+        UMAPB_SYNC(s);
         return v;
     }
 };
@@ -319,7 +319,7 @@ SpectralResult spectral_init(int32_t n, const int64_t* ptr, const int32_t* idx, 
 
     int64_t nnz = 0;
     UMAPB_CUDA(cudaMemcpyAsync(&nnz, ptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-    UMAPB_CUDA(cudaStreamSynchronize(s));
+    UMAPB_SYNC(s);
     DevArray<double> sums(n, s), lap(std::max<int64_t>(nnz, 1), s);
     degree_sqrt_kernel<T><<<grid_for(n, 256), 256, 0, s>>>(n, ptr, w, sums.get());
     UMAPB_LAUNCH_CHECK();
@@ -424,13 +424,13 @@ SpectralResult spectral_init(int32_t n, const int64_t* ptr, const int32_t* idx, 
         UMAPB_LAUNCH_CHECK();
         std::vector<int> hw(nev);
         UMAPB_CUDA(cudaMemcpyAsync(hw.data(), where.get(), sizeof(int) * nev, cudaMemcpyDeviceToHost, s));
-        UMAPB_CUDA(cudaStreamSynchronize(s));
+        UMAPB_SYNC(s);
         for (int c = 0; c < nev; ++c) {
             const int32_t i = (hw[c] >= 0 && hw[c] < n) ? hw[c] : 0;
             double v = 0;
             UMAPB_CUDA(cudaMemcpyAsync(&v, L.tmp.get() + static_cast<size_t>(c) * n + i, sizeof(double),
                                        cudaMemcpyDeviceToHost, s));
-            UMAPB_CUDA(cudaStreamSynchronize(s));
+            UMAPB_SYNC(s);
             sign[c] = (v < 0) ? -1.0 : 1.0;
         }
     }
@@ -441,7 +441,7 @@ SpectralResult spectral_init(int32_t n, const int64_t* ptr, const int32_t* idx, 
     UMAPB_LAUNCH_CHECK();
     unsigned long long mbits = 0;
     UMAPB_CUDA(cudaMemcpyAsync(&mbits, mx.get(), sizeof(mbits), cudaMemcpyDeviceToHost, s));
-    UMAPB_CUDA(cudaStreamSynchronize(s));
+    UMAPB_SYNC(s);
     double max_val;
     std::memcpy(&max_val, &mbits, sizeof(double));
     const double expansion = (max_val > 0 ? scale / max_val : 1);
@@ -456,7 +456,7 @@ SpectralResult spectral_init(int32_t n, const int64_t* ptr, const int32_t* idx, 
             ntotal, Y, jitter_sd, static_cast<uint32_t>(seed) ^ RNG_JITTER, static_cast<uint32_t>(seed >> 32));
         UMAPB_LAUNCH_CHECK();
     }
-    UMAPB_CUDA(cudaStreamSynchronize(s));
+    UMAPB_SYNC(s);
     res.ok = true;
     return res;
 }

@@ -48,8 +48,17 @@ void knn_exact(const T* data, int32_t n, int32_t dim, int32_t k, int32_t* out_id
 bool knn_tc_supported(int32_t dim, int kcap);
 void knn_tc_candidates(const float* data, int32_t n, int32_t dim, int kcap, int32_t* cand_idx, float* cand_d2,
                        float* norms_out, int* d_err, cudaStream_t s);
+// Batched: instance i is data rows [inst[i], inst[i + 1]) (host vector).
+void knn_tc_candidates_batched(const float* data, const std::vector<int32_t>& inst, int32_t dim, int kcap,
+                               int32_t* cand_idx, float* cand_d2, int* d_err, cudaStream_t s);
 // Number of queries the last float kNN recomputed in FP64 (certainty check).
 int& last_knn_redo_count();
+
+// Exact kNN of every observation within its own instance (instance i is data
+// rows [inst[i], inst[i + 1]), host vector); indices are data rows.
+template <typename T>
+void knn_exact_batched(const T* data, const std::vector<int32_t>& inst, int32_t dim, int32_t k, int32_t* out_idx,
+                       T* out_dist, cudaStream_t s);
 
 // ---- similarities (similarities.cu) -----------------------------------------
 template <typename T>
@@ -62,9 +71,12 @@ template <typename T>
 void combine_neighbor_sets(int32_t n, const int64_t* ptr, const int32_t* idx, const T* w, int64_t nnz_in,
                            double mix_ratio, DeviceCsr<T>& out, cudaStream_t s);
 
+// inst_start (device, num_inst + 1 entries) splits the rows into independent
+// instances, each with its own maximum weight (batched runs); NULL: one instance.
 template <typename T>
 void similarities_to_epochs(int32_t n, const int64_t* ptr, const int32_t* idx, const T* w, int64_t nnz,
-                            int num_epochs, double negative_sample_rate, DeviceEpochs<T>& out, cudaStream_t s);
+                            int num_epochs, double negative_sample_rate, DeviceEpochs<T>& out, cudaStream_t s,
+                            const int32_t* inst_start = nullptr, int32_t num_inst = 1);
 
 // Number of connected components (undirected union-find); status word set on timeout.
 int64_t count_components(int32_t n, const int64_t* ptr, const int32_t* idx, int* d_status, cudaStream_t s);
@@ -100,11 +112,32 @@ public:
     void counts(int first, int last, int64_t* out, cudaStream_t s);
     // Schedule state (enext, enneg) at 'epoch' into device arrays.
     void state_at(int epoch, T* enext, T* enneg, cudaStream_t s);
-    size_t event_budget_bytes = 0;  // 0: one third of free device memory
+    size_t event_budget_bytes = 0;  // window buffer cap; 0: 1 GiB (sgd.cu, WINDOW_BYTES)
+    // Batched runs: instance i owns observations [inst_start[i], inst_start[i+1])
+    // (device array of num_inst + 1 entries); negative samples stay inside it.
+    void set_instances(const int32_t* inst_start, int32_t num_inst) {
+        inst_start_ = inst_start;
+        num_inst_ = num_inst;
+    }
+    // Record each window's epochs as one CUDA graph and launch that.
+    bool use_graphs = false;
+    // Minimum number of ordered head slices per epoch (sgd.cu, run()).
+    int min_phases = default_min_phases();
+    static int default_min_phases();
+    // Pick the epoch kernel's launch shape (block size, blocks per SM) by
+    // timing candidates on a scratch copy of the layout (sgd.cu, tune()).
+    bool autotune = false;
+    int block_size() const { return block_; }
+    int blocks_per_sm() const { return blocks_per_sm_; }
 
 private:
     void build_window(int first, int last_wanted, cudaStream_t s);
+    template <class Launch>
+    void tune(T* Y, int num_dim, int first, int stop, Launch& launch, cudaStream_t s);
+    int block_ = 256, blocks_per_sm_ = 8;
     const DeviceEpochs<T>* ep_ = nullptr;
+    const int32_t* inst_start_ = nullptr;
+    int32_t num_inst_ = 1;
     int base_epoch_ = 0;
     DevArray<T> enext_, enneg_;    // schedule state at state_epoch_
     int state_epoch_ = 0;          // epoch the state arrays describe
