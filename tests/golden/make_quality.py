@@ -1,0 +1,97 @@
+"""Reference layout quality on the benchmark workloads (tests/golden/quality_<workload>.json).
+
+Runs the reference pipeline (oracle/_ref/libumappp_ref.so: the reference's
+headers compiled against the project's stand-ins) on the host cores, on the
+benchmark's seeded Gaussian mixture: exact kNN (the reference's brute-force
+search), initialize() and Status::run() with the benchmark's options, for a
+few optimisation seeds.  Records, per seed, the fuzzy cross-entropy of the
+layout over the union graph and its trustworthiness (k = 15) on a fixed,
+seeded sample of query points.  The device test
+(tests/test_gpu_quality.py) recomputes both for the device's layout on the
+same data and queries.
+
+    python tests/golden/make_quality.py [--workload mixture_1m] [--seeds 2]
+        [--knn-cache PATH]     # .npz with the kNN, reused if present
+
+The 1M-point workload takes about half an hour on 8 cores (mostly the
+exact kNN).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import bench  # noqa: E402
+import oracle  # noqa: E402
+
+QUERY_SEED = 123
+NUM_QUERIES = 1000
+
+
+def query_sample(n: int) -> np.ndarray:
+    return np.sort(np.random.default_rng(QUERY_SEED).choice(n, size=min(NUM_QUERIES, n), replace=False)).astype(np.int32)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="mixture_1m", choices=sorted(bench.CONFIGS))
+    ap.add_argument("--seeds", type=int, default=2)
+    ap.add_argument("--threads", type=int, default=os.cpu_count() or 1)
+    ap.add_argument("--knn-cache", default=None)
+    args = ap.parse_args()
+
+    n, dim, _, _, _, k, epochs = bench.CONFIGS[args.workload]
+    X = bench.make_data(args.workload)
+    t0 = time.time()
+    if args.knn_cache and os.path.exists(args.knn_cache):
+        z = np.load(args.knn_cache)
+        idx, dist = z["idx"], z["dist"]
+    else:
+        idx, dist = oracle.ref_knn(X, k, nthreads=args.threads)
+        if args.knn_cache:
+            np.savez(args.knn_cache, idx=idx, dist=dist)
+    print(f"knn {time.time() - t0:.0f} s", flush=True)
+    nl = oracle.CSR.from_dense(idx, dist)
+    w, _, _ = oracle.neighbor_similarities(nl.astype(np.float64))
+    g = oracle.combine_neighbor_sets(w, 1.0)
+    a, b = oracle.find_ab(1.0, 0.1)
+    q = query_sample(n)
+
+    runs = []
+    for s in range(args.seeds):
+        seed = 1234567890 + s
+        Y = np.zeros((n, 2), np.float32)
+        t0 = time.time()
+        st = oracle.ref_initialize(nl, 2, Y, num_epochs=epochs, optimize_seed=seed, num_threads=args.threads,
+                                   num_threads_optimize=args.threads, num_threads_spectral=args.threads)
+        st.run(Y)
+        secs = time.time() - t0
+        ce = oracle.cross_entropy(g, Y, a, b)
+        tr = oracle.trustworthiness(X, Y, 15, queries=q)
+        runs.append({"optimize_seed": seed, "cross_entropy": ce, "trustworthiness": tr, "seconds": round(secs, 1)})
+        print(runs[-1], flush=True)
+
+    out = {
+        "workload": args.workload, "n": n, "dim": dim, "k": k, "epochs": epochs,
+        "data": "bench.make_data(workload) (seeded Gaussian mixture)",
+        "trust_k": 15, "query_seed": QUERY_SEED, "num_queries": int(len(q)),
+        "cross_entropy_graph": "FP64 similarities + union of the exact kNN, oracle.cross_entropy",
+        "reference": runs,
+    }
+    path = os.path.join(HERE, f"quality_{args.workload}.json")
+    with open(path, "w") as f:
+        json.dump(out, f, indent=1)
+    print("wrote", path)
+
+
+if __name__ == "__main__":
+    main()
