@@ -194,7 +194,10 @@ class Status:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            lib().umapb_status_free(h)
+            try:
+                lib().umapb_status_free(h)
+            except Exception:   # interpreter shutdown: module globals already gone
+                pass
             self._h = None
 
     def run(self, embedding, epoch_limit: Optional[int] = None) -> None:

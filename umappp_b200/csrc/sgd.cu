@@ -366,17 +366,20 @@ __global__ void seg_first_kernel(const int64_t* __restrict__ seg_pos, int64_t ns
     }
 }
 
-// Negative samples are gathered NEG_BATCH at a time: their indices do not
-// depend on the layout, so all loads of a batch (and the tail's) are in flight
-// together, and the head then takes the updates in sequence.
-constexpr int NEG_BATCH = 12;
+// Negative samples are gathered NB at a time: their indices do not depend on
+// the layout, so all loads of a batch (and the tail's) are in flight together,
+// and the head then takes the updates in sequence.  NB and the minimum number
+// of resident 256-thread blocks (which caps the registers per thread) trade
+// gathers in flight per thread against resident threads; the variants are
+// listed in SGD_2D_VARIANTS.
 
 // One thread per segment: the head's firing edges are processed in CSR order
 // with the head kept in registers, each edge's attractive step (head and tail)
 // followed by its negative samples -- the per-row sequence of
 // optimize_layout.hpp:136-180.  The tail moves by a vector atomic; the head's
 // total displacement is added once at the end.
-__global__ void __launch_bounds__(256) sgd_epoch_2d_f32(const int64_t* __restrict__ seg_first, int w,
+template <int NB, int MINB>
+__global__ void __launch_bounds__(256, MINB) sgd_epoch_2d_f32(const int64_t* __restrict__ seg_first, int w,
                                                         const int64_t* __restrict__ seg_pos,
                                                         const int2* __restrict__ ht, const uint16_t* __restrict__ nneg,
                                                         float2* __restrict__ Y, SgdParams<float> p) {
@@ -398,11 +401,11 @@ __global__ void __launch_bounds__(256) sgd_epoch_2d_f32(const int64_t* __restric
             bool attract = true;
             do {
                 // issue this batch's gathers, then apply the updates in order
-                const int m = remaining < NEG_BATCH ? remaining : NEG_BATCH;
-                int32_t ks[NEG_BATCH];
-                float2 yk[NEG_BATCH];
+                const int m = remaining < NB ? remaining : NB;
+                int32_t ks[NB];
+                float2 yk[NB];
 #pragma unroll
-                for (int i = 0; i < NEG_BATCH; ++i) {
+                for (int i = 0; i < NB; ++i) {
                     if (i < m) {
                         ks[i] = nbase + rng.bounded(nsize);
                         yk[i] = __ldcg(&Y[ks[i]]);
@@ -420,7 +423,7 @@ __global__ void __launch_bounds__(256) sgd_epoch_2d_f32(const int64_t* __restric
                     attract = false;
                 }
 #pragma unroll
-                for (int i = 0; i < NEG_BATCH; ++i) {
+                for (int i = 0; i < NB; ++i) {
                     if (i < m && ks[i] != h) {
                         const float dx = hx - yk[i].x, dy = hy - yk[i].y;
                         const float d2 = floor_eps(dx * dx + dy * dy);
@@ -434,6 +437,33 @@ __global__ void __launch_bounds__(256) sgd_epoch_2d_f32(const int64_t* __restric
         }
         atomicAdd(&Y[h], make_float2(hx - y0.x, hy - y0.y));
     }
+}
+
+struct Sgd2dVariant {
+    void (*kernel)(const int64_t*, int, const int64_t*, const int2*, const uint16_t*, float2*, SgdParams<float>);
+    int neg_batch, min_blocks;
+};
+const Sgd2dVariant SGD_2D_VARIANTS[] = {
+    {sgd_epoch_2d_f32<12, 1>, 12, 1},   // 80 registers: 3 blocks of 256 per SM
+    {sgd_epoch_2d_f32<12, 4>, 12, 4},   // 64 registers
+    {sgd_epoch_2d_f32<8, 4>, 8, 4},     // default
+    {sgd_epoch_2d_f32<6, 6>, 6, 6},     // 40 registers
+};
+constexpr int NUM_SGD_2D_VARIANTS = sizeof(SGD_2D_VARIANTS) / sizeof(SGD_2D_VARIANTS[0]);
+
+// Resident blocks per SM of variant v at 'block' threads (occupancy query, cached).
+int sgd_2d_resident(int v, int block) {
+    static int cache[NUM_SGD_2D_VARIANTS][2] = {};
+    const int bi = block == 128 ? 0 : 1;
+    if (cache[v][bi] == 0) {
+        int r = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, SGD_2D_VARIANTS[v].kernel, block, 0) != cudaSuccess || r < 1) {
+            cudaGetLastError();
+            r = 1;
+        }
+        cache[v][bi] = r;
+    }
+    return cache[v][bi];
 }
 
 // Any dimension (up to MAX_GENERIC_DIM) and either precision; same per-segment order.
@@ -488,6 +518,16 @@ __global__ void __launch_bounds__(128) sgd_epoch_generic(const int64_t* __restri
         }
         for (int d = 0; d < dim; ++d) atomicAdd(yh + d, head[d] - orig[d]);
     }
+}
+
+// Grid size as a multiple of the resident blocks (UMAPB_SGD_GRID_MULTIPLE, default 1).
+int grid_multiple() {
+    static const int v = [] {
+        const char* e = std::getenv("UMAPB_SGD_GRID_MULTIPLE");
+        const int x = e ? std::atoi(e) : 0;
+        return (x >= 1 && x <= 64) ? x : 1;
+    }();
+    return v;
 }
 
 int sm_count() {
@@ -655,7 +695,7 @@ template <typename T>
 template <class Launch>
 void SgdEngine<T>::tune(T* Y, int num_dim, int first, int stop, Launch& launch, cudaStream_t s) {
     static std::mutex mu;
-    static std::map<int, std::pair<int, int>> cache;
+    static std::map<int, std::pair<int, int>> cache;   // size class -> (block, variant)
     int w = -1;
     for (int e = (first + stop) / 2; e < stop && w < 0; ++e) {
         const int ww = e - window_begin_;
@@ -670,33 +710,34 @@ void SgdEngine<T>::tune(T* Y, int num_dim, int first, int stop, Launch& launch, 
         auto it = cache.find(key);
         if (it != cache.end()) {
             block_ = it->second.first;
-            blocks_per_sm_ = it->second.second;
+            variant_ = it->second.second;
             return;
         }
     }
     const size_t total = static_cast<size_t>(ep_->n) * num_dim;
     DevArray<T> scratch(total, s);
     cudaEvent_t a = event_get(), b = event_get();
-    const int candidates[][2] = {{128, 8}, {128, 16}, {256, 4}, {256, 8}, {256, 12}};
     float best = 1e30f;
-    for (const auto& c : candidates) {
-        UMAPB_CUDA(cudaMemcpyAsync(scratch.get(), Y, total * sizeof(T), cudaMemcpyDeviceToDevice, s));
-        UMAPB_CUDA(cudaEventRecord(a, s));
-        launch(scratch.get(), window_begin_ + w, w, c[0], c[1]);
-        UMAPB_CUDA(cudaEventRecord(b, s));
-        UMAPB_CUDA(cudaEventSynchronize(b));
-        float t = 0;
-        UMAPB_CUDA(cudaEventElapsedTime(&t, a, b));
-        if (t < best) {
-            best = t;
-            block_ = c[0];
-            blocks_per_sm_ = c[1];
+    for (int v = 0; v < NUM_SGD_2D_VARIANTS; ++v) {
+        for (int blk : {128, 256}) {
+            UMAPB_CUDA(cudaMemcpyAsync(scratch.get(), Y, total * sizeof(T), cudaMemcpyDeviceToDevice, s));
+            UMAPB_CUDA(cudaEventRecord(a, s));
+            launch(scratch.get(), window_begin_ + w, w, blk, v);
+            UMAPB_CUDA(cudaEventRecord(b, s));
+            UMAPB_CUDA(cudaEventSynchronize(b));
+            float t = 0;
+            UMAPB_CUDA(cudaEventElapsedTime(&t, a, b));
+            if (t < best) {
+                best = t;
+                block_ = blk;
+                variant_ = v;
+            }
         }
     }
     event_put(a);
     event_put(b);
     std::lock_guard<std::mutex> lock(mu);
-    cache[key] = std::make_pair(block_, blocks_per_sm_);
+    cache[key] = std::make_pair(block_, variant_);
 }
 
 template <typename T>
@@ -726,8 +767,8 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
     float sched_ms = 0, sgd_ms = 0;
     const int blocks_gen = sm_count() * 8;
 
-    // One epoch launch of window slot w on Yp, with the 2-d kernel's launch shape.
-    auto launch = [&](T* Yp, int e_abs, int w, int block, int blocks_per_sm) {
+    // One epoch launch of window slot w on Yp, with the 2-d kernel's block size and variant.
+    auto launch = [&](T* Yp, int e_abs, int w, int block, int variant) {
         const T epoch_t = static_cast<T>(e_abs);
         // alpha = lr * (1 - epoch / num_epochs) in the reference's types (optimize_layout.hpp:132-133)
         p.alpha = static_cast<T>(static_cast<double>(lr) * (1.0 - static_cast<double>(epoch_t / static_cast<T>(total))));
@@ -736,7 +777,8 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
         if (nsegs == 0) return;
         const bool use_2d = std::is_same<T, float>::value && num_dim == 2;
         const int blk = use_2d ? block : 128;
-        const unsigned g = use_2d ? grid_for(nsegs, block, sm_count() * blocks_per_sm) : grid_for(nsegs, 128, blocks_gen);
+        const int resident = use_2d ? sm_count() * sgd_2d_resident(variant, block) : blocks_gen;
+        const unsigned g = grid_for(nsegs, blk, static_cast<unsigned>(resident * grid_multiple()));
         // Parallel updates read positions that the serial order would already
         // have moved; when every event of an epoch is in flight at once the
         // layouts come out measurably tighter (lower edge cross-entropy) than
@@ -746,7 +788,7 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
         // by the grid-stride loop, and needs fewer explicit phases.
         int phases = std::max(1, min_phases);
         if (num_inst_ <= 1) {
-            const int64_t threads = static_cast<int64_t>(g) * blk;
+            const int64_t threads = static_cast<int64_t>(std::min<int64_t>(g, resident)) * blk;
             const int64_t rounds = (nsegs + threads - 1) / threads;
             phases = static_cast<int>(std::max<int64_t>(1, (phases + rounds - 1) / rounds));
         }
@@ -755,8 +797,8 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
             p.phase = ph;
             if (use_2d) {
                 if constexpr (std::is_same<T, float>::value) {
-                    sgd_epoch_2d_f32<<<g, blk, 0, s>>>(seg_first_.get(), w, seg_pos_.get(), ht_.get(), nneg_.get(),
-                                                       reinterpret_cast<float2*>(Yp), p);
+                    SGD_2D_VARIANTS[variant].kernel<<<g, blk, 0, s>>>(seg_first_.get(), w, seg_pos_.get(), ht_.get(),
+                                                                      nneg_.get(), reinterpret_cast<float2*>(Yp), p);
                 }
             } else {
                 sgd_epoch_generic<T><<<g, 128, 0, s>>>(seg_first_.get(), w, seg_pos_.get(), ht_.get(), nneg_.get(),
@@ -783,7 +825,7 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
         // optionally record this window's epoch launches as one CUDA graph
         cudaGraph_t graph = nullptr;
         if (use_graphs) UMAPB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        for (; e < stop; ++e) launch(Y, e, e - window_begin_, block_, blocks_per_sm_);
+        for (; e < stop; ++e) launch(Y, e, e - window_begin_, block_, variant_);
         if (use_graphs) {
             UMAPB_CUDA(cudaStreamEndCapture(s, &graph));
             cudaGraphExec_t exec = nullptr;
@@ -834,6 +876,18 @@ int SgdEngine<T>::default_min_phases() {
         const char* e = std::getenv("UMAPB_SGD_PHASES");
         const int x = e ? std::atoi(e) : 0;
         return (x >= 1 && x <= 64) ? x : 4;
+    }();
+    return v;
+}
+
+// UMAPB_SGD_VARIANT selects the 2-d kernel variant (index into
+// SGD_2D_VARIANTS) when the launch shape is not tuned.
+template <typename T>
+int SgdEngine<T>::default_variant() {
+    static const int v = [] {
+        const char* e = std::getenv("UMAPB_SGD_VARIANT");
+        const int x = e ? std::atoi(e) : -1;
+        return (x >= 0 && x < NUM_SGD_2D_VARIANTS) ? x : 2;   // measured fastest at 100k and 1M points
     }();
     return v;
 }

@@ -124,17 +124,18 @@ public:
     // Minimum number of ordered head slices per epoch (sgd.cu, run()).
     int min_phases = default_min_phases();
     static int default_min_phases();
-    // Pick the epoch kernel's launch shape (block size, blocks per SM) by
-    // timing candidates on a scratch copy of the layout (sgd.cu, tune()).
+    // Pick the 2-d epoch kernel's block size and variant by timing the
+    // candidates on a scratch copy of the layout (sgd.cu, tune()).
     bool autotune = false;
     int block_size() const { return block_; }
-    int blocks_per_sm() const { return blocks_per_sm_; }
+    int variant() const { return variant_; }   // 2-d kernel variant (sgd.cu, SGD_2D_VARIANTS)
 
 private:
     void build_window(int first, int last_wanted, cudaStream_t s);
     template <class Launch>
     void tune(T* Y, int num_dim, int first, int stop, Launch& launch, cudaStream_t s);
-    int block_ = 256, blocks_per_sm_ = 8;
+    static int default_variant();
+    int block_ = 256, variant_ = default_variant();
     const DeviceEpochs<T>* ep_ = nullptr;
     const int32_t* inst_start_ = nullptr;
     int32_t num_inst_ = 1;
