@@ -181,6 +181,12 @@ int umapb_knn(int dtype, size_t data_dim, int32_t num_obs, const void* data, int
  * set could not be certified by the error bound and were recomputed in FP64. */
 int umapb_knn_last_fp64_recomputed(void);
 
+/* Largest error of the tensor-core squared distances of the last float kNN
+ * on this process, relative to |q|^2 + max |r|^2 (the scale of the bound that
+ * decides which queries are recomputed in FP64); 0 if the last search did not
+ * use tensor cores.  No reference counterpart: a precision diagnostic. */
+double umapb_knn_last_tc_error(void);
+
 /*
  * neighbor_similarities (include/umappp/neighbor_similarities.hpp:53-207):
  * replaces the distances of each CSR row by membership weights in place.

@@ -54,6 +54,25 @@ def test_knn_f64_bit_exact(umap, n, dim, k):
     assert np.array_equal(dist, rdist)
 
 
+@pytest.mark.parametrize("kind", ["f16", "tf32"])
+@pytest.mark.parametrize("n,dim,k", [(3000, 50, 15), (2500, 90, 10), (700, 20, 20), (300, 63, 15)])
+def test_knn_tensor_core_operands(umap, monkeypatch, kind, n, dim, k):
+    # both operand splits give the exact neighbours; the candidate distances stay
+    # inside the bound that decides FP64 recomputation (2^-17 of |q|^2 + max |r|^2)
+    monkeypatch.setenv("UMAPB_KNN_TC_KIND", kind)
+    X = oracle.gaussian_mixture(n, dim, 8, 3.0, seed=n + dim + k, dtype=np.float32)
+    X *= np.float32(37.5)   # not a power of two: the FP16 scaling must stay exact
+    idx, dist = umap.knn(X, k)
+    ridx, rdist = oracle.knn(X, k)
+    assert _same_neighbors(idx, ridx, rdist) == 0
+    assert rel_err(dist, rdist) <= 1e-6
+    err = umap.lib().umapb_knn_last_tc_error()
+    if kind == "tf32" and dim + 1 > 64:
+        assert err == 0.0          # no TF32 tensor-core path at this width: SIMT search
+    else:
+        assert 0.0 < err < 2.0 ** -17, err
+
+
 def test_knn_duplicates_and_ties(umap):
     rng = np.random.default_rng(3)
     base = rng.normal(size=(50, 4))

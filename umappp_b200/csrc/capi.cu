@@ -609,6 +609,8 @@ int umapb_knn(int dtype, size_t data_dim, int32_t num_obs, const void* data, int
 
 int umapb_knn_last_fp64_recomputed(void) { return last_knn_redo_count(); }
 
+double umapb_knn_last_tc_error(void) { return last_knn_tc_error(); }
+
 int umapb_neighbor_similarities(int dtype, int32_t num_obs, const int64_t* row_ptr, void* distances,
                                 double local_connectivity, double bandwidth, double min_k_dist_scale, int use_newton,
                                 double* rho_out, double* sigma_out) {

@@ -16,6 +16,7 @@
 // Double data: the FP64 kernel directly, with multiply and add kept separate
 // so the sums round exactly as a sequential FP64 loop.
 #include <algorithm>
+#include <cstring>
 #include <cfloat>
 #include <cstdlib>
 #include <vector>
@@ -27,6 +28,17 @@ namespace umapb {
 int& last_knn_redo_count() {
     static int count = 0;
     return count;
+}
+
+static float bits_to_float(unsigned int b) {
+    float f;
+    std::memcpy(&f, &b, sizeof(f));
+    return f;
+}
+
+double& last_knn_tc_error() {
+    static double worst = 0.0;
+    return worst;
 }
 
 namespace {
@@ -146,7 +158,8 @@ __global__ void knn_rescore_kernel(const float* __restrict__ data, int32_t n, in
                                    int32_t* __restrict__ out_idx, float* __restrict__ out_dist,
                                    double* __restrict__ out_dist64, int32_t* __restrict__ redo,
                                    int32_t* __restrict__ redo_count, const float* __restrict__ norms,
-                                   const unsigned int* __restrict__ norm_max_bits, double tc_rel) {
+                                   const unsigned int* __restrict__ norm_max_bits, double tc_rel,
+                                   unsigned int* __restrict__ tc_err_bits) {
     const int32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n) return;
     double d64[KCAP];
@@ -154,6 +167,10 @@ __global__ void knn_rescore_kernel(const float* __restrict__ data, int32_t n, in
     const int32_t* ci = cand_idx + static_cast<size_t>(q) * KCAP;
     const float* xq = data + static_cast<size_t>(q) * dim;
     int m = 0;
+    float worst = 0.0f;   // largest |FP32 candidate distance - FP64 distance| / (|q|^2 + max |r|^2)
+    const double err_scale = (norms && tc_err_bits)
+                                 ? 1.0 / (static_cast<double>(norms[q]) + static_cast<double>(__uint_as_float(*norm_max_bits)) + 1e-300)
+                                 : 0.0;
     for (int c = 0; c < KCAP; ++c) {
         const int32_t j = ci[c];
         double s = 0;
@@ -162,6 +179,10 @@ __global__ void knn_rescore_kernel(const float* __restrict__ data, int32_t n, in
             for (int d = 0; d < dim; ++d) {
                 const double diff = static_cast<double>(xq[d]) - static_cast<double>(xj[d]);
                 s = __dadd_rn(s, __dmul_rn(diff, diff));
+            }
+            if (err_scale > 0.0) {
+                const double e = fabs(static_cast<double>(cand_d2[static_cast<size_t>(q) * KCAP + c]) - s) * err_scale;
+                worst = fmaxf(worst, static_cast<float>(e));
             }
         } else {
             s = CUDART_INF;
@@ -199,6 +220,7 @@ __global__ void knn_rescore_kernel(const float* __restrict__ data, int32_t n, in
         const int32_t slot = atomicAdd(redo_count, 1);
         redo[slot] = q;
     }
+    if (err_scale > 0.0 && worst > 0.0f) atomicMax(tc_err_bits, __float_as_uint(worst));
     for (int c = 0; c < k; ++c) {
         out_idx[static_cast<size_t>(q) * k + c] = id[c];
         const double dd = sqrt(d64[c]);
@@ -279,14 +301,20 @@ void run_f32(const float* data, int32_t n, int32_t dim, int32_t k, int32_t* out_
     }
     DevArray<int32_t> redo(n, s), redo_count(1, s);
     redo_count.zero(s);
+    DevArray<unsigned int> tc_err(1, s);
+    tc_err.zero(s);
     knn_rescore_kernel<KCAP><<<(n + 127) / 128, 128, 0, s>>>(data, n, dim, k, ci.get(), cd.get(), out_idx, out_dist,
                                                              out_dist64, redo.get(), redo_count.get(),
-                                                             tc ? norms.get() : nullptr, norm_max.get(), TC_REL_BOUND);
+                                                             tc ? norms.get() : nullptr, norm_max.get(), TC_REL_BOUND,
+                                                             tc_err.get());
     UMAPB_LAUNCH_CHECK();
     int32_t nredo = 0;
+    unsigned int err_bits = 0;
     UMAPB_CUDA(cudaMemcpyAsync(&nredo, redo_count.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaMemcpyAsync(&err_bits, tc_err.get(), sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
     UMAPB_SYNC(s);
     last_knn_redo_count() = nredo;
+    last_knn_tc_error() = tc ? static_cast<double>(bits_to_float(err_bits)) : 0.0;
     if (nredo > 0) {
         // exact FP64 search for the uncertain queries (same output rows)
         if (k + 8 <= 32) {
@@ -340,14 +368,19 @@ void run_f32_batched(const float* data, const std::vector<int32_t>& inst, int32_
     UMAPB_LAUNCH_CHECK();
     DevArray<int32_t> redo(n, s), redo_count(1, s);
     redo_count.zero(s);
+    DevArray<unsigned int> tc_err(1, s);
+    tc_err.zero(s);
     knn_rescore_kernel<KCAP><<<(n + 127) / 128, 128, 0, s>>>(data, n, dim, k, ci.get(), cd.get(), out_idx, out_dist,
                                                              nullptr, redo.get(), redo_count.get(), norms.get(),
-                                                             norm_max.get(), TC_REL_BOUND);
+                                                             norm_max.get(), TC_REL_BOUND, tc_err.get());
     UMAPB_LAUNCH_CHECK();
     int32_t nredo = 0;
+    unsigned int err_bits = 0;
     UMAPB_CUDA(cudaMemcpyAsync(&nredo, redo_count.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaMemcpyAsync(&err_bits, tc_err.get(), sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
     UMAPB_SYNC(s);
     last_knn_redo_count() = nredo;
+    last_knn_tc_error() = static_cast<double>(bits_to_float(err_bits));
     if (nredo > 0) {
         std::vector<int32_t> rq(nredo);
         UMAPB_CUDA(cudaMemcpyAsync(rq.data(), redo.get(), nredo * sizeof(int32_t), cudaMemcpyDeviceToHost, s));

@@ -14,9 +14,11 @@
 //              of two TMEM accumulators (128 lanes x 128 FP32 columns each),
 //              tcgen05.commit to the ring's "empty" and the accumulator's
 //              "full" mbarriers; it also owns the TMEM allocation;
-//   warps 2-5  epilogue: tcgen05.ld of the accumulator rows (one query per
-//              thread), distance, and a sorted register list of the KCAP best
-//              (distance, index) candidates.
+//   warps 2-9  epilogue: tcgen05.ld of the accumulator rows (one query per
+//              thread, each row split between two warps by column halves), a
+//              one-compare-per-column screen against the current k-th
+//              distance, and sorted register lists of the KCAP best
+//              (distance, index) candidates, merged per row at the end.
 // Operands are K-major with the 128-byte swizzle (TMA box 128 rows x 32 FP32,
 // UMMA shared-memory descriptors with SBO = 1024 B), no cluster multicast.
 // Every mbarrier wait is bounded: on expiry the kernel records an error,
@@ -27,86 +29,26 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
+#include <cstring>
 #include <mutex>
 
 #include "stages.cuh"
+#include "tc_ptx.cuh"
 
 namespace umapb {
 
 namespace {
 
+using namespace tc;
+
 constexpr int TC_M = 128;         // queries per CTA
 constexpr int TC_N = 128;         // references per tile
 constexpr int TC_KCHUNK = 32;     // FP32 elements per 128-byte swizzle row
 constexpr int TC_STAGES = 2;
-constexpr int TC_THREADS = 192;   // 6 warps
+constexpr int TC_EPI_WARPS = 8;
+constexpr int TC_THREADS = 64 + 32 * TC_EPI_WARPS;   // producer, MMA, 8 epilogue warps
 constexpr uint32_t TC_TMEM_COLS = 256;   // two 128-column accumulators
-constexpr long long WAIT_LIMIT = 1ll << 26;
-
-// ------------------------------------------------------------ PTX helpers --
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Bounded wait; returns false (and raises the abort flag) on expiry or abort.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* err) {
-    for (long long i = 0; i < WAIT_LIMIT; ++i) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if (*abort_flag) return false;
-        if (i > 64) __nanosleep(32);
-    }
-    *abort_flag = 1;
-    atomicExch(err, DEV_TIMEOUT);
-    return false;
-}
-
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-            smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-// K-major, 128-byte swizzled operand: rows of 128 B, 8-row atoms of 1024 B.
-__device__ __forceinline__ uint64_t smem_desc(const void* p) {
-    const uint64_t addr = smem_u32(p);
-    uint64_t d = 0;
-    d |= (addr >> 4) & 0x3FFFull;               // start address
-    d |= uint64_t(1) << 16;                     // leading byte offset (unused for swizzled K-major)
-    d |= uint64_t(1024 >> 4) << 32;             // stride byte offset: 8 rows x 128 B
-    d |= uint64_t(1) << 46;                     // descriptor version (sm_100)
-    d |= uint64_t(2) << 61;                     // layout: 128-byte swizzle
-    return d;
-}
 
 // Instruction descriptor: D = F32, A = B = TF32, both K-major, M = 128, N = TC_N.
 constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | (uint32_t(TC_N >> 3) << 17) | (uint32_t(TC_M >> 4) << 24);
@@ -118,41 +60,6 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t a, uint64_t b
         "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
         "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate)
         : "memory");
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t* bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ void tmem_load32(uint32_t taddr, uint32_t (&r)[32]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-
-template <int KCAP>
-__device__ __forceinline__ void insert_sorted(float (&bd)[KCAP], int (&bi)[KCAP], float cd, int ci) {
-#pragma unroll
-    for (int i = KCAP - 1; i > 0; --i) {
-        if (cd < bd[i - 1]) {
-            bd[i] = bd[i - 1];
-            bi[i] = bi[i - 1];
-        } else if (cd < bd[i]) {
-            bd[i] = cd;
-            bi[i] = ci;
-        }
-    }
-    if (cd < bd[0]) {
-        bd[0] = cd;
-        bi[0] = ci;
-    }
 }
 
 // ------------------------------------------------------------ prep kernel --
@@ -234,21 +141,6 @@ struct TcSmem {
     int abort_flag;
 };
 
-// Register-array element by a run-time index via a 5-level select tree
-// (keeps the array in registers; dynamic indexing would spill it).
-__device__ __forceinline__ float select32(const float (&v)[32], int i) {
-    float t16[16], t8[8], t4[4], t2[2];
-#pragma unroll
-    for (int j = 0; j < 16; ++j) t16[j] = (i & 16) ? v[j + 16] : v[j];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) t8[j] = (i & 8) ? t16[j + 8] : t16[j];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) t4[j] = (i & 4) ? t8[j + 4] : t8[j];
-#pragma unroll
-    for (int j = 0; j < 2; ++j) t2[j] = (i & 2) ? t4[j + 2] : t4[j];
-    return (i & 1) ? t2[1] : t2[0];
-}
-
 template <int KC, int KCAP>
 __global__ void __launch_bounds__(TC_THREADS, 1) knn_tc_kernel(const __grid_constant__ CUtensorMap map_ahi,
                                                                const __grid_constant__ CUtensorMap map_alo,
@@ -292,7 +184,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_tc_kernel(const __grid_cons
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&sm.tmem_full[b], 1);
-            mbar_init(&sm.tmem_empty[b], 128);
+            mbar_init(&sm.tmem_empty[b], 32 * TC_EPI_WARPS);
         }
         mbar_init(&sm.a_full, 1);
         sm.abort_flag = 0;
@@ -364,8 +256,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_tc_kernel(const __grid_cons
             }
         }
     } else {
-        // epilogue: thread <-> query row (TMEM lane) 32 * (warp % 4) + lane
+        // Epilogue, 8 warps: warp w reads TMEM lanes 32 * (w % 4) .. + 31 (one
+        // query row per thread) and half (w - 2) / 4 of each tile's 128 columns;
+        // the two halves of a row keep separate candidate lists, merged at the end.
         const int quarter = warp & 3;
+        const int half = (warp - 2) >> 2;
         const int row = quarter * 32 + lane;
         const int q = q_base + row;
         const float qn = (q < q_limit) ? norms[q] : 0.0f;
@@ -377,43 +272,63 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_tc_kernel(const __grid_cons
             bi[i] = -1;
         }
         float thr = CUDART_INF_F;
+        // d2 = qn - 2 acc < thr  <=>  acc > (qn - thr) / 2; rounded down, so the
+        // screen admits every column the exact test below would
+        float athr = -CUDART_INF_F;
         for (int it = 0; it < n_tiles; ++it) {
             const int buf = it & 1;
             if (!mbar_wait(&sm.tmem_full[buf], (it >> 1) & 1, abort_flag, err)) break;
             tc_fence_after();
-            const uint32_t taddr = tmem_base + (uint32_t(quarter * 32) << 16) + buf * TC_N;
-            const bool diag = ((ref_tile0 + it) * TC_N == q_base);
+            const uint32_t taddr = tmem_base + (uint32_t(quarter * 32) << 16) + buf * TC_N + half * (TC_N / 2);
+            const int col0 = (ref_tile0 + it) * TC_N + half * (TC_N / 2);   // operand row of column 0
+            const bool diag = (col0 <= q && q < col0 + TC_N / 2);
             // reference columns at or past q_limit are padding (their distances
             // are finite, so they are masked out rather than left to lose)
-            const int valid = q_limit - (ref_tile0 + it) * TC_N;
+            const int valid = q_limit - col0;
 #pragma unroll 1
-            for (int ch = 0; ch < TC_N / 32; ++ch) {
+            for (int ch = 0; ch < TC_N / 64; ++ch) {
                 uint32_t r[32];
                 tmem_load32(taddr + ch * 32, r);
-                float d2[32];
                 uint32_t mask = 0;
 #pragma unroll
-                for (int i = 0; i < 32; ++i) {
-                    d2[i] = fmaf(-2.0f, __uint_as_float(r[i]), qn);
-                    mask |= (d2[i] < thr ? 1u : 0u) << i;
-                }
-                if (diag && ch == (row >> 5)) mask &= ~(1u << (row & 31));   // self
+                for (int i = 0; i < 32; ++i) mask |= (__uint_as_float(r[i]) > athr ? 1u : 0u) << i;
+                if (diag && (q - col0) / 32 == ch) mask &= ~(1u << ((q - col0) & 31));   // self
                 const int vc = valid - ch * 32;
                 if (vc < 32) mask &= (vc <= 0) ? 0u : ((1u << vc) - 1u);
                 while (mask) {   // rare: candidates better than the current k-th
                     const int i = __ffs(mask) - 1;
                     mask &= mask - 1;
-                    const float v = select32(d2, i);
+                    const float v = fmaf(-2.0f, __uint_as_float(select32(r, i)), qn);
                     if (v < thr) {
-                        insert_sorted<KCAP>(bd, bi, v, (ref_tile0 + it) * TC_N + ch * 32 + i + shift);
+                        insert_sorted<KCAP>(bd, bi, v, col0 + ch * 32 + i + shift);
                         thr = bd[KCAP - 1];
+                        athr = __fmul_rd(0.5f, __fsub_rd(qn, thr));
                     }
                 }
             }
             tc_fence_before();
             mbar_arrive(&sm.tmem_empty[buf]);
         }
-        if (q < q_limit) {
+        // Merge the halves through shared memory (the query tile's space: every
+        // MMA has completed once the last accumulator was seen full).
+        float* merge_d = &sm.a_hi[0][0];
+        int* merge_i = reinterpret_cast<int*>(&sm.a_lo[0][0]);
+        const bool ok = (*abort_flag == 0);
+        if (half == 1 && ok) {
+#pragma unroll
+            for (int i = 0; i < KCAP; ++i) {
+                merge_d[i * TC_M + row] = bd[i];
+                merge_i[i * TC_M + row] = bi[i];
+            }
+        }
+        asm volatile("bar.sync 1, %0;" ::"n"(TC_EPI_WARPS * 32) : "memory");
+        if (half == 0 && ok && q < q_limit) {
+            for (int i = 0; i < KCAP; ++i) {
+                const float v = merge_d[i * TC_M + row];
+                if (!(v < thr)) break;   // the partner's list is sorted
+                insert_sorted<KCAP>(bd, bi, v, merge_i[i * TC_M + row]);
+                thr = bd[KCAP - 1];
+            }
             const size_t out_row = static_cast<size_t>(q + shift);   // data row of this query
 #pragma unroll
             for (int i = 0; i < KCAP; ++i) {
@@ -524,11 +439,31 @@ void run_candidates(const float* data, int32_t n, int32_t dim, int kcap, int32_t
     // the operand arrays are released stream-ordered, after the kernel
 }
 
+// Operand type of the candidate search: FP16 pairs (knn_tc16.cu, default) or
+// TF32 pairs (this file); UMAPB_KNN_TC_KIND=tf32 selects the latter.
+bool use_f16_operands() {
+    const char* e = std::getenv("UMAPB_KNN_TC_KIND");   // read per search: tests switch it
+    return !(e && std::strcmp(e, "tf32") == 0);
+}
+
+bool tf32_supported(int32_t dim, int kcap) {
+    // the norm rides in one extra K column: dim + 1 columns in two 32-wide chunks
+    return dim >= 1 && dim + 1 <= 2 * TC_KCHUNK && (kcap == 16 || kcap == 24 || kcap == 32);
+}
+
 }  // namespace
 
-// The norm rides in one extra K column, so dim + 1 columns must fit in two 32-wide chunks.
 bool knn_tc_supported(int32_t dim, int kcap) {
-    return dim >= 1 && dim + 1 <= 2 * TC_KCHUNK && (kcap == 16 || kcap == 24 || kcap == 32);
+    return tf32_supported(dim, kcap) || (use_f16_operands() && knn_tc16_supported(dim, kcap));
+}
+
+// Scale for the FP16 search, or 0 when the TF32 search is to be used.
+static float f16_scale_or_zero(const float* data, size_t count, int32_t dim, int kcap, cudaStream_t s) {
+    if (!use_f16_operands() || !knn_tc16_supported(dim, kcap)) return 0.0f;
+    const float scale = knn_tc16_scale(data, count, s);
+    require(scale > 0.0f || tf32_supported(dim, kcap),
+            "tensor-core kNN: the data have no finite maximum in [2^-60, 2^60] for the FP16 search");
+    return scale;
 }
 
 // Candidate lists (KCAP per query, FP32 squared distances, ascending) from the
@@ -538,18 +473,28 @@ void knn_tc_candidates(const float* data, int32_t n, int32_t dim, int kcap, int3
                        float* norms_out, int* d_err, cudaStream_t s) {
     require(knn_tc_supported(dim, kcap), "tensor-core kNN: unsupported dimension or candidate count");
     const int32_t n_pad = ((n + TC_M - 1) / TC_M) * TC_M;
+    const float scale = f16_scale_or_zero(data, static_cast<size_t>(n) * dim, dim, kcap, s);
+    if (scale > 0.0f) {
+        const int rows = TC_M * knn_tc16_query_tiles(dim);
+        knn_tc16_run(data, n, dim, kcap, scale, n_pad, nullptr, (n_pad + rows - 1) / rows, nullptr, nullptr, cand_idx,
+                     cand_d2, norms_out, d_err, s);
+        return;
+    }
     run_candidates(data, n, dim, kcap, n_pad, nullptr, n_pad / TC_M, nullptr, nullptr, cand_idx, cand_d2, norms_out,
                    d_err, s);
 }
 
 // Batched: instance i is data rows [inst[i], inst[i + 1]); every query's
 // candidates come from its own instance only.  Each instance is placed at a
-// 128-row boundary of the operands, so a CTA's query tile and reference tiles
-// all belong to one instance.  Candidate indices are data rows.
+// 128-row boundary of the operands, so a CTA's query tiles and reference
+// tiles all belong to one instance (a CTA's last query tile may run past its
+// instance; those rows are masked).  Candidate indices are data rows.
 void knn_tc_candidates_batched(const float* data, const std::vector<int32_t>& inst, int32_t dim, int kcap,
                                int32_t* cand_idx, float* cand_d2, int* d_err, cudaStream_t s) {
     require(knn_tc_supported(dim, kcap), "tensor-core kNN: unsupported dimension or candidate count");
     const int ninst = static_cast<int>(inst.size()) - 1;
+    const float scale = f16_scale_or_zero(data, static_cast<size_t>(inst[ninst]) * dim, dim, kcap, s);
+    const int qt = scale > 0.0f ? knn_tc16_query_tiles(dim) : 1;
     std::vector<int32_t> pad_start(ninst + 1, 0);
     for (int i = 0; i < ninst; ++i) {
         const int32_t len = inst[i + 1] - inst[i];
@@ -563,7 +508,7 @@ void knn_tc_candidates_batched(const float* data, const std::vector<int32_t>& in
         const int32_t len = inst[i + 1] - inst[i];
         for (int32_t r = 0; r < len; ++r) src[pad_start[i] + r] = inst[i] + r;
         const int32_t tiles = (len + TC_M - 1) / TC_M;
-        for (int32_t t = 0; t < tiles; ++t) {
+        for (int32_t t = 0; t < tiles; t += qt) {
             tasks.push_back(make_int4(pad_start[i] + t * TC_M, pad_start[i] / TC_N, tiles, pad_start[i] + len));
             shifts.push_back(inst[i] - pad_start[i]);
         }
@@ -575,8 +520,13 @@ void knn_tc_candidates_batched(const float* data, const std::vector<int32_t>& in
     UMAPB_CUDA(cudaMemcpyAsync(d_src.get(), src.data(), src.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
     UMAPB_CUDA(cudaMemcpyAsync(d_tasks.get(), tasks.data(), tasks.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
     UMAPB_CUDA(cudaMemcpyAsync(d_shift.get(), shifts.data(), shifts.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-    run_candidates(data, inst[ninst], dim, kcap, n_pad, d_src.get(), static_cast<int32_t>(tasks.size()), d_tasks.get(),
-                   d_shift.get(), cand_idx, cand_d2, norms.get(), d_err, s);
+    if (scale > 0.0f) {
+        knn_tc16_run(data, inst[ninst], dim, kcap, scale, n_pad, d_src.get(), static_cast<int32_t>(tasks.size()),
+                     d_tasks.get(), d_shift.get(), cand_idx, cand_d2, norms.get(), d_err, s);
+    } else {
+        run_candidates(data, inst[ninst], dim, kcap, n_pad, d_src.get(), static_cast<int32_t>(tasks.size()),
+                       d_tasks.get(), d_shift.get(), cand_idx, cand_d2, norms.get(), d_err, s);
+    }
     UMAPB_SYNC(s);   // the host vectors above are the copies' sources
 }
 

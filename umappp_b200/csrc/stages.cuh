@@ -51,8 +51,20 @@ void knn_tc_candidates(const float* data, int32_t n, int32_t dim, int kcap, int3
 // Batched: instance i is data rows [inst[i], inst[i + 1]) (host vector).
 void knn_tc_candidates_batched(const float* data, const std::vector<int32_t>& inst, int32_t dim, int kcap,
                                int32_t* cand_idx, float* cand_d2, int* d_err, cudaStream_t s);
+// FP16-operand variant (knn_tc16.cu): power-of-two scale of the data (0 when
+// unusable), support test, query tiles per CTA, and the search itself.
+float knn_tc16_scale(const float* data, size_t count, cudaStream_t s);
+bool knn_tc16_supported(int32_t dim, int kcap);
+int knn_tc16_query_tiles(int32_t dim);
+void knn_tc16_run(const float* data, int32_t n, int32_t dim, int kcap, float scale, int32_t n_pad,
+                  const int32_t* pad_src, int32_t ctas, const int4* tasks, const int32_t* shifts, int32_t* cand_idx,
+                  float* cand_d2, float* norms_pad, int* d_err, cudaStream_t s);
 // Number of queries the last float kNN recomputed in FP64 (certainty check).
 int& last_knn_redo_count();
+// Largest |tensor-core FP32 squared distance - FP64 squared distance| /
+// (|q|^2 + max |r|^2) over the candidates of the last float kNN (0 without
+// the tensor-core search).
+double& last_knn_tc_error();
 
 // Exact kNN of every observation within its own instance (instance i is data
 // rows [inst[i], inst[i + 1]), host vector); indices are data rows.
