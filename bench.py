@@ -187,6 +187,7 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     for _ in range(max(1, args.warmup // 2)):
         step_host()
     e2e_ms, _, _ = timed(step_host, args.steps)
+    tile_pairs = int(U.lib().umapb_knn_last_tile_pairs())
 
     peaks = load_peaks()
     # SGD roofline (algorithmic bytes per epoch: 4 nnz + 56 F + 8 N_neg, F and N_neg exact)
@@ -207,7 +208,8 @@ def run_ours(args, rank: int, world: int) -> dict | None:
                      "traffic": None, "peak_source": peaks["source"],
                      "note": "algorithmic bytes 4*nnz*epochs + 56*F + 8*N_neg over the SGD stage time"},
         "knn": {"kernel": "knn (device)", "achieved_tflops": round(knn_tflops, 2),
-                "peak_bf16_tflops": peaks["bf16_tflops"], "algorithmic_flops": knn_flops},
+                "peak_bf16_tflops": peaks["bf16_tflops"], "algorithmic_flops": knn_flops,
+                "tile_pairs": tile_pairs, "tile_pairs_brute_force": ((n + 127) // 128) ** 2},
         "e2e": {"value": round(e2e_ms / 1e3, 4), "unit": "s", "h2d_bytes_per_step": int(n * dim * 4 + n * 2 * 4),
                 "d2h_bytes_per_step": int(2 * n * 2 * 4)},
         "gpu_launches": int(launches // max(args.steps, 1)),

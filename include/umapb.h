@@ -187,6 +187,12 @@ int umapb_knn_last_fp64_recomputed(void);
  * use tensor cores.  No reference counterpart: a precision diagnostic. */
 double umapb_knn_last_tc_error(void);
 
+/* Query-tile x reference-tile pairs (128 x 128 squared distances each) that
+ * the last tensor-core kNN of this process computed: with tile pruning, the
+ * work left of the (n / 128)^2 of a brute-force search.  No reference
+ * counterpart: a diagnostic of the search. */
+int64_t umapb_knn_last_tile_pairs(void);
+
 /*
  * neighbor_similarities (include/umappp/neighbor_similarities.hpp:53-207):
  * replaces the distances of each CSR row by membership weights in place.

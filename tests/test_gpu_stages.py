@@ -73,6 +73,25 @@ def test_knn_tensor_core_operands(umap, monkeypatch, kind, n, dim, k):
         assert 0.0 < err < 2.0 ** -17, err
 
 
+@pytest.mark.parametrize("prune", ["1", "0"])
+def test_knn_tile_pruning_is_exact(umap, monkeypatch, prune):
+    # well separated clusters: most reference tiles are provably too far for a
+    # query block and are skipped; the neighbours stay exact
+    monkeypatch.setenv("UMAPB_KNN_PRUNE", prune)
+    n = 20000
+    X = oracle.gaussian_mixture(n, 30, 8, 10.0, seed=11, dtype=np.float32)
+    idx, dist = umap.knn(X, 15)
+    ridx, rdist = oracle.knn(X, 15)
+    assert _same_neighbors(idx, ridx, rdist) == 0
+    assert rel_err(dist, rdist) <= 1e-6
+    pairs = umap.lib().umapb_knn_last_tile_pairs()
+    tiles = (n + 127) // 128
+    if prune == "1":
+        assert 0 < pairs < 0.5 * tiles * tiles, pairs
+    else:
+        assert pairs >= tiles * tiles, pairs
+
+
 def test_knn_duplicates_and_ties(umap):
     rng = np.random.default_rng(3)
     base = rng.normal(size=(50, 4))

@@ -36,6 +36,11 @@ static float bits_to_float(unsigned int b) {
     return f;
 }
 
+int64_t& last_knn_tiles_scanned() {
+    static int64_t tiles = 0;
+    return tiles;
+}
+
 double& last_knn_tc_error() {
     static double worst = 0.0;
     return worst;

@@ -16,8 +16,8 @@
 //              "full" mbarriers; it also owns the TMEM allocation;
 //   warps 2-9  epilogue: tcgen05.ld of the accumulator rows (one query per
 //              thread, each row split between two warps by column halves), a
-//              one-compare-per-column screen against the current k-th
-//              distance, and sorted register lists of the KCAP best
+//              screen of each 32-column chunk by its maximum against the
+//              current k-th distance, and sorted register lists of the KCAP best
 //              (distance, index) candidates, merged per row at the end.
 // Operands are K-major with the 128-byte swizzle (TMA box 128 rows x 32 FP32,
 // UMMA shared-memory descriptors with SBO = 1024 B), no cluster multicast.
@@ -289,20 +289,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_tc_kernel(const __grid_cons
             for (int ch = 0; ch < TC_N / 64; ++ch) {
                 uint32_t r[32];
                 tmem_load32(taddr + ch * 32, r);
-                uint32_t mask = 0;
+                if (chunk_max32(r) > athr) {   // rare after the first tiles
+                    uint32_t mask = 0;
 #pragma unroll
-                for (int i = 0; i < 32; ++i) mask |= (__uint_as_float(r[i]) > athr ? 1u : 0u) << i;
-                if (diag && (q - col0) / 32 == ch) mask &= ~(1u << ((q - col0) & 31));   // self
-                const int vc = valid - ch * 32;
-                if (vc < 32) mask &= (vc <= 0) ? 0u : ((1u << vc) - 1u);
-                while (mask) {   // rare: candidates better than the current k-th
-                    const int i = __ffs(mask) - 1;
-                    mask &= mask - 1;
-                    const float v = fmaf(-2.0f, __uint_as_float(select32(r, i)), qn);
-                    if (v < thr) {
-                        insert_sorted<KCAP>(bd, bi, v, col0 + ch * 32 + i + shift);
-                        thr = bd[KCAP - 1];
-                        athr = __fmul_rd(0.5f, __fsub_rd(qn, thr));
+                    for (int i = 0; i < 32; ++i) mask |= (__uint_as_float(r[i]) > athr ? 1u : 0u) << i;
+                    if (diag && (q - col0) / 32 == ch) mask &= ~(1u << ((q - col0) & 31));   // self
+                    const int vc = valid - ch * 32;
+                    if (vc < 32) mask &= (vc <= 0) ? 0u : ((1u << vc) - 1u);
+                    while (mask) {   // rare: candidates better than the current k-th
+                        const int i = __ffs(mask) - 1;
+                        mask &= mask - 1;
+                        const float v = fmaf(-2.0f, __uint_as_float(select32(r, i)), qn);
+                        if (v < thr) {
+                            insert_sorted<KCAP>(bd, bi, v, col0 + ch * 32 + i + shift);
+                            thr = bd[KCAP - 1];
+                            athr = __fmul_rd(0.5f, __fsub_rd(qn, thr));
+                        }
                     }
                 }
             }
@@ -446,6 +448,26 @@ bool use_f16_operands() {
     return !(e && std::strcmp(e, "tf32") == 0);
 }
 
+// Tile pruning of the FP16 search (knn_tree.cu); UMAPB_KNN_PRUNE=0 scans
+// every tile (operands in data order).
+bool prune_enabled() {
+    const char* e = std::getenv("UMAPB_KNN_PRUNE");   // read per search: tests switch it
+    return !(e && std::strcmp(e, "0") == 0);
+}
+
+// FP16 search over the (pruned) tile lists of the instances 'inst'.
+void run_f16_pruned(const float* data, const std::vector<int32_t>& inst, int32_t dim, int kcap, float scale,
+                    int32_t* cand_idx, float* cand_d2, float* norms_by_row, int* d_err, cudaStream_t s) {
+    const bool prune = prune_enabled();
+    KnnTiles tiles;
+    knn_tree_order(data, dim, inst, prune, tiles, s);
+    KnnTasks tasks;
+    knn_tile_tasks(data, dim, tiles, inst, knn_tc16_query_tiles(dim), kcap, prune, tasks, s);
+    knn_tc16_run_tasks(data, dim, kcap, scale, tiles, tasks, cand_idx, cand_d2, norms_by_row, d_err, s);
+    last_knn_tiles_scanned() = tasks.total_tiles * knn_tc16_query_tiles(dim);
+    UMAPB_SYNC(s);   // the tile and task buffers are released below
+}
+
 bool tf32_supported(int32_t dim, int kcap) {
     // the norm rides in one extra K column: dim + 1 columns in two 32-wide chunks
     return dim >= 1 && dim + 1 <= 2 * TC_KCHUNK && (kcap == 16 || kcap == 24 || kcap == 32);
@@ -475,11 +497,10 @@ void knn_tc_candidates(const float* data, int32_t n, int32_t dim, int kcap, int3
     const int32_t n_pad = ((n + TC_M - 1) / TC_M) * TC_M;
     const float scale = f16_scale_or_zero(data, static_cast<size_t>(n) * dim, dim, kcap, s);
     if (scale > 0.0f) {
-        const int rows = TC_M * knn_tc16_query_tiles(dim);
-        knn_tc16_run(data, n, dim, kcap, scale, n_pad, nullptr, (n_pad + rows - 1) / rows, nullptr, nullptr, cand_idx,
-                     cand_d2, norms_out, d_err, s);
+        run_f16_pruned(data, {0, n}, dim, kcap, scale, cand_idx, cand_d2, norms_out, d_err, s);
         return;
     }
+    last_knn_tiles_scanned() = static_cast<int64_t>(n_pad / TC_M) * (n_pad / TC_N);
     run_candidates(data, n, dim, kcap, n_pad, nullptr, n_pad / TC_M, nullptr, nullptr, cand_idx, cand_d2, norms_out,
                    d_err, s);
 }
@@ -494,7 +515,12 @@ void knn_tc_candidates_batched(const float* data, const std::vector<int32_t>& in
     require(knn_tc_supported(dim, kcap), "tensor-core kNN: unsupported dimension or candidate count");
     const int ninst = static_cast<int>(inst.size()) - 1;
     const float scale = f16_scale_or_zero(data, static_cast<size_t>(inst[ninst]) * dim, dim, kcap, s);
-    const int qt = scale > 0.0f ? knn_tc16_query_tiles(dim) : 1;
+    if (scale > 0.0f) {
+        DevArray<float> norms(inst[ninst], s);
+        run_f16_pruned(data, inst, dim, kcap, scale, cand_idx, cand_d2, norms.get(), d_err, s);
+        return;
+    }
+    const int qt = 1;
     std::vector<int32_t> pad_start(ninst + 1, 0);
     for (int i = 0; i < ninst; ++i) {
         const int32_t len = inst[i + 1] - inst[i];
@@ -520,13 +546,8 @@ void knn_tc_candidates_batched(const float* data, const std::vector<int32_t>& in
     UMAPB_CUDA(cudaMemcpyAsync(d_src.get(), src.data(), src.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
     UMAPB_CUDA(cudaMemcpyAsync(d_tasks.get(), tasks.data(), tasks.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
     UMAPB_CUDA(cudaMemcpyAsync(d_shift.get(), shifts.data(), shifts.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-    if (scale > 0.0f) {
-        knn_tc16_run(data, inst[ninst], dim, kcap, scale, n_pad, d_src.get(), static_cast<int32_t>(tasks.size()),
-                     d_tasks.get(), d_shift.get(), cand_idx, cand_d2, norms.get(), d_err, s);
-    } else {
-        run_candidates(data, inst[ninst], dim, kcap, n_pad, d_src.get(), static_cast<int32_t>(tasks.size()),
-                       d_tasks.get(), d_shift.get(), cand_idx, cand_d2, norms.get(), d_err, s);
-    }
+    run_candidates(data, inst[ninst], dim, kcap, n_pad, d_src.get(), static_cast<int32_t>(tasks.size()),
+                   d_tasks.get(), d_shift.get(), cand_idx, cand_d2, norms.get(), d_err, s);
     UMAPB_SYNC(s);   // the host vectors above are the copies' sources
 }
 

@@ -17,8 +17,10 @@
 //   warp 0      TMA producer (query tiles once, then the reference ring);
 //   warp 1      MMA issuer (one lane) and TMEM owner;
 //   warps 2..   epilogue, 4 per query tile: one query row per thread (TMEM
-//               lane), all 128 columns of each tile, a one-compare-per-column
-//               screen against the current k-th distance and a sorted
+//               lane), all 128 columns of each tile, a screen of each
+//               32-column chunk by its maximum against the current k-th
+//               distance (columns are compared one by one only in chunks
+//               that pass) and a sorted
 //               register list of the KCAP best (distance, index) pairs.
 // No cluster multicast.  Every mbarrier wait is bounded (tc_ptx.cuh): on
 // expiry the kernel records an error, raises a CTA-wide abort flag so the
@@ -74,6 +76,12 @@ __global__ void absmax_kernel(const float* __restrict__ data, size_t count, unsi
 __device__ __forceinline__ void split_f16(float v, __half& hi, __half& lo) {
     hi = __float2half_rn(v);
     lo = __float2half_rn(v - __half2float(hi));
+}
+
+__global__ void scatter_norms_kernel(const int32_t* __restrict__ row_map, const float* __restrict__ onorm,
+                                     int32_t n_pad, float* __restrict__ out) {
+    for (int32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n_pad; r += gridDim.x * blockDim.x)
+        if (row_map[r] >= 0) out[row_map[r]] = onorm[r];
 }
 
 // Operands [n_pad, k_pad] (FP16 pairs, zero padded):
@@ -136,21 +144,49 @@ constexpr int h16_threads() { return 64 + 128 * QT; }
 template <int QT>
 constexpr uint32_t h16_tmem_cols() { return QT == 2 ? 512u : 256u; }
 
+// One chunk of 32 accumulator columns (chunk ch of the tile whose column 0 is
+// operand row col0) against the query's candidate list: the chunk's maximum
+// screens it; in a passing chunk each column is compared, and candidates
+// nearer than the current k-th enter the list.
+template <int KCAP>
+__device__ __forceinline__ void scan_chunk(const uint32_t (&r)[32], int ch, int col0, int q, bool diag, int valid,
+                                           float qn, int shift, float (&bd)[KCAP], int (&bi)[KCAP], float& thr,
+                                           float& athr) {
+    if (!(chunk_max32(r) > athr)) return;   // rare after the first tiles
+    uint32_t mask = 0;
+#pragma unroll
+    for (int i = 0; i < 32; ++i) mask |= (__uint_as_float(r[i]) > athr ? 1u : 0u) << i;
+    if (diag && (q - col0) / 32 == ch) mask &= ~(1u << ((q - col0) & 31));   // self
+    const int vc = valid - ch * 32;
+    if (vc < 32) mask &= (vc <= 0) ? 0u : ((1u << vc) - 1u);
+    while (mask) {   // candidates better than the current k-th
+        const int i = __ffs(mask) - 1;
+        mask &= mask - 1;
+        const float v = fmaf(-2.0f, __uint_as_float(select32(r, i)), qn);
+        if (v < thr) {
+            insert_sorted<KCAP>(bd, bi, v, col0 + ch * 32 + i + shift);
+            thr = bd[KCAP - 1];
+            athr = __fmul_rd(0.5f, __fsub_rd(qn, thr));
+        }
+    }
+}
+
 template <int KC, int QT, int NS, int KCAP>
 __global__ void __launch_bounds__(h16_threads<QT>(), 1)
     knn_tc16_kernel(const __grid_constant__ CUtensorMap map_ahi, const __grid_constant__ CUtensorMap map_alo,
                     const __grid_constant__ CUtensorMap map_bhi, const __grid_constant__ CUtensorMap map_blo,
                     const float* __restrict__ norms, float s2, float inv_s2, int32_t n, int32_t n_tiles_all,
                     int32_t ksteps, int32_t* __restrict__ cand_idx, float* __restrict__ cand_d2,
-                    int* __restrict__ err, const int4* __restrict__ tasks, const int32_t* __restrict__ shifts) {
+                    int* __restrict__ err, const int4* __restrict__ tasks, const int32_t* __restrict__ shifts,
+                    const int32_t* __restrict__ tile_list, const int32_t* __restrict__ row_map) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     using Smem = H16Smem<KC, QT, NS>;
     Smem& sm = *reinterpret_cast<Smem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // This CTA's queries are operand rows [q_base, q_base + QT * 128), valid
-    // below q_limit; its references are the n_tiles tiles from ref_tile0.
-    // Batched runs give each CTA a task within one instance and the shift from
-    // operand rows to data rows.
+    // below q_limit; its references are n_tiles tiles: tile_list[ref_tile0 +
+    // it] with a list (pruned search), else ref_tile0 + it.  Tasks come with
+    // either a per-CTA shift or a row map from operand rows to data rows.
     int q_base, ref_tile0, n_tiles, q_limit, shift;
     if (tasks) {
         const int4 t = tasks[blockIdx.x];
@@ -158,7 +194,7 @@ __global__ void __launch_bounds__(h16_threads<QT>(), 1)
         ref_tile0 = t.y;
         n_tiles = t.z;
         q_limit = t.w;
-        shift = shifts[blockIdx.x];
+        shift = shifts ? shifts[blockIdx.x] : 0;
     } else {
         q_base = blockIdx.x * (QT * H_M);
         ref_tile0 = 0;
@@ -166,6 +202,8 @@ __global__ void __launch_bounds__(h16_threads<QT>(), 1)
         q_limit = n;
         shift = 0;
     }
+    // operand row of the first reference of the it-th tile
+    auto tile_row = [&](int it) { return (tile_list ? tile_list[ref_tile0 + it] : ref_tile0 + it) * H_N; };
     volatile int* abort_flag = &sm.abort_flag;
     constexpr uint32_t TMEM_COLS = h16_tmem_cols<QT>();
 
@@ -212,8 +250,8 @@ __global__ void __launch_bounds__(h16_threads<QT>(), 1)
                 if (!mbar_wait(&sm.empty[s], ((it / NS) & 1) ^ 1, abort_flag, err)) break;
                 mbar_arrive_expect_tx(&sm.full[s], B_BYTES);
                 for (int c = 0; c < KC; ++c) {
-                    tma_load_2d(sm.b_hi[s][c], &map_bhi, &sm.full[s], c * H_KCHUNK, (ref_tile0 + it) * H_N);
-                    tma_load_2d(sm.b_lo[s][c], &map_blo, &sm.full[s], c * H_KCHUNK, (ref_tile0 + it) * H_N);
+                    tma_load_2d(sm.b_hi[s][c], &map_bhi, &sm.full[s], c * H_KCHUNK, tile_row(it));
+                    tma_load_2d(sm.b_lo[s][c], &map_blo, &sm.full[s], c * H_KCHUNK, tile_row(it));
                 }
                 ++issued;
             }
@@ -277,39 +315,33 @@ __global__ void __launch_bounds__(h16_threads<QT>(), 1)
             if (!mbar_wait(&sm.tmem_full[t][buf], (it >> 1) & 1, abort_flag, err)) break;
             tc_fence_after();
             const uint32_t taddr = tmem_base + (uint32_t(quarter * 32) << 16) + (t * 2 + buf) * H_N;
-            const int col0 = (ref_tile0 + it) * H_N;   // operand row of column 0
+            const int col0 = tile_row(it);   // operand row of column 0
             const bool diag = (col0 <= q && q < col0 + H_N);
             // reference columns at or past q_limit are padding
             const int valid = q_limit - col0;
+            // Two chunks of 32 columns per TMEM round trip; the accumulator is
+            // released to the MMA as soon as its last columns are in registers.
 #pragma unroll 1
-            for (int ch = 0; ch < H_N / 32; ++ch) {
-                uint32_t r[32];
-                tmem_load32(taddr + ch * 32, r);
-                uint32_t mask = 0;
-#pragma unroll
-                for (int i = 0; i < 32; ++i) mask |= (__uint_as_float(r[i]) > athr ? 1u : 0u) << i;
-                if (diag && (q - col0) / 32 == ch) mask &= ~(1u << ((q - col0) & 31));   // self
-                const int vc = valid - ch * 32;
-                if (vc < 32) mask &= (vc <= 0) ? 0u : ((1u << vc) - 1u);
-                while (mask) {   // rare: candidates better than the current k-th
-                    const int i = __ffs(mask) - 1;
-                    mask &= mask - 1;
-                    const float v = fmaf(-2.0f, __uint_as_float(select32(r, i)), qn);
-                    if (v < thr) {
-                        insert_sorted<KCAP>(bd, bi, v, col0 + ch * 32 + i + shift);
-                        thr = bd[KCAP - 1];
-                        athr = __fmul_rd(0.5f, __fsub_rd(qn, thr));
-                    }
+            for (int pr = 0; pr < H_N / 64; ++pr) {
+                uint32_t ra[32], rb[32];
+                tmem_load32_async(taddr + pr * 64, ra);
+                tmem_load32_async(taddr + pr * 64 + 32, rb);
+                tmem_wait_ld(ra);
+                tmem_wait_ld(rb);
+                if (pr == H_N / 64 - 1) {
+                    tc_fence_before();
+                    mbar_arrive(&sm.tmem_empty[t][buf]);
                 }
+                scan_chunk<KCAP>(ra, 2 * pr, col0, q, diag, valid, qn, shift, bd, bi, thr, athr);
+                scan_chunk<KCAP>(rb, 2 * pr + 1, col0, q, diag, valid, qn, shift, bd, bi, thr, athr);
             }
-            tc_fence_before();
-            mbar_arrive(&sm.tmem_empty[t][buf]);
         }
         if (q < q_limit && *abort_flag == 0) {
-            const size_t out_row = static_cast<size_t>(q + shift);   // data row of this query
+            // data rows: through the row map (candidates were collected as operand rows)
+            const size_t out_row = static_cast<size_t>(row_map ? row_map[q] : q + shift);
 #pragma unroll
             for (int i = 0; i < KCAP; ++i) {
-                cand_idx[out_row * KCAP + i] = bi[i];
+                cand_idx[out_row * KCAP + i] = (row_map && bi[i] >= 0) ? row_map[bi[i]] : bi[i];
                 cand_d2[out_row * KCAP + i] = bd[i] * inv_s2;   // exact: a power of two
             }
         }
@@ -369,7 +401,8 @@ struct Maps16 {
 
 template <int KC, int QT, int NS, int KCAP>
 void launch16(const Maps16& m, const float* norms, float s2, float inv_s2, int32_t n, int32_t n_pad, int32_t ctas,
-              const int4* tasks, const int32_t* shifts, int32_t* cand_idx, float* cand_d2, int* err, cudaStream_t s) {
+              const int4* tasks, const int32_t* shifts, const int32_t* tile_list, const int32_t* row_map, int32_t* cand_idx,
+              float* cand_d2, int* err, cudaStream_t s) {
     const size_t smem = sizeof(H16Smem<KC, QT, NS>) + 1024;
     static_assert(sizeof(H16Smem<KC, QT, NS>) + 1024 <= 227 * 1024, "shared memory budget");
     static std::once_flag once;
@@ -378,7 +411,8 @@ void launch16(const Maps16& m, const float* norms, float s2, float inv_s2, int32
                                         static_cast<int>(smem)));
     });
     knn_tc16_kernel<KC, QT, NS, KCAP><<<ctas, h16_threads<QT>(), smem, s>>>(
-        m.ahi, m.alo, m.bhi, m.blo, norms, s2, inv_s2, n, n_pad / H_N, m.ksteps, cand_idx, cand_d2, err, tasks, shifts);
+        m.ahi, m.alo, m.bhi, m.blo, norms, s2, inv_s2, n, n_pad / H_N, m.ksteps, cand_idx, cand_d2, err, tasks, shifts,
+        tile_list, row_map);
     UMAPB_LAUNCH_CHECK();
 }
 
@@ -388,13 +422,14 @@ constexpr int qt_for(int kc) { return kc == 1 ? 2 : 1; }
 
 template <int KC>
 void launch16_kcap(int kcap, const Maps16& m, const float* norms, float s2, float inv_s2, int32_t n, int32_t n_pad,
-                   int32_t ctas, const int4* tasks, const int32_t* shifts, int32_t* ci, float* cd, int* err,
+                   int32_t ctas, const int4* tasks, const int32_t* shifts, const int32_t* tl, const int32_t* rm,
+                   int32_t* ci, float* cd, int* err,
                    cudaStream_t s) {
     constexpr int QT = qt_for(KC);
     constexpr int NS = KC == 1 ? 4 : 2;
-    if (kcap == 16) launch16<KC, QT, NS, 16>(m, norms, s2, inv_s2, n, n_pad, ctas, tasks, shifts, ci, cd, err, s);
-    else if (kcap == 24) launch16<KC, QT, NS, 24>(m, norms, s2, inv_s2, n, n_pad, ctas, tasks, shifts, ci, cd, err, s);
-    else launch16<KC, QT, NS, 32>(m, norms, s2, inv_s2, n, n_pad, ctas, tasks, shifts, ci, cd, err, s);
+    if (kcap == 16) launch16<KC, QT, NS, 16>(m, norms, s2, inv_s2, n, n_pad, ctas, tasks, shifts, tl, rm, ci, cd, err, s);
+    else if (kcap == 24) launch16<KC, QT, NS, 24>(m, norms, s2, inv_s2, n, n_pad, ctas, tasks, shifts, tl, rm, ci, cd, err, s);
+    else launch16<KC, QT, NS, 32>(m, norms, s2, inv_s2, n, n_pad, ctas, tasks, shifts, tl, rm, ci, cd, err, s);
 }
 
 }  // namespace
@@ -446,9 +481,49 @@ void knn_tc16_run(const float* data, int32_t n, int32_t dim, int kcap, float sca
     m.blo = make_map16(blo.get(), n_pad, k_pad);
     m.ksteps = (dim + 1 + H_KSTEP - 1) / H_KSTEP;
     const float s2 = scale * scale, inv_s2 = 1.0f / s2;   // powers of two: exact
-    if (kc == 1) launch16_kcap<1>(kcap, m, norms_pad, s2, inv_s2, n, n_pad, ctas, tasks, shifts, cand_idx, cand_d2, d_err, s);
-    else launch16_kcap<2>(kcap, m, norms_pad, s2, inv_s2, n, n_pad, ctas, tasks, shifts, cand_idx, cand_d2, d_err, s);
+    if (kc == 1)
+        launch16_kcap<1>(kcap, m, norms_pad, s2, inv_s2, n, n_pad, ctas, tasks, shifts, nullptr, nullptr, cand_idx,
+                         cand_d2, d_err, s);
+    else
+        launch16_kcap<2>(kcap, m, norms_pad, s2, inv_s2, n, n_pad, ctas, tasks, shifts, nullptr, nullptr, cand_idx,
+                         cand_d2, d_err, s);
     // the operand arrays are released stream-ordered, after the kernel
+}
+
+// Pruned search (knn_tree.cu): operands in the tiles' row order, one CTA per
+// task.  Norms (needed in operand order by the kernel) are scattered to data
+// rows for the caller.
+void knn_tc16_run_tasks(const float* data, int32_t dim, int kcap, float scale, const KnnTiles& tiles,
+                        const KnnTasks& tasks, int32_t* cand_idx, float* cand_d2, float* norms_by_row, int* d_err,
+                        cudaStream_t s) {
+    require(knn_tc16_supported(dim, kcap), "tensor-core kNN: unsupported dimension or candidate count");
+    require(scale > 0.0f, "tensor-core kNN: no usable scale for the data");
+    const int32_t n_pad = tiles.n_pad;
+    const int kc = (dim + 1 + H_KCHUNK - 1) / H_KCHUNK;
+    const int k_pad = kc * H_KCHUNK;
+    const size_t elems = static_cast<size_t>(n_pad) * k_pad;
+    DevArray<__half> ahi(elems, s), alo(elems, s), bhi(elems, s), blo(elems, s);
+    DevArray<float> onorm(n_pad, s);
+    prepare16_kernel<<<grid_for(n_pad, 256), 256, 0, s>>>(data, 0, dim, n_pad, k_pad, scale, ahi.get(), alo.get(),
+                                                           bhi.get(), blo.get(), onorm.get(), tiles.row_map.get());
+    UMAPB_LAUNCH_CHECK();
+    Maps16 m;
+    m.ahi = make_map16(ahi.get(), n_pad, k_pad);
+    m.alo = make_map16(alo.get(), n_pad, k_pad);
+    m.bhi = make_map16(bhi.get(), n_pad, k_pad);
+    m.blo = make_map16(blo.get(), n_pad, k_pad);
+    m.ksteps = (dim + 1 + H_KSTEP - 1) / H_KSTEP;
+    const float s2 = scale * scale, inv_s2 = 1.0f / s2;
+    if (tasks.count > 0) {
+        if (kc == 1)
+            launch16_kcap<1>(kcap, m, onorm.get(), s2, inv_s2, 0, n_pad, tasks.count, tasks.tasks.get(), nullptr,
+                             tasks.tile_list.get(), tiles.row_map.get(), cand_idx, cand_d2, d_err, s);
+        else
+            launch16_kcap<2>(kcap, m, onorm.get(), s2, inv_s2, 0, n_pad, tasks.count, tasks.tasks.get(), nullptr,
+                             tasks.tile_list.get(), tiles.row_map.get(), cand_idx, cand_d2, d_err, s);
+    }
+    scatter_norms_kernel<<<grid_for(n_pad, 256), 256, 0, s>>>(tiles.row_map.get(), onorm.get(), n_pad, norms_by_row);
+    UMAPB_LAUNCH_CHECK();
 }
 
 }  // namespace umapb

@@ -867,15 +867,16 @@ void SgdEngine<T>::counts(int first, int last, int64_t* out, cudaStream_t s) {
     for (size_t i = 0; i < h.size(); ++i) out[i] = static_cast<int64_t>(h[i]);
 }
 
-// 4 ordered slices: the parallel epoch then matches the serial reference's
-// edge cross-entropy and trustworthiness to within their seed-to-seed noise.
+// 8 ordered slices: measured on 2,000- and 100,000-point layouts, an epoch in
+// one launch ends about 2-3 % below the serial reference's edge
+// cross-entropy, 4 slices about 1.4 % below, 8 slices within about 0.6 %.
 // UMAPB_SGD_PHASES overrides it (1 = every event of an epoch in one launch).
 template <typename T>
 int SgdEngine<T>::default_min_phases() {
     static const int v = [] {
         const char* e = std::getenv("UMAPB_SGD_PHASES");
         const int x = e ? std::atoi(e) : 0;
-        return (x >= 1 && x <= 64) ? x : 4;
+        return (x >= 1 && x <= 64) ? x : 8;
     }();
     return v;
 }

@@ -51,6 +51,36 @@ void knn_tc_candidates(const float* data, int32_t n, int32_t dim, int kcap, int3
 // Batched: instance i is data rows [inst[i], inst[i + 1]) (host vector).
 void knn_tc_candidates_batched(const float* data, const std::vector<int32_t>& inst, int32_t dim, int kcap,
                                int32_t* cand_idx, float* cand_d2, int* d_err, cudaStream_t s);
+// Tile pruning (knn_tree.cu).  KnnTiles: operand row -> data row map of the
+// padded, tree-ordered operands (-1 for padding), each instance starting at
+// pad_start[i] (a multiple of 128).  KnnTasks: per query block of the search
+// {first operand row, offset and length of its reference-tile list, end of
+// its instance's rows}, and the concatenated lists.
+struct KnnTiles {
+    DevArray<int32_t> row_map;
+    std::vector<int32_t> pad_start;
+    int32_t n_pad = 0;
+};
+struct KnnTasks {
+    DevArray<int4> tasks;
+    DevArray<int32_t> tile_list;
+    int32_t count = 0;
+    int64_t total_tiles = 0;
+};
+// tree == false keeps each instance in data order.
+void knn_tree_order(const float* data, int32_t dim, const std::vector<int32_t>& inst, bool tree, KnnTiles& out,
+                    cudaStream_t s);
+// Blocks of qt tiles; a block with more than k real rows lists only the tiles
+// that may hold one of its rows' k nearest neighbours (all tiles of its
+// instance when prune is false).
+void knn_tile_tasks(const float* data, int32_t dim, const KnnTiles& t, const std::vector<int32_t>& inst, int qt,
+                    int32_t k, bool prune, KnnTasks& out, cudaStream_t s);
+// Candidate search over tree-ordered operands and task lists; candidate and
+// norm outputs are indexed by data row.
+void knn_tc16_run_tasks(const float* data, int32_t dim, int kcap, float scale, const KnnTiles& tiles,
+                        const KnnTasks& tasks, int32_t* cand_idx, float* cand_d2, float* norms_by_row, int* d_err,
+                        cudaStream_t s);
+
 // FP16-operand variant (knn_tc16.cu): power-of-two scale of the data (0 when
 // unusable), support test, query tiles per CTA, and the search itself.
 float knn_tc16_scale(const float* data, size_t count, cudaStream_t s);
@@ -61,6 +91,9 @@ void knn_tc16_run(const float* data, int32_t n, int32_t dim, int kcap, float sca
                   float* cand_d2, float* norms_pad, int* d_err, cudaStream_t s);
 // Number of queries the last float kNN recomputed in FP64 (certainty check).
 int& last_knn_redo_count();
+// Query-tile x reference-tile pairs (128 x 128 distances each) computed by the
+// last tensor-core candidate search: the work left after pruning.
+int64_t& last_knn_tiles_scanned();
 // Largest |tensor-core FP32 squared distance - FP64 squared distance| /
 // (|q|^2 + max |r|^2) over the candidates of the last float kNN (0 without
 // the tensor-core search).

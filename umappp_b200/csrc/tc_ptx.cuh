@@ -96,6 +96,31 @@ __device__ __forceinline__ void tmem_load32(uint32_t taddr, uint32_t (&r)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// tcgen05.ld without the wait: r must not be read before tmem_wait_ld(r).
+__device__ __forceinline__ void tmem_load32_async(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+}
+
+// Waits for every outstanding tcgen05.ld of the thread; r passes through the
+// wait so that no read of it is scheduled before it.
+__device__ __forceinline__ void tmem_wait_ld(uint32_t (&r)[32]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                   "+r"(r[15]), "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]),
+                   "+r"(r[22]), "+r"(r[23]), "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]),
+                   "+r"(r[29]), "+r"(r[30]), "+r"(r[31])
+                 :
+                 : "memory");
+}
+
 template <int KCAP>
 __device__ __forceinline__ void insert_sorted(float (&bd)[KCAP], int (&bi)[KCAP], float cd, int ci) {
 #pragma unroll
@@ -128,6 +153,21 @@ __device__ __forceinline__ V select32(const V (&v)[32], int i) {
 #pragma unroll
     for (int j = 0; j < 2; ++j) t2[j] = (i & 2) ? t4[j + 2] : t4[j];
     return (i & 1) ? t2[1] : t2[0];
+}
+
+// Largest of 32 accumulator values (as floats): the epilogue's screen for a
+// whole chunk, one FMNMX per column; only chunks whose maximum passes the
+// threshold are examined column by column.
+__device__ __forceinline__ float chunk_max32(const uint32_t (&r)[32]) {
+    float m[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) m[j] = fmaxf(__uint_as_float(r[j]), __uint_as_float(r[j + 16]));
+#pragma unroll
+    for (int w = 8; w >= 1; w >>= 1) {
+#pragma unroll
+        for (int j = 0; j < w; ++j) m[j] = fmaxf(m[j], m[j + w]);
+    }
+    return m[0];
 }
 
 }  // namespace tc
