@@ -193,6 +193,11 @@ double umapb_knn_last_tc_error(void);
  * counterpart: a diagnostic of the search. */
 int64_t umapb_knn_last_tile_pairs(void);
 
+/* Device time in milliseconds of the last tensor-core candidate kernel
+ * (FP16 search) of this process, from CUDA events around its launch.  No
+ * reference counterpart: a measurement hook. */
+double umapb_knn_last_kernel_ms(void);
+
 /*
  * neighbor_similarities (include/umappp/neighbor_similarities.hpp:53-207):
  * replaces the distances of each CSR row by membership weights in place.

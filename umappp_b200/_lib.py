@@ -65,6 +65,7 @@ SIGNATURES = {
     "umapb_knn_last_fp64_recomputed": (_c_int, []),
     "umapb_knn_last_tc_error": (_c_dbl, []),
     "umapb_knn_last_tile_pairs": (_c_i64, []),
+    "umapb_knn_last_kernel_ms": (_c_dbl, []),
     "umapb_neighbor_similarities": (_c_int, [_c_int, _c_i32, _vp, _vp, _c_dbl, _c_dbl, _c_dbl, _c_int, _vp, _vp]),
     "umapb_combine_neighbor_sets": (_c_int, [_c_int, _c_i32, _vp, _vp, _vp, _c_dbl, _vp, _vp, _vp, _c_i64, _vp]),
     "umapb_similarities_to_epochs": (_c_int, [_c_int, _c_i32, _vp, _vp, _vp, _c_int, _c_dbl, _vp, _vp, _vp, _vp,

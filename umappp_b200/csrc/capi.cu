@@ -613,6 +613,8 @@ double umapb_knn_last_tc_error(void) { return last_knn_tc_error(); }
 
 int64_t umapb_knn_last_tile_pairs(void) { return last_knn_tiles_scanned(); }
 
+double umapb_knn_last_kernel_ms(void) { return last_knn_kernel_ms(); }
+
 int umapb_neighbor_similarities(int dtype, int32_t num_obs, const int64_t* row_ptr, void* distances,
                                 double local_connectivity, double bandwidth, double min_k_dist_scale, int use_newton,
                                 double* rho_out, double* sigma_out) {

@@ -41,6 +41,11 @@ int64_t& last_knn_tiles_scanned() {
     return tiles;
 }
 
+float& last_knn_kernel_ms() {
+    static float ms = 0.0f;
+    return ms;
+}
+
 double& last_knn_tc_error() {
     static double worst = 0.0;
     return worst;

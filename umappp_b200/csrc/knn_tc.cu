@@ -463,8 +463,9 @@ void run_f16_pruned(const float* data, const std::vector<int32_t>& inst, int32_t
     knn_tree_order(data, dim, inst, prune, tiles, s);
     KnnTasks tasks;
     knn_tile_tasks(data, dim, tiles, inst, knn_tc16_query_tiles(dim), kcap, prune, tasks, s);
-    knn_tc16_run_tasks(data, dim, kcap, scale, tiles, tasks, cand_idx, cand_d2, norms_by_row, d_err, s);
-    last_knn_tiles_scanned() = tasks.total_tiles * knn_tc16_query_tiles(dim);
+    knn_tc16_run_tasks(data, dim, kcap, scale, tiles, tasks, cand_idx, cand_d2, norms_by_row, d_err, s,
+                       &last_knn_kernel_ms());
+    last_knn_tiles_scanned() = tasks.total_tiles;
     UMAPB_SYNC(s);   // the tile and task buffers are released below
 }
 

@@ -86,7 +86,7 @@ __global__ void scatter_norms_kernel(const int32_t* __restrict__ row_map, const 
 
 // Operands [n_pad, k_pad] (FP16 pairs, zero padded):
 //   queries    A = [x s, 1]
-//   references B = [x s, -|x s|^2 / 2]
+//   references B = [x s, -|x s|^2 / 2]   (-60000 in the norm column of padding rows)
 // norms[i] = |x_i|^2 (FP64 sum rounded to FP32, unscaled; +inf for padding).
 // pad_src (batched runs) maps operand row i to its data row, or -1 for a
 // padding row; without it, rows below n are data rows.
@@ -112,9 +112,13 @@ __global__ void prepare16_kernel(const float* __restrict__ data, int32_t n, int3
             if (real && d < dim) split_f16(data[src * dim + d] * s, h, l);
             a_hi[row + d] = h;
             a_lo[row + d] = l;
-            if (d == dim && real) {
-                a_hi[row + d] = __float2half_rn(1.0f);
-                split_f16(static_cast<float>(-0.5 * nrm * s2), h, l);
+            if (d == dim) {
+                if (real) {
+                    a_hi[row + d] = __float2half_rn(1.0f);
+                    split_f16(static_cast<float>(-0.5 * nrm * s2), h, l);
+                } else {
+                    h = __float2half_rn(-60000.0f);   // padding reference: d2 beyond any candidate
+                }
             }
             b_hi[row + d] = h;
             b_lo[row + d] = l;
@@ -171,39 +175,57 @@ __device__ __forceinline__ void scan_chunk(const uint32_t (&r)[32], int ch, int 
     }
 }
 
+// Merged walk over the (ascending) reference-tile lists of a CTA's query
+// tiles: next() yields each tile of the union once, with the mask of the
+// query tiles whose lists hold it.
+template <int QT>
+struct ListWalk {
+    const int32_t* list[QT];
+    int32_t len[QT];
+    int32_t pos[QT];
+    __device__ __forceinline__ bool next(int32_t& tile, unsigned& mask) {
+        tile = INT32_MAX;
+#pragma unroll
+        for (int t = 0; t < QT; ++t)
+            if (pos[t] < len[t]) tile = min(tile, list[t][pos[t]]);
+        if (tile == INT32_MAX) return false;
+        mask = 0;
+#pragma unroll
+        for (int t = 0; t < QT; ++t)
+            if (pos[t] < len[t] && list[t][pos[t]] == tile) {
+                mask |= 1u << t;
+                ++pos[t];
+            }
+        return true;
+    }
+};
+
+// One CTA per task {first operand row, first query tile, query tiles, -}:
+// query tile t (rows q_base + 128 t ..) scans the reference tiles
+// tile_list[qlist_off[qt0 + t] .. + qlist_len[qt0 + t]).  Candidates are kept
+// as operand rows and written by data row through row_map (-1: padding row).
 template <int KC, int QT, int NS, int KCAP>
 __global__ void __launch_bounds__(h16_threads<QT>(), 1)
     knn_tc16_kernel(const __grid_constant__ CUtensorMap map_ahi, const __grid_constant__ CUtensorMap map_alo,
                     const __grid_constant__ CUtensorMap map_bhi, const __grid_constant__ CUtensorMap map_blo,
-                    const float* __restrict__ norms, float s2, float inv_s2, int32_t n, int32_t n_tiles_all,
-                    int32_t ksteps, int32_t* __restrict__ cand_idx, float* __restrict__ cand_d2,
-                    int* __restrict__ err, const int4* __restrict__ tasks, const int32_t* __restrict__ shifts,
-                    const int32_t* __restrict__ tile_list, const int32_t* __restrict__ row_map) {
+                    const float* __restrict__ norms, float s2, float inv_s2, int32_t ksteps,
+                    int32_t* __restrict__ cand_idx, float* __restrict__ cand_d2, int* __restrict__ err,
+                    const int4* __restrict__ tasks, const int64_t* __restrict__ qlist_off,
+                    const int32_t* __restrict__ qlist_len, const int32_t* __restrict__ tile_list,
+                    const int32_t* __restrict__ row_map) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     using Smem = H16Smem<KC, QT, NS>;
     Smem& sm = *reinterpret_cast<Smem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // This CTA's queries are operand rows [q_base, q_base + QT * 128), valid
-    // below q_limit; its references are n_tiles tiles: tile_list[ref_tile0 +
-    // it] with a list (pruned search), else ref_tile0 + it.  Tasks come with
-    // either a per-CTA shift or a row map from operand rows to data rows.
-    int q_base, ref_tile0, n_tiles, q_limit, shift;
-    if (tasks) {
-        const int4 t = tasks[blockIdx.x];
-        q_base = t.x;
-        ref_tile0 = t.y;
-        n_tiles = t.z;
-        q_limit = t.w;
-        shift = shifts ? shifts[blockIdx.x] : 0;
-    } else {
-        q_base = blockIdx.x * (QT * H_M);
-        ref_tile0 = 0;
-        n_tiles = n_tiles_all;
-        q_limit = n;
-        shift = 0;
+    const int4 task = tasks[blockIdx.x];
+    const int32_t q_base = task.x, qt0 = task.y, nq = task.z;
+    ListWalk<QT> walk;
+#pragma unroll
+    for (int t = 0; t < QT; ++t) {
+        walk.list[t] = tile_list + (t < nq ? qlist_off[qt0 + t] : 0);
+        walk.len[t] = t < nq ? qlist_len[qt0 + t] : 0;
+        walk.pos[t] = 0;
     }
-    // operand row of the first reference of the it-th tile
-    auto tile_row = [&](int it) { return (tile_list ? tile_list[ref_tile0 + it] : ref_tile0 + it) * H_N; };
     volatile int* abort_flag = &sm.abort_flag;
     constexpr uint32_t TMEM_COLS = h16_tmem_cols<QT>();
 
@@ -245,13 +267,15 @@ __global__ void __launch_bounds__(h16_threads<QT>(), 1)
                     tma_load_2d(sm.a_lo[t][c], &map_alo, &sm.a_full, c * H_KCHUNK, q_base + t * H_M);
                 }
             }
-            for (int it = 0; it < n_tiles; ++it) {
-                const int s = it % NS;
-                if (!mbar_wait(&sm.empty[s], ((it / NS) & 1) ^ 1, abort_flag, err)) break;
+            int32_t tile;
+            unsigned mask;
+            for (int u = 0; walk.next(tile, mask); ++u) {
+                const int s = u % NS;
+                if (!mbar_wait(&sm.empty[s], ((u / NS) & 1) ^ 1, abort_flag, err)) break;
                 mbar_arrive_expect_tx(&sm.full[s], B_BYTES);
                 for (int c = 0; c < KC; ++c) {
-                    tma_load_2d(sm.b_hi[s][c], &map_bhi, &sm.full[s], c * H_KCHUNK, tile_row(it));
-                    tma_load_2d(sm.b_lo[s][c], &map_blo, &sm.full[s], c * H_KCHUNK, tile_row(it));
+                    tma_load_2d(sm.b_hi[s][c], &map_bhi, &sm.full[s], c * H_KCHUNK, tile * H_N);
+                    tma_load_2d(sm.b_lo[s][c], &map_blo, &sm.full[s], c * H_KCHUNK, tile * H_N);
                 }
                 ++issued;
             }
@@ -259,12 +283,19 @@ __global__ void __launch_bounds__(h16_threads<QT>(), 1)
     } else if (warp == 1) {
         if (lane == 0 && mbar_wait(&sm.a_full, 0, abort_flag, err)) {
             bool ok = true;
-            for (int it = 0; it < n_tiles && ok; ++it) {
-                const int s = it % NS;
-                const int buf = it & 1;
-                if (!mbar_wait(&sm.full[s], (it / NS) & 1, abort_flag, err)) break;
+            int32_t used[QT];   // accumulator rounds of each query tile so far
+#pragma unroll
+            for (int t = 0; t < QT; ++t) used[t] = 0;
+            int32_t tile;
+            unsigned mask;
+            for (int u = 0; ok && walk.next(tile, mask); ++u) {
+                const int s = u % NS;
+                if (!mbar_wait(&sm.full[s], (u / NS) & 1, abort_flag, err)) break;
                 for (int t = 0; t < QT; ++t) {
-                    if (!mbar_wait(&sm.tmem_empty[t][buf], ((it >> 1) & 1) ^ 1, abort_flag, err)) {
+                    if (!(mask & (1u << t))) continue;
+                    const int c_t = used[t]++;
+                    const int buf = c_t & 1;
+                    if (!mbar_wait(&sm.tmem_empty[t][buf], ((c_t >> 1) & 1) ^ 1, abort_flag, err)) {
                         ok = false;
                         break;
                     }
@@ -298,7 +329,8 @@ __global__ void __launch_bounds__(h16_threads<QT>(), 1)
         const int quarter = warp & 3;
         const int row = quarter * 32 + lane;
         const int q = q_base + t * H_M + row;
-        const float qn = (q < q_limit) ? norms[q] * s2 : 0.0f;   // |q s|^2
+        const int32_t src = (t < nq) ? row_map[q] : -1;   // data row, -1: padding or no tile
+        const float qn = (src >= 0) ? norms[q] * s2 : 0.0f;   // |q s|^2
         float bd[KCAP];
         int bi[KCAP];
 #pragma unroll
@@ -310,15 +342,15 @@ __global__ void __launch_bounds__(h16_threads<QT>(), 1)
         // d2 = qn - 2 acc < thr  <=>  acc > (qn - thr) / 2; rounded down, so the
         // screen admits every column the exact test below would
         float athr = -CUDART_INF_F;
-        for (int it = 0; it < n_tiles; ++it) {
-            const int buf = it & 1;
-            if (!mbar_wait(&sm.tmem_full[t][buf], (it >> 1) & 1, abort_flag, err)) break;
+        const int32_t* my_list = walk.list[t];
+        const int32_t my_len = walk.len[t];
+        for (int c_t = 0; c_t < my_len; ++c_t) {
+            const int buf = c_t & 1;
+            if (!mbar_wait(&sm.tmem_full[t][buf], (c_t >> 1) & 1, abort_flag, err)) break;
             tc_fence_after();
             const uint32_t taddr = tmem_base + (uint32_t(quarter * 32) << 16) + (t * 2 + buf) * H_N;
-            const int col0 = tile_row(it);   // operand row of column 0
+            const int col0 = my_list[c_t] * H_N;   // operand row of column 0
             const bool diag = (col0 <= q && q < col0 + H_N);
-            // reference columns at or past q_limit are padding
-            const int valid = q_limit - col0;
             // Two chunks of 32 columns per TMEM round trip; the accumulator is
             // released to the MMA as soon as its last columns are in registers.
 #pragma unroll 1
@@ -332,16 +364,16 @@ __global__ void __launch_bounds__(h16_threads<QT>(), 1)
                     tc_fence_before();
                     mbar_arrive(&sm.tmem_empty[t][buf]);
                 }
-                scan_chunk<KCAP>(ra, 2 * pr, col0, q, diag, valid, qn, shift, bd, bi, thr, athr);
-                scan_chunk<KCAP>(rb, 2 * pr + 1, col0, q, diag, valid, qn, shift, bd, bi, thr, athr);
+                scan_chunk<KCAP>(ra, 2 * pr, col0, q, diag, H_N, qn, 0, bd, bi, thr, athr);
+                scan_chunk<KCAP>(rb, 2 * pr + 1, col0, q, diag, H_N, qn, 0, bd, bi, thr, athr);
             }
         }
-        if (q < q_limit && *abort_flag == 0) {
+        if (src >= 0 && *abort_flag == 0) {
             // data rows: through the row map (candidates were collected as operand rows)
-            const size_t out_row = static_cast<size_t>(row_map ? row_map[q] : q + shift);
+            const size_t out_row = static_cast<size_t>(src);
 #pragma unroll
             for (int i = 0; i < KCAP; ++i) {
-                cand_idx[out_row * KCAP + i] = (row_map && bi[i] >= 0) ? row_map[bi[i]] : bi[i];
+                cand_idx[out_row * KCAP + i] = bi[i] >= 0 ? row_map[bi[i]] : -1;
                 cand_d2[out_row * KCAP + i] = bd[i] * inv_s2;   // exact: a power of two
             }
         }
@@ -400,9 +432,8 @@ struct Maps16 {
 };
 
 template <int KC, int QT, int NS, int KCAP>
-void launch16(const Maps16& m, const float* norms, float s2, float inv_s2, int32_t n, int32_t n_pad, int32_t ctas,
-              const int4* tasks, const int32_t* shifts, const int32_t* tile_list, const int32_t* row_map, int32_t* cand_idx,
-              float* cand_d2, int* err, cudaStream_t s) {
+void launch16(const Maps16& m, const float* norms, float s2, float inv_s2, int32_t ctas, const KnnTasks& tk,
+              const int32_t* row_map, int32_t* cand_idx, float* cand_d2, int* err, cudaStream_t s) {
     const size_t smem = sizeof(H16Smem<KC, QT, NS>) + 1024;
     static_assert(sizeof(H16Smem<KC, QT, NS>) + 1024 <= 227 * 1024, "shared memory budget");
     static std::once_flag once;
@@ -411,8 +442,8 @@ void launch16(const Maps16& m, const float* norms, float s2, float inv_s2, int32
                                         static_cast<int>(smem)));
     });
     knn_tc16_kernel<KC, QT, NS, KCAP><<<ctas, h16_threads<QT>(), smem, s>>>(
-        m.ahi, m.alo, m.bhi, m.blo, norms, s2, inv_s2, n, n_pad / H_N, m.ksteps, cand_idx, cand_d2, err, tasks, shifts,
-        tile_list, row_map);
+        m.ahi, m.alo, m.bhi, m.blo, norms, s2, inv_s2, m.ksteps, cand_idx, cand_d2, err, tk.tasks.get(),
+        tk.qlist_off.get(), tk.qlist_len.get(), tk.tile_list.get(), row_map);
     UMAPB_LAUNCH_CHECK();
 }
 
@@ -421,15 +452,13 @@ void launch16(const Maps16& m, const float* norms, float s2, float inv_s2, int32
 constexpr int qt_for(int kc) { return kc == 1 ? 2 : 1; }
 
 template <int KC>
-void launch16_kcap(int kcap, const Maps16& m, const float* norms, float s2, float inv_s2, int32_t n, int32_t n_pad,
-                   int32_t ctas, const int4* tasks, const int32_t* shifts, const int32_t* tl, const int32_t* rm,
-                   int32_t* ci, float* cd, int* err,
-                   cudaStream_t s) {
+void launch16_kcap(int kcap, const Maps16& m, const float* norms, float s2, float inv_s2, int32_t ctas,
+                   const KnnTasks& tk, const int32_t* rm, int32_t* ci, float* cd, int* err, cudaStream_t s) {
     constexpr int QT = qt_for(KC);
     constexpr int NS = KC == 1 ? 4 : 2;
-    if (kcap == 16) launch16<KC, QT, NS, 16>(m, norms, s2, inv_s2, n, n_pad, ctas, tasks, shifts, tl, rm, ci, cd, err, s);
-    else if (kcap == 24) launch16<KC, QT, NS, 24>(m, norms, s2, inv_s2, n, n_pad, ctas, tasks, shifts, tl, rm, ci, cd, err, s);
-    else launch16<KC, QT, NS, 32>(m, norms, s2, inv_s2, n, n_pad, ctas, tasks, shifts, tl, rm, ci, cd, err, s);
+    if (kcap == 16) launch16<KC, QT, NS, 16>(m, norms, s2, inv_s2, ctas, tk, rm, ci, cd, err, s);
+    else if (kcap == 24) launch16<KC, QT, NS, 24>(m, norms, s2, inv_s2, ctas, tk, rm, ci, cd, err, s);
+    else launch16<KC, QT, NS, 32>(m, norms, s2, inv_s2, ctas, tk, rm, ci, cd, err, s);
 }
 
 }  // namespace
@@ -459,43 +488,12 @@ float knn_tc16_scale(const float* data, size_t count, cudaStream_t s) {
     return std::ldexp(1.0f, -e);
 }
 
-// Operands over n_pad rows (pad_src: operand row -> data row in batched runs)
-// scaled by 'scale' (knn_tc16_scale), and one launch over 'ctas' CTAs (tasks
-// as in the kernel).
-void knn_tc16_run(const float* data, int32_t n, int32_t dim, int kcap, float scale, int32_t n_pad,
-                  const int32_t* pad_src, int32_t ctas, const int4* tasks, const int32_t* shifts, int32_t* cand_idx,
-                  float* cand_d2, float* norms_pad, int* d_err, cudaStream_t s) {
-    require(knn_tc16_supported(dim, kcap), "tensor-core kNN: unsupported dimension or candidate count");
-    require(scale > 0.0f, "tensor-core kNN: no usable scale for the data");
-    const int kc = (dim + 1 + H_KCHUNK - 1) / H_KCHUNK;
-    const int k_pad = kc * H_KCHUNK;
-    const size_t elems = static_cast<size_t>(n_pad) * k_pad;
-    DevArray<__half> ahi(elems, s), alo(elems, s), bhi(elems, s), blo(elems, s);
-    prepare16_kernel<<<grid_for(n_pad, 256), 256, 0, s>>>(data, n, dim, n_pad, k_pad, scale, ahi.get(), alo.get(),
-                                                           bhi.get(), blo.get(), norms_pad, pad_src);
-    UMAPB_LAUNCH_CHECK();
-    Maps16 m;
-    m.ahi = make_map16(ahi.get(), n_pad, k_pad);
-    m.alo = make_map16(alo.get(), n_pad, k_pad);
-    m.bhi = make_map16(bhi.get(), n_pad, k_pad);
-    m.blo = make_map16(blo.get(), n_pad, k_pad);
-    m.ksteps = (dim + 1 + H_KSTEP - 1) / H_KSTEP;
-    const float s2 = scale * scale, inv_s2 = 1.0f / s2;   // powers of two: exact
-    if (kc == 1)
-        launch16_kcap<1>(kcap, m, norms_pad, s2, inv_s2, n, n_pad, ctas, tasks, shifts, nullptr, nullptr, cand_idx,
-                         cand_d2, d_err, s);
-    else
-        launch16_kcap<2>(kcap, m, norms_pad, s2, inv_s2, n, n_pad, ctas, tasks, shifts, nullptr, nullptr, cand_idx,
-                         cand_d2, d_err, s);
-    // the operand arrays are released stream-ordered, after the kernel
-}
-
 // Pruned search (knn_tree.cu): operands in the tiles' row order, one CTA per
 // task.  Norms (needed in operand order by the kernel) are scattered to data
 // rows for the caller.
 void knn_tc16_run_tasks(const float* data, int32_t dim, int kcap, float scale, const KnnTiles& tiles,
                         const KnnTasks& tasks, int32_t* cand_idx, float* cand_d2, float* norms_by_row, int* d_err,
-                        cudaStream_t s) {
+                        cudaStream_t s, float* kernel_ms) {
     require(knn_tc16_supported(dim, kcap), "tensor-core kNN: unsupported dimension or candidate count");
     require(scale > 0.0f, "tensor-core kNN: no usable scale for the data");
     const int32_t n_pad = tiles.n_pad;
@@ -514,16 +512,25 @@ void knn_tc16_run_tasks(const float* data, int32_t dim, int kcap, float scale, c
     m.blo = make_map16(blo.get(), n_pad, k_pad);
     m.ksteps = (dim + 1 + H_KSTEP - 1) / H_KSTEP;
     const float s2 = scale * scale, inv_s2 = 1.0f / s2;
+    cudaEvent_t ev0 = event_get(), ev1 = event_get();
+    UMAPB_CUDA(cudaEventRecord(ev0, s));
     if (tasks.count > 0) {
         if (kc == 1)
-            launch16_kcap<1>(kcap, m, onorm.get(), s2, inv_s2, 0, n_pad, tasks.count, tasks.tasks.get(), nullptr,
-                             tasks.tile_list.get(), tiles.row_map.get(), cand_idx, cand_d2, d_err, s);
+            launch16_kcap<1>(kcap, m, onorm.get(), s2, inv_s2, tasks.count, tasks, tiles.row_map.get(), cand_idx,
+                             cand_d2, d_err, s);
         else
-            launch16_kcap<2>(kcap, m, onorm.get(), s2, inv_s2, 0, n_pad, tasks.count, tasks.tasks.get(), nullptr,
-                             tasks.tile_list.get(), tiles.row_map.get(), cand_idx, cand_d2, d_err, s);
+            launch16_kcap<2>(kcap, m, onorm.get(), s2, inv_s2, tasks.count, tasks, tiles.row_map.get(), cand_idx,
+                             cand_d2, d_err, s);
     }
+    UMAPB_CUDA(cudaEventRecord(ev1, s));
     scatter_norms_kernel<<<grid_for(n_pad, 256), 256, 0, s>>>(tiles.row_map.get(), onorm.get(), n_pad, norms_by_row);
     UMAPB_LAUNCH_CHECK();
+    if (kernel_ms) {
+        UMAPB_CUDA(cudaEventSynchronize(ev1));
+        UMAPB_CUDA(cudaEventElapsedTime(kernel_ms, ev0, ev1));
+    }
+    event_put(ev0);
+    event_put(ev1);
 }
 
 }  // namespace umapb

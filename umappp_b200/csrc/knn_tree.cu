@@ -24,6 +24,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 #include <vector>
 
 #include "stages.cuh"
@@ -33,6 +34,10 @@ namespace umapb {
 namespace {
 
 constexpr int TREE_LEAF = 128;
+// A cut goes at the widest gap of a segment's sorted projections (and starts a
+// new padded run) when that gap exceeds this many times the typical spacing
+// of the middle half; otherwise the cut keeps tiles whole.
+constexpr float GAP_FACTOR = 16.0f;
 
 // Projection key of every position: the point's coordinates dotted with the
 // difference of two points of its segment; 0 in segments that are leaves.
@@ -62,30 +67,57 @@ __global__ void iota_kernel(int32_t* __restrict__ v, int32_t n) {
     for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = i;
 }
 
-// out[i] = row_map[idx[i]] (or -1 where idx[i] < 0)
-__global__ void gather_rows_kernel(const int32_t* __restrict__ idx, size_t count, const int32_t* __restrict__ row_map,
-                                   int32_t* __restrict__ out) {
-    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < count; i += size_t(gridDim.x) * blockDim.x)
-        out[i] = idx[i] >= 0 ? row_map[idx[i]] : -1;
-}
-
-__global__ void pad_order_kernel(const int32_t* __restrict__ perm, int32_t ninst, const int32_t* __restrict__ inst,
-                                 const int32_t* __restrict__ pad_start, int32_t n_pad, int32_t* __restrict__ row_map) {
-    for (int32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n_pad; r += gridDim.x * blockDim.x) {
-        int lo = 0, hi = ninst - 1;   // instance whose padded range holds r
+// Widest gap between consecutive sorted keys with the cut in the middle half
+// of each active segment j ([start + len/4, start + 3 len/4]): every position
+// of every middle half folds (gap bits, reversed position) into its segment's
+// 64-bit maximum, so that ties go to the smallest position.
+__global__ void widest_gap_kernel(const float* __restrict__ keys, int32_t nact, const int32_t* __restrict__ seg_start,
+                                  const int32_t* __restrict__ seg_end, const int64_t* __restrict__ mid_off,
+                                  int64_t total, unsigned long long* __restrict__ best) {
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x) {
+        int lo = 0, hi = nact - 1;   // segment of middle-half item i: last offset <= i
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (pad_start[mid] <= r) lo = mid; else hi = mid - 1;
+            if (mid_off[mid] <= i) lo = mid; else hi = mid - 1;
         }
-        const int32_t off = r - pad_start[lo];
-        row_map[r] = (off < inst[lo + 1] - inst[lo]) ? perm[inst[lo] + off] : -1;
+        const int32_t st = seg_start[lo], len = seg_end[lo] - st;
+        const int32_t p = st + max(1, len / 4) + static_cast<int32_t>(i - mid_off[lo]);
+        const float g = fmaxf(keys[p] - keys[p - 1], 0.0f);
+        const unsigned long long key = (static_cast<unsigned long long>(__float_as_uint(g)) << 32) |
+                                       static_cast<unsigned long long>(0xffffffffu - static_cast<uint32_t>(p - st));
+        atomicMax(&best[lo], key);
+    }
+}
+
+// Sorted keys at the ends of each segment's middle half.
+__global__ void middle_spread_kernel(const float* __restrict__ keys, int32_t nact, const int32_t* __restrict__ seg_start,
+                                     const int32_t* __restrict__ seg_end, float* __restrict__ lo_key,
+                                     float* __restrict__ hi_key) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nact; j += gridDim.x * blockDim.x) {
+        const int32_t st = seg_start[j], len = seg_end[j] - st;
+        lo_key[j] = keys[st + max(1, len / 4)];
+        hi_key[j] = keys[st + (3 * len) / 4];
+    }
+}
+
+// row_map[run_dst[r] + i] = perm[run_src[r] + i] for the points of every run.
+__global__ void place_runs_kernel(const int32_t* __restrict__ perm, int32_t nrun, const int32_t* __restrict__ run_src,
+                                  const int32_t* __restrict__ run_len, const int32_t* __restrict__ run_dst, int32_t n,
+                                  int32_t* __restrict__ row_map) {
+    for (int32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        int lo = 0, hi = nrun - 1;   // run holding position p: last source start <= p
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (run_src[mid] <= p) lo = mid; else hi = mid - 1;
+        }
+        row_map[run_dst[lo] + (p - run_src[lo])] = perm[p];
     }
 }
 
 // Centroid, radius and real-row count of every group of 'rows' operand rows.
 __global__ void group_bounds_kernel(const float* __restrict__ data, int32_t dim, const int32_t* __restrict__ row_map,
                                     int32_t rows, float* __restrict__ centroid, float* __restrict__ radius,
-                                    int32_t* __restrict__ count) {
+                                    int32_t* __restrict__ count, float* __restrict__ centroid_t, int32_t ngroups) {
     const int32_t g = blockIdx.x;
     const int32_t r0 = g * rows;
     __shared__ double red[256];
@@ -105,6 +137,7 @@ __global__ void group_bounds_kernel(const float* __restrict__ data, int32_t dim,
             if (src >= 0) s += data[static_cast<size_t>(src) * dim + d];
         }
         cg[d] = m ? static_cast<float>(s / m) : 0.0f;
+        if (centroid_t) centroid_t[static_cast<size_t>(d) * ngroups + g] = cg[d];   // [dim][groups] copy
     }
     __syncthreads();
     double worst = 0;
@@ -131,39 +164,61 @@ __global__ void group_bounds_kernel(const float* __restrict__ data, int32_t dim,
     }
 }
 
-// Whether reference tile t may hold a neighbour of a query in block b.
-__device__ __forceinline__ bool tile_needed(const float* __restrict__ cb, float rb, const float* __restrict__ ct,
-                                            float rt, int dim) {
+// Distance between the centroid cb (shared memory) and tile t's centroid, read
+// from the [dim][tiles] copy ct (coalesced across a warp), rounded down.
+__device__ __forceinline__ double centroid_distance_t(const float* __restrict__ cb, const float* __restrict__ ct,
+                                                      int32_t ntiles, int32_t t, int dim) {
     double s = 0;
     for (int d = 0; d < dim; ++d) {
-        const double v = static_cast<double>(cb[d]) - ct[d];
+        const double v = static_cast<double>(cb[d]) - ct[static_cast<size_t>(d) * ntiles + t];
         s += v * v;
     }
-    const double lb = sqrt(s) * (1.0 - 1e-9) - rb - rt;
-    return lb <= 2.0 * rb;
+    return sqrt(s) * (1.0 - 1e-9);
 }
 
-// One warp per query block: count (write == false) or write the indices of
-// the reference tiles of its instance that it needs, in ascending order.
-__global__ void tile_lists_kernel(int32_t nblocks, int32_t block_rows, const int32_t* __restrict__ blk_tile0,
-                                  const int32_t* __restrict__ blk_ntiles, const float* __restrict__ bc,
-                                  const float* __restrict__ br, const int32_t* __restrict__ bcount,
-                                  const float* __restrict__ tc, const float* __restrict__ tr, int32_t dim, int32_t k,
-                                  bool prune, const int64_t* __restrict__ offsets, int32_t* __restrict__ counts,
-                                  int32_t* __restrict__ lists) {
-    const int lane = threadIdx.x & 31;
-    const int32_t b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (b >= nblocks) return;
-    const int32_t t0 = blk_tile0[b], nt = blk_ntiles[b];
-    const bool all = !prune || bcount[b] < k + 1;
-    const float* cb = bc + static_cast<size_t>(b) * dim;
-    const float rb = br[b];
+// One warp per query tile b (tiles [t0, t0 + nt) of its instance).
+// Radius rho of b's k-neighbourhoods: every query q of b has at least k other
+// points within rho --
+//   2 R_b                                if b holds k + 1 or more points,
+//   R_b + |c_b - c_w| + R_w (upper)      for any tile w with k + 1 or more points,
+// the smallest of these (infinite if none applies).  Tile t is needed unless
+// |c_b - c_t| - R_b - R_t > rho.  Counts (lists == nullptr) or writes the
+// needed tiles in ascending order.
+constexpr int LIST_WARPS = 8;
+constexpr int MAX_TREE_DIM = 128;
+__global__ void __launch_bounds__(32 * LIST_WARPS)
+    tile_lists_kernel(int32_t nq, const int32_t* __restrict__ q_tile0, const int32_t* __restrict__ q_ntiles,
+                      const float* __restrict__ ct, int32_t ntiles, const float* __restrict__ tr,
+                      const int32_t* __restrict__ tcount, int32_t dim, int32_t k, bool prune,
+                      const int64_t* __restrict__ offsets, int32_t* __restrict__ counts,
+                      int32_t* __restrict__ lists) {
+    __shared__ float cbs[LIST_WARPS][MAX_TREE_DIM];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int32_t b = blockIdx.x * LIST_WARPS + wib;
+    if (b >= nq) return;   // whole warps
+    float* cb = cbs[wib];
+    for (int d = lane; d < dim; d += 32) cb[d] = ct[static_cast<size_t>(d) * ntiles + b];
+    __syncwarp();
+    const int32_t t0 = q_tile0[b], nt = q_ntiles[b];
+    const double rb = tr[b];
+    double rho = (tcount[b] >= k + 1) ? 2.0 * rb : CUDART_INF;
+    if (prune) {
+        for (int32_t base = 0; base < nt; base += 32) {
+            const int32_t w = t0 + base + lane;
+            if (base + lane < nt && w != b && tcount[w] >= k + 1) {
+                const double dist_up = centroid_distance_t(cb, ct, ntiles, w, dim) * (1.0 + 4e-9);
+                rho = fmin(rho, rb + dist_up + tr[w]);
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) rho = fmin(rho, __shfl_xor_sync(0xffffffffu, rho, o));
+    }
+    const bool all = !prune || !(rho < CUDART_INF);
     int64_t out = lists ? offsets[b] : 0;
     int32_t total = 0;
     for (int32_t base = 0; base < nt; base += 32) {
         const int32_t t = t0 + base + lane;
         bool need = false;
-        if (base + lane < nt) need = all || tile_needed(cb, rb, tc + static_cast<size_t>(t) * dim, tr[t], dim);
+        if (base + lane < nt) need = all || t == b || centroid_distance_t(cb, ct, ntiles, t, dim) - rb - tr[t] <= rho;
         const unsigned m = __ballot_sync(0xffffffffu, need);
         if (lists && need) lists[out + __popc(m & ((1u << lane) - 1u))] = t;
         out += __popc(m);
@@ -178,20 +233,22 @@ void knn_tree_order(const float* data, int32_t dim, const std::vector<int32_t>& 
                     cudaStream_t s) {
     const int ninst = static_cast<int>(inst.size()) - 1;
     const int32_t n = inst[ninst];
-    out.pad_start.assign(ninst + 1, 0);
-    for (int i = 0; i < ninst; ++i) {
-        const int32_t len = inst[i + 1] - inst[i];
-        out.pad_start[i + 1] = out.pad_start[i] + ((len + TREE_LEAF - 1) / TREE_LEAF) * TREE_LEAF;
-    }
-    out.n_pad = std::max(out.pad_start[ninst], TREE_LEAF);
     DevArray<int32_t> perm(n, s), perm2(n, s);
     DevArray<float> keys(n, s), keys2(n, s);
     iota_kernel<<<grid_for(n, 256), 256, 0, s>>>(perm.get(), n);
     UMAPB_LAUNCH_CHECK();
 
-    // segments over positions of perm; the instances to begin with
-    std::vector<int32_t> st(inst.begin(), inst.end() - 1), len(ninst);
-    for (int i = 0; i < ninst; ++i) len[i] = inst[i + 1] - inst[i];
+    // Segments over positions of perm, the instances to begin with.  A segment
+    // starts at a tile boundary of its run (a stretch of operand rows between
+    // two hard cuts, padded to whole tiles); soft cuts keep tile alignment,
+    // hard cuts (at a wide gap of the projections, as between two clusters)
+    // start a new run, so that no tile spans the gap.
+    struct Seg {
+        int32_t start, len;
+        bool hard_end;
+    };
+    std::vector<Seg> seg(ninst);
+    for (int i = 0; i < ninst; ++i) seg[i] = {inst[i], inst[i + 1] - inst[i], true};
     uint64_t h = 0x9E3779B97F4A7C15ull;
     auto next = [&h]() {   // splitmix64: the choice of the two direction points
         uint64_t z = (h += 0x9E3779B97F4A7C15ull);
@@ -200,19 +257,20 @@ void knn_tree_order(const float* data, int32_t dim, const std::vector<int32_t>& 
         return z ^ (z >> 31);
     };
     DevArray<int32_t> d_start, d_end, d_a, d_b;
-    for (int level = 0; tree && level < 40; ++level) {
-        const int nseg = static_cast<int>(st.size());
-        std::vector<int32_t> a(nseg, -1), b(nseg, -1), en(nseg);
-        bool any = false;
+    for (int level = 0; tree && level < 64; ++level) {
+        const int nseg = static_cast<int>(seg.size());
+        std::vector<int32_t> st(nseg), en(nseg), a(nseg, -1), b(nseg, -1);
+        std::vector<int32_t> act;   // segments split at this level
         for (int g = 0; g < nseg; ++g) {
-            en[g] = st[g] + len[g];
-            if (len[g] > TREE_LEAF) {
-                any = true;
-                a[g] = st[g] + static_cast<int32_t>(next() % static_cast<uint64_t>(len[g]));
-                b[g] = st[g] + static_cast<int32_t>(next() % static_cast<uint64_t>(len[g]));
+            st[g] = seg[g].start;
+            en[g] = seg[g].start + seg[g].len;
+            if (seg[g].len > TREE_LEAF) {
+                act.push_back(g);
+                a[g] = st[g] + static_cast<int32_t>(next() % static_cast<uint64_t>(seg[g].len));
+                b[g] = st[g] + static_cast<int32_t>(next() % static_cast<uint64_t>(seg[g].len));
             }
         }
-        if (!any) break;
+        if (act.empty()) break;
         d_start.reserve(nseg, s);
         d_end.reserve(nseg, s);
         d_a.reserve(nseg, s);
@@ -233,33 +291,104 @@ void knn_tree_order(const float* data, int32_t dim, const std::vector<int32_t>& 
                                                            perm2.get(), n, nseg, d_start.get(), d_end.get(), s));
         }
         std::swap(perm, perm2);
-        UMAPB_SYNC(s);   // the host segment tables are the copies' sources
-        std::vector<int32_t> st2, len2;
-        st2.reserve(2 * nseg);
-        len2.reserve(2 * nseg);
+        // widest gap of the sorted projections in the middle half of each split segment
+        const int nact = static_cast<int>(act.size());
+        std::vector<int32_t> ast(nact), aen(nact);
+        std::vector<int64_t> moff(nact + 1, 0);
+        std::vector<float> spread(nact);
+        for (int j = 0; j < nact; ++j) {
+            ast[j] = st[act[j]];
+            aen[j] = en[act[j]];
+            const int32_t len = aen[j] - ast[j];
+            moff[j + 1] = moff[j] + ((3 * len) / 4 - std::max(1, len / 4) + 1);
+        }
+        DevArray<int32_t> d_ast(nact, s), d_aen(nact, s);
+        DevArray<int64_t> d_moff(nact + 1, s);
+        DevArray<unsigned long long> d_best(nact, s);
+        DevArray<float> d_lo(nact, s), d_hi(nact, s);
+        UMAPB_CUDA(cudaMemcpyAsync(d_ast.get(), ast.data(), nact * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+        UMAPB_CUDA(cudaMemcpyAsync(d_aen.get(), aen.data(), nact * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+        UMAPB_CUDA(cudaMemcpyAsync(d_moff.get(), moff.data(), (nact + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+        d_best.zero(s);
+        widest_gap_kernel<<<grid_for(static_cast<size_t>(moff[nact]), 256), 256, 0, s>>>(
+            keys2.get(), nact, d_ast.get(), d_aen.get(), d_moff.get(), moff[nact], d_best.get());
+        UMAPB_LAUNCH_CHECK();
+        middle_spread_kernel<<<grid_for(nact, 128), 128, 0, s>>>(keys2.get(), nact, d_ast.get(), d_aen.get(), d_lo.get(),
+                                                                 d_hi.get());
+        UMAPB_LAUNCH_CHECK();
+        std::vector<unsigned long long> best(nact);
+        std::vector<float> klo(nact), khi(nact);
+        UMAPB_CUDA(cudaMemcpyAsync(best.data(), d_best.get(), nact * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+        UMAPB_CUDA(cudaMemcpyAsync(klo.data(), d_lo.get(), nact * sizeof(float), cudaMemcpyDeviceToHost, s));
+        UMAPB_CUDA(cudaMemcpyAsync(khi.data(), d_hi.get(), nact * sizeof(float), cudaMemcpyDeviceToHost, s));
+        UMAPB_SYNC(s);   // also: the host tables above are the copies' sources
+        std::vector<int32_t> gpos(nact);
+        std::vector<float> gap(nact);
+        for (int j = 0; j < nact; ++j) {
+            const uint32_t gbits = static_cast<uint32_t>(best[j] >> 32);
+            std::memcpy(&gap[j], &gbits, sizeof(float));
+            gpos[j] = static_cast<int32_t>(0xffffffffu - static_cast<uint32_t>(best[j] & 0xffffffffu));
+            spread[j] = khi[j] - klo[j];
+        }
+        std::vector<Seg> nseg2;
+        nseg2.reserve(2 * nseg);
+        int j = 0;
         for (int g = 0; g < nseg; ++g) {
-            if (len[g] > TREE_LEAF) {
-                const int32_t tiles = (len[g] + TREE_LEAF - 1) / TREE_LEAF;
-                const int32_t left = (tiles + 1) / 2 * TREE_LEAF;
-                st2.push_back(st[g]);
-                len2.push_back(left);
-                st2.push_back(st[g] + left);
-                len2.push_back(len[g] - left);
+            const Seg x = seg[g];
+            if (x.len <= TREE_LEAF) {
+                nseg2.push_back(x);
+                continue;
+            }
+            // a gap far wider than the typical spacing of the middle half
+            const float typical = spread[j] / (0.5f * x.len);
+            const bool hard = x.len >= 2 * TREE_LEAF && gpos[j] > 0 && gap[j] > GAP_FACTOR * typical &&
+                              gap[j] > 0.0f;
+            if (hard) {
+                const int32_t left = gpos[j];
+                nseg2.push_back({x.start, left, true});
+                nseg2.push_back({x.start + left, x.len - left, x.hard_end});
             } else {
-                st2.push_back(st[g]);
-                len2.push_back(len[g]);
+                const int32_t tiles = (x.len + TREE_LEAF - 1) / TREE_LEAF;
+                const int32_t left = (tiles + 1) / 2 * TREE_LEAF;
+                nseg2.push_back({x.start, left, false});
+                nseg2.push_back({x.start + left, x.len - left, x.hard_end});
+            }
+            ++j;
+        }
+        seg.swap(nseg2);
+    }
+
+    // runs (segments up to a hard end) laid out one after another, each padded to whole tiles
+    std::vector<int32_t> run_src, run_len, run_dst;
+    out.pad_start.assign(ninst + 1, 0);
+    int32_t pos = 0, inst_i = 0;
+    {
+        int32_t rs = -1, rl = 0;
+        for (const Seg& x : seg) {
+            if (rs < 0) rs = x.start;
+            rl += x.len;
+            if (x.hard_end) {
+                while (inst_i < ninst && inst[inst_i] == rs) out.pad_start[inst_i++] = pos;   // an instance's first run
+                run_src.push_back(rs);
+                run_len.push_back(rl);
+                run_dst.push_back(pos);
+                pos += ((rl + TREE_LEAF - 1) / TREE_LEAF) * TREE_LEAF;
+                rs = -1;
+                rl = 0;
             }
         }
-        st.swap(st2);
-        len.swap(len2);
     }
-    DevArray<int32_t> d_inst(inst.size(), s), d_pad(out.pad_start.size(), s);
-    UMAPB_CUDA(cudaMemcpyAsync(d_inst.get(), inst.data(), inst.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-    UMAPB_CUDA(cudaMemcpyAsync(d_pad.get(), out.pad_start.data(), out.pad_start.size() * sizeof(int32_t),
-                               cudaMemcpyHostToDevice, s));
+    out.pad_start[ninst] = pos;
+    out.n_pad = std::max(pos, TREE_LEAF);
+    const int nrun = static_cast<int>(run_src.size());
+    DevArray<int32_t> d_rs(nrun, s), d_rl(nrun, s), d_rd(nrun, s);
+    UMAPB_CUDA(cudaMemcpyAsync(d_rs.get(), run_src.data(), nrun * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    UMAPB_CUDA(cudaMemcpyAsync(d_rl.get(), run_len.data(), nrun * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    UMAPB_CUDA(cudaMemcpyAsync(d_rd.get(), run_dst.data(), nrun * sizeof(int32_t), cudaMemcpyHostToDevice, s));
     out.row_map.allocate(out.n_pad, s);
-    pad_order_kernel<<<grid_for(out.n_pad, 256), 256, 0, s>>>(perm.get(), ninst, d_inst.get(), d_pad.get(), out.n_pad,
-                                                              out.row_map.get());
+    UMAPB_CUDA(cudaMemsetAsync(out.row_map.get(), 0xff, out.n_pad * sizeof(int32_t), s));   // -1: padding
+    place_runs_kernel<<<grid_for(n, 256), 256, 0, s>>>(perm.get(), nrun, d_rs.get(), d_rl.get(), d_rd.get(), n,
+                                                       out.row_map.get());
     UMAPB_LAUNCH_CHECK();
     UMAPB_SYNC(s);   // host vectors above
 }
@@ -267,80 +396,62 @@ void knn_tree_order(const float* data, int32_t dim, const std::vector<int32_t>& 
 void knn_tile_tasks(const float* data, int32_t dim, const KnnTiles& t, const std::vector<int32_t>& inst, int qt,
                     int32_t k, bool prune, KnnTasks& out, cudaStream_t s) {
     const int ninst = static_cast<int>(inst.size()) - 1;
-    const int32_t block_rows = TREE_LEAF * qt;
     const int32_t ntiles = t.n_pad / TREE_LEAF;
-    // query blocks: qt tiles each, never across an instance boundary
-    std::vector<int32_t> qbase, qlimit, tile0, ntl;
+    // every tile's instance tile range; CTAs of qt tiles within an instance
+    std::vector<int32_t> tile0(ntiles, 0), ntl(ntiles, 0);
+    std::vector<int4> tasks;
     for (int i = 0; i < ninst; ++i) {
-        const int32_t p0 = t.pad_start[i], p1 = t.pad_start[i + 1];
-        for (int32_t r = p0; r < p1; r += block_rows) {
-            qbase.push_back(r);
-            qlimit.push_back(p0 + (inst[i + 1] - inst[i]));
-            tile0.push_back(p0 / TREE_LEAF);
-            ntl.push_back((p1 - p0) / TREE_LEAF);
+        const int32_t a = t.pad_start[i] / TREE_LEAF, b = t.pad_start[i + 1] / TREE_LEAF;
+        for (int32_t x = a; x < b; ++x) {
+            tile0[x] = a;
+            ntl[x] = b - a;
         }
+        for (int32_t x = a; x < b; x += qt) tasks.push_back(make_int4(x * TREE_LEAF, x, std::min(qt, b - x), 0));
     }
-    const int32_t nb = static_cast<int32_t>(qbase.size());
-    // bounds of the reference tiles and of the query blocks (a block may run
-    // into the next instance's rows; those rows are excluded by its own map)
-    DevArray<float> tcen(static_cast<size_t>(ntiles) * dim, s), trad(ntiles, s), bcen(static_cast<size_t>(nb) * dim, s),
-        brad(nb, s);
-    DevArray<int32_t> tcnt(ntiles, s), bcnt(nb, s);
-    group_bounds_kernel<<<ntiles, 128, 0, s>>>(data, dim, t.row_map.get(), TREE_LEAF, tcen.get(), trad.get(), tcnt.get());
+    require(dim <= MAX_TREE_DIM, "tile pruning supports up to 128 dimensions");
+    DevArray<float> tcen(static_cast<size_t>(ntiles) * dim, s), tcen_t(static_cast<size_t>(ntiles) * dim, s),
+        trad(ntiles, s);
+    DevArray<int32_t> tcnt(ntiles, s);
+    group_bounds_kernel<<<ntiles, 128, 0, s>>>(data, dim, t.row_map.get(), TREE_LEAF, tcen.get(), trad.get(), tcnt.get(),
+                                               tcen_t.get(), ntiles);
     UMAPB_LAUNCH_CHECK();
-    // a query block's rows: its own map entries, cut at its instance's end
-    DevArray<int32_t> bmap(static_cast<size_t>(nb) * block_rows, s);
-    {
-        std::vector<int32_t> idx(static_cast<size_t>(nb) * block_rows);
-        for (int32_t b = 0; b < nb; ++b)
-            for (int32_t r = 0; r < block_rows; ++r) {
-                const int32_t row = qbase[b] + r;
-                idx[static_cast<size_t>(b) * block_rows + r] = (row < qlimit[b]) ? row : -1;
-            }
-        DevArray<int32_t> d_idx(idx.size(), s);
-        UMAPB_CUDA(cudaMemcpyAsync(d_idx.get(), idx.data(), idx.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-        gather_rows_kernel<<<grid_for(idx.size(), 256), 256, 0, s>>>(d_idx.get(), idx.size(), t.row_map.get(),
-                                                                     bmap.get());
-        UMAPB_LAUNCH_CHECK();
-        UMAPB_SYNC(s);
-    }
-    group_bounds_kernel<<<nb, 128, 0, s>>>(data, dim, bmap.get(), block_rows, bcen.get(), brad.get(), bcnt.get());
+    DevArray<int32_t> d_tile0(ntiles, s), d_ntl(ntiles, s);
+    out.qlist_len.allocate(ntiles, s);
+    out.qlist_off.allocate(ntiles, s);
+    UMAPB_CUDA(cudaMemcpyAsync(d_tile0.get(), tile0.data(), ntiles * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    UMAPB_CUDA(cudaMemcpyAsync(d_ntl.get(), ntl.data(), ntiles * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    const unsigned warps_grid = static_cast<unsigned>((ntiles + LIST_WARPS - 1) / LIST_WARPS);
+    tile_lists_kernel<<<warps_grid, 32 * LIST_WARPS, 0, s>>>(ntiles, d_tile0.get(), d_ntl.get(), tcen_t.get(), ntiles,
+                                                             trad.get(), tcnt.get(), dim, k, prune, nullptr,
+                                                             out.qlist_len.get(), nullptr);
     UMAPB_LAUNCH_CHECK();
-
-    DevArray<int32_t> d_tile0(nb, s), d_ntl(nb, s), counts(nb, s);
-    DevArray<int64_t> offsets(nb + 1, s);
-    UMAPB_CUDA(cudaMemcpyAsync(d_tile0.get(), tile0.data(), nb * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-    UMAPB_CUDA(cudaMemcpyAsync(d_ntl.get(), ntl.data(), nb * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-    const unsigned warps_grid = static_cast<unsigned>((static_cast<int64_t>(nb) * 32 + 255) / 256);
-    tile_lists_kernel<<<warps_grid, 256, 0, s>>>(nb, block_rows, d_tile0.get(), d_ntl.get(), bcen.get(), brad.get(),
-                                                 bcnt.get(), tcen.get(), trad.get(), dim, k, prune, nullptr,
-                                                 counts.get(), nullptr);
-    UMAPB_LAUNCH_CHECK();
-    std::vector<int32_t> hc(nb);
-    UMAPB_CUDA(cudaMemcpyAsync(hc.data(), counts.get(), nb * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    std::vector<int32_t> hc(ntiles);
+    UMAPB_CUDA(cudaMemcpyAsync(hc.data(), out.qlist_len.get(), ntiles * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     UMAPB_SYNC(s);
-    std::vector<int64_t> ho(nb + 1, 0);
-    for (int32_t b = 0; b < nb; ++b) ho[b + 1] = ho[b] + hc[b];
-    out.total_tiles = ho[nb];
-    out.tile_list.allocate(std::max<int64_t>(ho[nb], 1), s);
-    UMAPB_CUDA(cudaMemcpyAsync(offsets.get(), ho.data(), (nb + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
-    tile_lists_kernel<<<warps_grid, 256, 0, s>>>(nb, block_rows, d_tile0.get(), d_ntl.get(), bcen.get(), brad.get(),
-                                                 bcnt.get(), tcen.get(), trad.get(), dim, k, prune, offsets.get(),
-                                                 counts.get(), out.tile_list.get());
+    std::vector<int64_t> ho(ntiles + 1, 0);
+    for (int32_t x = 0; x < ntiles; ++x) ho[x + 1] = ho[x] + hc[x];
+    out.total_tiles = ho[ntiles];
+    out.tile_list.allocate(std::max<int64_t>(ho[ntiles], 1), s);
+    UMAPB_CUDA(cudaMemcpyAsync(out.qlist_off.get(), ho.data(), ntiles * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    tile_lists_kernel<<<warps_grid, 32 * LIST_WARPS, 0, s>>>(ntiles, d_tile0.get(), d_ntl.get(), tcen_t.get(), ntiles,
+                                                             trad.get(), tcnt.get(), dim, k, prune, out.qlist_off.get(),
+                                                             out.qlist_len.get(), out.tile_list.get());
     UMAPB_LAUNCH_CHECK();
-    // tasks, longest lists first (they are scheduled first and finish together)
-    std::vector<int32_t> order(nb);
-    for (int32_t b = 0; b < nb; ++b) order[b] = b;
-    std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return hc[x] > hc[y]; });
-    std::vector<int4> tasks(nb);
-    for (int32_t j = 0; j < nb; ++j) {
-        const int32_t b = order[j];
-        require(ho[b] <= INT32_MAX, "tile lists too long", UMAPB_ERR_OVERFLOW);
-        tasks[j] = make_int4(qbase[b], static_cast<int32_t>(ho[b]), hc[b], qlimit[b]);
+    // CTAs with the most reference tiles first (they are scheduled first and finish together)
+    std::vector<int64_t> work(tasks.size());
+    for (size_t j = 0; j < tasks.size(); ++j) {
+        int64_t w = 0;
+        for (int x = 0; x < tasks[j].z; ++x) w += hc[tasks[j].y + x];
+        work[j] = w;
     }
-    out.count = nb;
-    out.tasks.allocate(nb, s);
-    UMAPB_CUDA(cudaMemcpyAsync(out.tasks.get(), tasks.data(), nb * sizeof(int4), cudaMemcpyHostToDevice, s));
+    std::vector<int32_t> order(tasks.size());
+    for (size_t j = 0; j < order.size(); ++j) order[j] = static_cast<int32_t>(j);
+    std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return work[x] > work[y]; });
+    std::vector<int4> sorted(tasks.size());
+    for (size_t j = 0; j < order.size(); ++j) sorted[j] = tasks[order[j]];
+    out.count = static_cast<int32_t>(sorted.size());
+    out.tasks.allocate(std::max<size_t>(sorted.size(), 1), s);
+    UMAPB_CUDA(cudaMemcpyAsync(out.tasks.get(), sorted.data(), sorted.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
     UMAPB_SYNC(s);   // host vectors above
 }
 

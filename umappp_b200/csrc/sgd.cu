@@ -38,12 +38,24 @@ namespace {
 constexpr int SCHED_BLOCK = 256;
 constexpr int MAX_WINDOW = 512;
 // Default cap on a window's event buffers (events, negative counts, segment
-// starts).  Windows of about a gigabyte keep the schedule's footprint small
-// next to the data and let the buffers be reused from window to window; one
-// buffer for a whole million-point run would be ~26 GB, and allocating that
-// afresh (and fragmenting the stream-ordered pool with it) costs more than
-// the extra count passes of smaller windows.
-constexpr size_t WINDOW_BYTES = size_t(1) << 30;
+// starts): 4 GiB, or 1/16 of the device's memory if that is less.  Every
+// window re-reads the whole edge state (count and write passes), so fewer,
+// larger windows cost less -- a million-point run needs ~18 B x 7.2M events
+// per epoch, 32 epochs to a 4 GiB window, 7 windows for 200 epochs -- while
+// one buffer for the whole run (~26 GB) would crowd the data.  The buffers are
+// kept from window to window and, through the workspace cache, across runs.
+size_t window_bytes() {
+    static const size_t v = [] {
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+            cudaGetLastError();
+            total_b = 0;
+        }
+        const size_t cap = size_t(4) << 30;
+        return total_b ? std::min(cap, total_b / 16) : (size_t(1) << 30);
+    }();
+    return v;
+}
 constexpr int MAX_GENERIC_DIM = 64;
 
 template <typename T>
@@ -624,7 +636,7 @@ void SgdEngine<T>::build_window(int first, int last_wanted, cudaStream_t s) {
     UMAPB_SYNC(s);
 
     // fit the window to the memory budget
-    const size_t budget = event_budget_bytes ? event_budget_bytes : WINDOW_BYTES;
+    const size_t budget = event_budget_bytes ? event_budget_bytes : window_bytes();
     // event record + (at most) one segment start per event
     const size_t per_event = sizeof(int2) + sizeof(uint16_t) + sizeof(int64_t);
     int Wk = W;

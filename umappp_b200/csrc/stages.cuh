@@ -62,38 +62,39 @@ struct KnnTiles {
     int32_t n_pad = 0;
 };
 struct KnnTasks {
-    DevArray<int4> tasks;
+    DevArray<int4> tasks;          // per CTA: {first operand row, first query tile, query tiles, 0}
+    DevArray<int64_t> qlist_off;   // per query tile: its reference tiles are
+    DevArray<int32_t> qlist_len;   //   tile_list[qlist_off .. + qlist_len)
     DevArray<int32_t> tile_list;
     int32_t count = 0;
-    int64_t total_tiles = 0;
+    int64_t total_tiles = 0;       // sum of the query tiles' list lengths
 };
 // tree == false keeps each instance in data order.
 void knn_tree_order(const float* data, int32_t dim, const std::vector<int32_t>& inst, bool tree, KnnTiles& out,
                     cudaStream_t s);
-// Blocks of qt tiles; a block with more than k real rows lists only the tiles
-// that may hold one of its rows' k nearest neighbours (all tiles of its
-// instance when prune is false).
+// Every query tile lists the reference tiles of its instance that may hold one
+// of its rows' k nearest neighbours (all of them when prune is false); CTAs
+// take qt consecutive query tiles of one instance.
 void knn_tile_tasks(const float* data, int32_t dim, const KnnTiles& t, const std::vector<int32_t>& inst, int qt,
                     int32_t k, bool prune, KnnTasks& out, cudaStream_t s);
 // Candidate search over tree-ordered operands and task lists; candidate and
 // norm outputs are indexed by data row.
 void knn_tc16_run_tasks(const float* data, int32_t dim, int kcap, float scale, const KnnTiles& tiles,
                         const KnnTasks& tasks, int32_t* cand_idx, float* cand_d2, float* norms_by_row, int* d_err,
-                        cudaStream_t s);
+                        cudaStream_t s, float* kernel_ms = nullptr);
 
 // FP16-operand variant (knn_tc16.cu): power-of-two scale of the data (0 when
 // unusable), support test, query tiles per CTA, and the search itself.
 float knn_tc16_scale(const float* data, size_t count, cudaStream_t s);
 bool knn_tc16_supported(int32_t dim, int kcap);
 int knn_tc16_query_tiles(int32_t dim);
-void knn_tc16_run(const float* data, int32_t n, int32_t dim, int kcap, float scale, int32_t n_pad,
-                  const int32_t* pad_src, int32_t ctas, const int4* tasks, const int32_t* shifts, int32_t* cand_idx,
-                  float* cand_d2, float* norms_pad, int* d_err, cudaStream_t s);
 // Number of queries the last float kNN recomputed in FP64 (certainty check).
 int& last_knn_redo_count();
 // Query-tile x reference-tile pairs (128 x 128 distances each) computed by the
 // last tensor-core candidate search: the work left after pruning.
 int64_t& last_knn_tiles_scanned();
+// Device time (ms) of the last tensor-core candidate kernel (FP16 search).
+float& last_knn_kernel_ms();
 // Largest |tensor-core FP32 squared distance - FP64 squared distance| /
 // (|q|^2 + max |r|^2) over the candidates of the last float kNN (0 without
 // the tensor-core search).
@@ -157,7 +158,7 @@ public:
     void counts(int first, int last, int64_t* out, cudaStream_t s);
     // Schedule state (enext, enneg) at 'epoch' into device arrays.
     void state_at(int epoch, T* enext, T* enneg, cudaStream_t s);
-    size_t event_budget_bytes = 0;  // window buffer cap; 0: 1 GiB (sgd.cu, WINDOW_BYTES)
+    size_t event_budget_bytes = 0;  // window buffer cap; 0: 4 GiB or 1/16 of device memory (sgd.cu)
     // Batched runs: instance i owns observations [inst_start[i], inst_start[i+1])
     // (device array of num_inst + 1 entries); negative samples stay inside it.
     void set_instances(const int32_t* inst_start, int32_t num_inst) {
