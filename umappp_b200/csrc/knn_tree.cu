@@ -39,12 +39,23 @@ constexpr int TREE_LEAF = 128;
 // of the middle half; otherwise the cut keeps tiles whole.
 constexpr float GAP_FACTOR = 16.0f;
 
-// Projection key of every position: the point's coordinates dotted with the
-// difference of two points of its segment; 0 in segments that are leaves.
+// Order-preserving map of a float to 32 unsigned bits, and its inverse.
+__device__ __forceinline__ uint32_t float_order_bits(float f) {
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float order_bits_float(uint32_t u) {
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+// Sort key of every position: its segment's index in the high bits, the
+// point's projection on the difference of two points of the segment in the
+// low 32 bits (0 in segments that are leaves).  One radix sort of these keys
+// sorts every segment at once and keeps the segments in place.
 __global__ void rp_keys_kernel(const float* __restrict__ data, int32_t dim, int32_t n,
                                const int32_t* __restrict__ perm, int32_t nseg, const int32_t* __restrict__ seg_start,
                                const int32_t* __restrict__ seg_a, const int32_t* __restrict__ seg_b,
-                               float* __restrict__ keys) {
+                               unsigned long long* __restrict__ keys) {
     for (int32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
         int lo = 0, hi = nseg - 1;   // segment of position p: last start <= p
         while (lo < hi) {
@@ -59,8 +70,12 @@ __global__ void rp_keys_kernel(const float* __restrict__ data, int32_t dim, int3
             const float* xb = data + static_cast<size_t>(perm[b]) * dim;
             for (int d = 0; d < dim; ++d) key = fmaf(x[d], xa[d] - xb[d], key);
         }
-        keys[p] = key;
+        keys[p] = (static_cast<unsigned long long>(lo) << 32) | float_order_bits(key);
     }
+}
+
+__device__ __forceinline__ float sorted_key(const unsigned long long* __restrict__ keys, int64_t p) {
+    return order_bits_float(static_cast<uint32_t>(keys[p] & 0xffffffffull));
 }
 
 __global__ void iota_kernel(int32_t* __restrict__ v, int32_t n) {
@@ -71,7 +86,8 @@ __global__ void iota_kernel(int32_t* __restrict__ v, int32_t n) {
 // of each active segment j ([start + len/4, start + 3 len/4]): every position
 // of every middle half folds (gap bits, reversed position) into its segment's
 // 64-bit maximum, so that ties go to the smallest position.
-__global__ void widest_gap_kernel(const float* __restrict__ keys, int32_t nact, const int32_t* __restrict__ seg_start,
+__global__ void widest_gap_kernel(const unsigned long long* __restrict__ keys, int32_t nact,
+                                  const int32_t* __restrict__ seg_start,
                                   const int32_t* __restrict__ seg_end, const int64_t* __restrict__ mid_off,
                                   int64_t total, unsigned long long* __restrict__ best) {
     for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x) {
@@ -82,7 +98,7 @@ __global__ void widest_gap_kernel(const float* __restrict__ keys, int32_t nact, 
         }
         const int32_t st = seg_start[lo], len = seg_end[lo] - st;
         const int32_t p = st + max(1, len / 4) + static_cast<int32_t>(i - mid_off[lo]);
-        const float g = fmaxf(keys[p] - keys[p - 1], 0.0f);
+        const float g = fmaxf(sorted_key(keys, p) - sorted_key(keys, p - 1), 0.0f);
         const unsigned long long key = (static_cast<unsigned long long>(__float_as_uint(g)) << 32) |
                                        static_cast<unsigned long long>(0xffffffffu - static_cast<uint32_t>(p - st));
         atomicMax(&best[lo], key);
@@ -90,13 +106,14 @@ __global__ void widest_gap_kernel(const float* __restrict__ keys, int32_t nact, 
 }
 
 // Sorted keys at the ends of each segment's middle half.
-__global__ void middle_spread_kernel(const float* __restrict__ keys, int32_t nact, const int32_t* __restrict__ seg_start,
+__global__ void middle_spread_kernel(const unsigned long long* __restrict__ keys, int32_t nact,
+                                     const int32_t* __restrict__ seg_start,
                                      const int32_t* __restrict__ seg_end, float* __restrict__ lo_key,
                                      float* __restrict__ hi_key) {
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nact; j += gridDim.x * blockDim.x) {
         const int32_t st = seg_start[j], len = seg_end[j] - st;
-        lo_key[j] = keys[st + max(1, len / 4)];
-        hi_key[j] = keys[st + (3 * len) / 4];
+        lo_key[j] = sorted_key(keys, st + max(1, len / 4));
+        hi_key[j] = sorted_key(keys, st + (3 * len) / 4);
     }
 }
 
@@ -164,16 +181,17 @@ __global__ void group_bounds_kernel(const float* __restrict__ data, int32_t dim,
     }
 }
 
-// Distance between the centroid cb (shared memory) and tile t's centroid, read
-// from the [dim][tiles] copy ct (coalesced across a warp), rounded down.
-__device__ __forceinline__ double centroid_distance_t(const float* __restrict__ cb, const float* __restrict__ ct,
-                                                      int32_t ntiles, int32_t t, int dim) {
-    double s = 0;
+// Squared distance between the centroid cb (shared memory) and tile t's
+// centroid, read from the [dim][tiles] copy ct (coalesced across a warp), in
+// FP32: relative error below dim * 2^-23, covered by the margins below.
+__device__ __forceinline__ float centroid_d2(const float* __restrict__ cb, const float* __restrict__ ct, int32_t ntiles,
+                                             int32_t t, int dim) {
+    float s = 0.0f;
     for (int d = 0; d < dim; ++d) {
-        const double v = static_cast<double>(cb[d]) - ct[static_cast<size_t>(d) * ntiles + t];
-        s += v * v;
+        const float v = cb[d] - ct[static_cast<size_t>(d) * ntiles + t];
+        s = fmaf(v, v, s);
     }
-    return sqrt(s) * (1.0 - 1e-9);
+    return s;
 }
 
 // One warp per query tile b (tiles [t0, t0 + nt) of its instance).
@@ -182,16 +200,17 @@ __device__ __forceinline__ double centroid_distance_t(const float* __restrict__ 
 //   2 R_b                                if b holds k + 1 or more points,
 //   R_b + |c_b - c_w| + R_w (upper)      for any tile w with k + 1 or more points,
 // the smallest of these (infinite if none applies).  Tile t is needed unless
-// |c_b - c_t| - R_b - R_t > rho.  Counts (lists == nullptr) or writes the
-// needed tiles in ascending order.
+// |c_b - c_t| - R_b - R_t > rho.  The needed tiles are written in ascending
+// order from lists[slot[b]] (room for nt entries), their number to counts[b].
 constexpr int LIST_WARPS = 8;
 constexpr int MAX_TREE_DIM = 128;
+constexpr float D2_LOW = 1.0f - 1.0e-4f;    // lower-bound factor on FP32 squared distances
+constexpr float D2_HIGH = 1.0f + 1.0e-4f;   // upper-bound factor
 __global__ void __launch_bounds__(32 * LIST_WARPS)
     tile_lists_kernel(int32_t nq, const int32_t* __restrict__ q_tile0, const int32_t* __restrict__ q_ntiles,
                       const float* __restrict__ ct, int32_t ntiles, const float* __restrict__ tr,
                       const int32_t* __restrict__ tcount, int32_t dim, int32_t k, bool prune,
-                      const int64_t* __restrict__ offsets, int32_t* __restrict__ counts,
-                      int32_t* __restrict__ lists) {
+                      const int64_t* __restrict__ slot, int32_t* __restrict__ counts, int32_t* __restrict__ lists) {
     __shared__ float cbs[LIST_WARPS][MAX_TREE_DIM];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int32_t b = blockIdx.x * LIST_WARPS + wib;
@@ -200,31 +219,34 @@ __global__ void __launch_bounds__(32 * LIST_WARPS)
     for (int d = lane; d < dim; d += 32) cb[d] = ct[static_cast<size_t>(d) * ntiles + b];
     __syncwarp();
     const int32_t t0 = q_tile0[b], nt = q_ntiles[b];
-    const double rb = tr[b];
-    double rho = (tcount[b] >= k + 1) ? 2.0 * rb : CUDART_INF;
+    const float rb = tr[b];
+    float rho = (tcount[b] >= k + 1) ? 2.0f * rb : CUDART_INF_F;
     if (prune) {
         for (int32_t base = 0; base < nt; base += 32) {
             const int32_t w = t0 + base + lane;
             if (base + lane < nt && w != b && tcount[w] >= k + 1) {
-                const double dist_up = centroid_distance_t(cb, ct, ntiles, w, dim) * (1.0 + 4e-9);
-                rho = fmin(rho, rb + dist_up + tr[w]);
+                const float dist_up = sqrtf(centroid_d2(cb, ct, ntiles, w, dim) * D2_HIGH) * D2_HIGH;
+                rho = fminf(rho, __fadd_ru(__fadd_ru(rb, dist_up), tr[w]));
             }
         }
-        for (int o = 16; o > 0; o >>= 1) rho = fmin(rho, __shfl_xor_sync(0xffffffffu, rho, o));
+        for (int o = 16; o > 0; o >>= 1) rho = fminf(rho, __shfl_xor_sync(0xffffffffu, rho, o));
     }
-    const bool all = !prune || !(rho < CUDART_INF);
-    int64_t out = lists ? offsets[b] : 0;
+    const bool all = !prune || !(rho < CUDART_INF_F);
+    int32_t* out = lists + slot[b];
     int32_t total = 0;
     for (int32_t base = 0; base < nt; base += 32) {
         const int32_t t = t0 + base + lane;
         bool need = false;
-        if (base + lane < nt) need = all || t == b || centroid_distance_t(cb, ct, ntiles, t, dim) - rb - tr[t] <= rho;
+        if (base + lane < nt) {
+            // needed unless |c_b - c_t| > rho + R_b + R_t (all non-negative: compare squares)
+            const float reach = rho + rb + tr[t];
+            need = all || t == b || centroid_d2(cb, ct, ntiles, t, dim) * D2_LOW <= reach * reach * D2_HIGH;
+        }
         const unsigned m = __ballot_sync(0xffffffffu, need);
-        if (lists && need) lists[out + __popc(m & ((1u << lane) - 1u))] = t;
-        out += __popc(m);
+        if (need) out[total + __popc(m & ((1u << lane) - 1u))] = t;
         total += __popc(m);
     }
-    if (!lists && lane == 0) counts[b] = total;
+    if (lane == 0) counts[b] = total;
 }
 
 }  // namespace
@@ -234,7 +256,7 @@ void knn_tree_order(const float* data, int32_t dim, const std::vector<int32_t>& 
     const int ninst = static_cast<int>(inst.size()) - 1;
     const int32_t n = inst[ninst];
     DevArray<int32_t> perm(n, s), perm2(n, s);
-    DevArray<float> keys(n, s), keys2(n, s);
+    DevArray<unsigned long long> keys(n, s), keys2(n, s);
     iota_kernel<<<grid_for(n, 256), 256, 0, s>>>(perm.get(), n);
     UMAPB_LAUNCH_CHECK();
 
@@ -282,13 +304,15 @@ void knn_tree_order(const float* data, int32_t dim, const std::vector<int32_t>& 
         rp_keys_kernel<<<grid_for(n, 256), 256, 0, s>>>(data, dim, n, perm.get(), nseg, d_start.get(), d_a.get(),
                                                         d_b.get(), keys.get());
         UMAPB_LAUNCH_CHECK();
+        int seg_bits = 1;
+        while ((1 << seg_bits) < nseg) ++seg_bits;
         size_t tb = 0;
-        UMAPB_CUDA(cub::DeviceSegmentedSort::SortPairs(nullptr, tb, keys.get(), keys2.get(), perm.get(), perm2.get(), n,
-                                                       nseg, d_start.get(), d_end.get(), s));
+        UMAPB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys.get(), keys2.get(), perm.get(), perm2.get(), n, 0,
+                                                   32 + seg_bits, s));
         {
             DevArray<unsigned char> temp(tb, s);
-            UMAPB_CUDA(cub::DeviceSegmentedSort::SortPairs(temp.get(), tb, keys.get(), keys2.get(), perm.get(),
-                                                           perm2.get(), n, nseg, d_start.get(), d_end.get(), s));
+            UMAPB_CUDA(cub::DeviceRadixSort::SortPairs(temp.get(), tb, keys.get(), keys2.get(), perm.get(), perm2.get(),
+                                                       n, 0, 32 + seg_bits, s));
         }
         std::swap(perm, perm2);
         // widest gap of the sorted projections in the middle half of each split segment
@@ -418,25 +442,23 @@ void knn_tile_tasks(const float* data, int32_t dim, const KnnTiles& t, const std
     DevArray<int32_t> d_tile0(ntiles, s), d_ntl(ntiles, s);
     out.qlist_len.allocate(ntiles, s);
     out.qlist_off.allocate(ntiles, s);
+    // list slots: every query tile has room for all tiles of its instance
+    std::vector<int64_t> ho(ntiles + 1, 0);
+    for (int32_t x = 0; x < ntiles; ++x) ho[x + 1] = ho[x] + ntl[x];
+    out.tile_list.allocate(std::max<int64_t>(ho[ntiles], 1), s);
     UMAPB_CUDA(cudaMemcpyAsync(d_tile0.get(), tile0.data(), ntiles * sizeof(int32_t), cudaMemcpyHostToDevice, s));
     UMAPB_CUDA(cudaMemcpyAsync(d_ntl.get(), ntl.data(), ntiles * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-    const unsigned warps_grid = static_cast<unsigned>((ntiles + LIST_WARPS - 1) / LIST_WARPS);
-    tile_lists_kernel<<<warps_grid, 32 * LIST_WARPS, 0, s>>>(ntiles, d_tile0.get(), d_ntl.get(), tcen_t.get(), ntiles,
-                                                             trad.get(), tcnt.get(), dim, k, prune, nullptr,
-                                                             out.qlist_len.get(), nullptr);
-    UMAPB_LAUNCH_CHECK();
-    std::vector<int32_t> hc(ntiles);
-    UMAPB_CUDA(cudaMemcpyAsync(hc.data(), out.qlist_len.get(), ntiles * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-    UMAPB_SYNC(s);
-    std::vector<int64_t> ho(ntiles + 1, 0);
-    for (int32_t x = 0; x < ntiles; ++x) ho[x + 1] = ho[x] + hc[x];
-    out.total_tiles = ho[ntiles];
-    out.tile_list.allocate(std::max<int64_t>(ho[ntiles], 1), s);
     UMAPB_CUDA(cudaMemcpyAsync(out.qlist_off.get(), ho.data(), ntiles * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    const unsigned warps_grid = static_cast<unsigned>((ntiles + LIST_WARPS - 1) / LIST_WARPS);
     tile_lists_kernel<<<warps_grid, 32 * LIST_WARPS, 0, s>>>(ntiles, d_tile0.get(), d_ntl.get(), tcen_t.get(), ntiles,
                                                              trad.get(), tcnt.get(), dim, k, prune, out.qlist_off.get(),
                                                              out.qlist_len.get(), out.tile_list.get());
     UMAPB_LAUNCH_CHECK();
+    std::vector<int32_t> hc(ntiles);
+    UMAPB_CUDA(cudaMemcpyAsync(hc.data(), out.qlist_len.get(), ntiles * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    UMAPB_SYNC(s);
+    out.total_tiles = 0;
+    for (int32_t x = 0; x < ntiles; ++x) out.total_tiles += hc[x];
     // CTAs with the most reference tiles first (they are scheduled first and finish together)
     std::vector<int64_t> work(tasks.size());
     for (size_t j = 0; j < tasks.size(); ++j) {

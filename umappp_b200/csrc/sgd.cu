@@ -298,6 +298,18 @@ __device__ __forceinline__ T repulse_coef(T d2, const SgdParams<T>& p) {
     return p.gamma2b / ((T(0.001) + d2) * (p.a * pow_b(d2, p.b) + T(1)));
 }
 
+// FP32 coefficients for the 2-d kernel with fused multiply-adds and the
+// approximate divide (__fdividef, 2 ulp): the step is stochastic and
+// clamped, and the per-event dependency chain is what bounds the kernel.
+__device__ __forceinline__ float attract_coef_fast(float d2, const SgdParams<float>& p) {
+    const float pd2b = pow_b(d2, p.b);
+    return __fdividef(p.neg2ab * pd2b, d2 * __fmaf_rn(p.a, pd2b, 1.0f));
+}
+
+__device__ __forceinline__ float repulse_coef_fast(float d2, const SgdParams<float>& p) {
+    return __fdividef(p.gamma2b, (0.001f + d2) * __fmaf_rn(p.a, pow_b(d2, p.b), 1.0f));
+}
+
 template <typename T>
 __device__ __forceinline__ T floor_eps(T d2) {
     const T e = FloatLimits<T>::epsilon();
@@ -425,8 +437,8 @@ __global__ void __launch_bounds__(256, MINB) sgd_epoch_2d_f32(const int64_t* __r
                 }
                 if (attract) {
                     const float dx = hx - yt.x, dy = hy - yt.y;
-                    const float d2 = floor_eps(dx * dx + dy * dy);
-                    const float cf = attract_coef(d2, p);
+                    const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
+                    const float cf = attract_coef_fast(d2, p);
                     const float gx = p.alpha * clamp4(cf * dx);
                     const float gy = p.alpha * clamp4(cf * dy);
                     hx += gx;
@@ -438,10 +450,10 @@ __global__ void __launch_bounds__(256, MINB) sgd_epoch_2d_f32(const int64_t* __r
                 for (int i = 0; i < NB; ++i) {
                     if (i < m && ks[i] != h) {
                         const float dx = hx - yk[i].x, dy = hy - yk[i].y;
-                        const float d2 = floor_eps(dx * dx + dy * dy);
-                        const float cf = repulse_coef(d2, p);
-                        hx += p.alpha * clamp4(cf * dx);
-                        hy += p.alpha * clamp4(cf * dy);
+                        const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
+                        const float cf = repulse_coef_fast(d2, p);
+                        hx = __fmaf_rn(p.alpha, clamp4(cf * dx), hx);
+                        hy = __fmaf_rn(p.alpha, clamp4(cf * dy), hy);
                     }
                 }
                 remaining -= m;
