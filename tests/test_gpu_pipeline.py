@@ -164,6 +164,19 @@ def test_partial_runs_follow_the_same_schedule(umap):
     assert np.array_equal(mid.epoch_of_next_negative_sample, ep.enneg)
 
 
+@pytest.mark.parametrize("n,epochs", [(3000, 500), (20000, 200)])
+def test_event_windows_self_check(umap, monkeypatch, n, epochs):
+    # every window's event lists are checked on the device against the
+    # schedule recomputed from the initial state (counts, negatives, head order)
+    monkeypatch.setenv("UMAPB_CHECK_SCHEDULE", "1")
+    X = oracle.gaussian_mixture(n, 12, 5, 4.0, seed=n, dtype=np.float32)
+    Y = np.zeros((n, 2), np.float32)
+    st = umap.initialize_from_data(X, 2, Y, umap.Options(num_epochs=epochs))
+    st.run(Y, epochs // 3)
+    st.run(Y)
+    assert st.epoch() == epochs and np.all(np.isfinite(Y))
+
+
 def test_initialize_method_semantics(umap):
     # tests/src/umappp.cpp:209-313
     nn = mock_neighbors(87, 5, seed=87)

@@ -544,6 +544,12 @@ __global__ void __launch_bounds__(128) sgd_epoch_generic(const int64_t* __restri
     }
 }
 
+// UMAPB_CHECK_SCHEDULE=1: verify every event window (SgdEngine::verify_window).
+bool check_schedule() {
+    const char* e = std::getenv("UMAPB_CHECK_SCHEDULE");
+    return e && *e && *e != '0';
+}
+
 // Grid size as a multiple of the resident blocks (UMAPB_SGD_GRID_MULTIPLE, default 1).
 int grid_multiple() {
     static const int v = [] {
@@ -707,6 +713,7 @@ void SgdEngine<T>::build_window(int first, int last_wanted, cudaStream_t s) {
     UMAPB_CUDA(cudaMemcpyAsync(&st, status.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
     UMAPB_SYNC(s);
     require(st == DEV_OK, "a negative-sample count exceeded 65535");
+    if (check_schedule()) verify_window(first, Wk, s);
     window_begin_ = first;
     window_end_ = first + Wk;
     state_epoch_ = window_end_;
@@ -868,6 +875,55 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
     for (auto& x : ev) event_put(x);
     if (ms_schedule) *ms_schedule = sched_ms;
     if (ms_sgd) *ms_sgd = sgd_ms;
+}
+
+// Self-check of the event windows (UMAPB_CHECK_SCHEDULE=1, used by the tests):
+// per epoch, the window's events and negative samples must equal the totals of
+// the schedule recomputed from the initial state, and the events of an epoch
+// must come in head order.
+
+__global__ void window_stats_kernel(const int2* __restrict__ ht, const uint16_t* __restrict__ nneg,
+                                    const int64_t* __restrict__ starts, unsigned long long* __restrict__ negs,
+                                    unsigned long long* __restrict__ disorder) {
+    const int w = blockIdx.x;
+    const int64_t a = starts[w], b = starts[w + 1];
+    unsigned long long sn = 0, bad = 0;
+    for (int64_t e = a + threadIdx.x; e < b; e += blockDim.x) {
+        sn += nneg[e];
+        if (e > a && ht[e - 1].x > ht[e].x) ++bad;
+    }
+    atomicAdd(&negs[w], sn);
+    atomicAdd(&disorder[w], bad);
+}
+
+template <typename T>
+void SgdEngine<T>::verify_window(int first, int W, cudaStream_t s) {
+    const int64_t nnz = ep_->nnz;
+    DevArray<T> en(nnz, s), enn(nnz, s);
+    state_at(first, en.get(), enn.get(), s);
+    DevArray<unsigned long long> totals(2 * static_cast<size_t>(W), s), negs(W, s), disorder(W, s);
+    totals.zero(s);
+    negs.zero(s);
+    disorder.zero(s);
+    if (nnz) {
+        const int64_t nblocks = (nnz + SCHED_BLOCK - 1) / SCHED_BLOCK;
+        sched_totals_kernel<T><<<static_cast<unsigned>(nblocks), SCHED_BLOCK, 0, s>>>(
+            nnz, ep_->eps.get(), en.get(), enn.get(), ep_->negative_sample_rate, first, W, totals.get());
+        UMAPB_LAUNCH_CHECK();
+    }
+    window_stats_kernel<<<W, 256, 0, s>>>(ht_.get(), nneg_.get(), epoch_offsets_.get(), negs.get(), disorder.get());
+    UMAPB_LAUNCH_CHECK();
+    std::vector<unsigned long long> ht_tot(2 * static_cast<size_t>(W)), hn(W), hd(W);
+    UMAPB_CUDA(cudaMemcpyAsync(ht_tot.data(), totals.get(), ht_tot.size() * sizeof(unsigned long long),
+                               cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaMemcpyAsync(hn.data(), negs.get(), W * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    UMAPB_CUDA(cudaMemcpyAsync(hd.data(), disorder.get(), W * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    UMAPB_SYNC(s);
+    for (int w = 0; w < W; ++w) {
+        const unsigned long long ev = static_cast<unsigned long long>(host_epoch_offsets_[w + 1] - host_epoch_offsets_[w]);
+        require(ev == ht_tot[2 * w] && hn[w] == ht_tot[2 * w + 1] && hd[w] == 0,
+                "schedule window self-check failed at epoch " + std::to_string(first + w), UMAPB_ERR_CUDA);
+    }
 }
 
 template <typename T>

@@ -178,6 +178,7 @@ public:
 
 private:
     void build_window(int first, int last_wanted, cudaStream_t s);
+    void verify_window(int first, int W, cudaStream_t s);
     template <class Launch>
     void tune(T* Y, int num_dim, int first, int stop, Launch& launch, cudaStream_t s);
     static int default_variant();
