@@ -45,6 +45,9 @@ CONFIGS = {
     "small_2k": (2_000, 10, 1, 0.0, "equal", 15, 500),
 }
 METRIC = "end-to-end s & SGD edge-updates/s, 1M pts; FP32/batched vs plain at equal trust"
+# DRAM bytes (read + write) per launch of the dominant kernels, from one ncu
+# capture each (profiles/knn_tc16_kernel.md, profiles/sgd_epoch_2d_f32.md).
+TRAFFIC = {"mixture_1m": {"knn_tc16_kernel": 3.94e9 + 0.22e9, "sgd_epoch_2d_f32": 95.9e6 + 0.8e6}}
 # Batched workload: 64 independent instances, sizes log-uniform in [500, 50000],
 # 30 dims, float32 5-cluster mixtures, k = 15, 200 epochs.
 BATCH = {"instances": 64, "min": 500, "max": 50_000, "dim": 30, "clusters": 5, "k": 15, "epochs": 200}
@@ -199,7 +202,8 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     sgd_gbs = sgd_bytes / (sgd_ms * 1e-3) / 1e9
     roof_sgd = {"bound": "hbm", "kernel": "sgd_epoch_2d_f32", "achieved": round(sgd_gbs, 1),
                 "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": round(sgd_gbs / peaks["hbm_gbs"], 4),
-                "traffic": None, "peak_source": peaks["source"], "time_ms": round(sgd_ms, 3),
+                "traffic": TRAFFIC.get(args.config, {}).get("sgd_epoch_2d_f32"), "traffic_unit": "bytes per epoch launch",
+                "peak_source": peaks["source"], "time_ms": round(sgd_ms, 3),
                 "note": "algorithmic bytes 4*nnz*epochs + 56*F + 8*N_neg over the SGD stage time (all epochs)"}
     # kNN roofline: the distances the pruned search computes (128 x 128 per tile pair,
     # 2*dim FLOP each, the FP32 GEMM count) over the kernel's device time
@@ -207,7 +211,8 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     knn_tflops = knn_flops / (knn_kernel_ms * 1e-3) / 1e12 if knn_kernel_ms > 0 else 0.0
     roof_knn = {"bound": "tensor", "kernel": "knn_tc16_kernel", "achieved": round(knn_tflops, 2),
                 "peak": peaks["bf16_tflops"], "unit": "TFLOP/s", "frac": round(knn_tflops / peaks["bf16_tflops"], 4),
-                "traffic": None, "peak_source": peaks["source"], "time_ms": round(knn_kernel_ms, 3),
+                "traffic": TRAFFIC.get(args.config, {}).get("knn_tc16_kernel"), "traffic_unit": "bytes per launch",
+                "peak_source": peaks["source"], "time_ms": round(knn_kernel_ms, 3),
                 "note": "2*dim FLOP per computed (query, reference) pair over the kernel's CUDA-event time; "
                         "peak = measured dense BF16 (FP16 runs at the same rate); the 3-product FP16 split "
                         "and the K padding (dim+1 -> 64) make the issued tensor work 3*64/dim times this",

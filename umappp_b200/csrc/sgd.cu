@@ -213,9 +213,6 @@ struct SgdParams {
     // draws its negative samples there.  num_inst <= 1: one instance of n.
     const int32_t* inst_start;
     int32_t num_inst;
-    // Phases: an epoch runs as num_phases launches; launch 'phase' processes
-    // the heads in the phase-th of num_phases equal slices of each instance.
-    int32_t phase, num_phases;
 };
 
 // Observation range [base, base + size) of the instance that owns h.
@@ -235,13 +232,6 @@ __device__ __forceinline__ void instance_range(int32_t h, const SgdParams<T>& p,
     size = static_cast<uint32_t>(p.inst_start[lo + 1] - base);
 }
 
-// Whether head h (in the instance [base, base + size)) belongs to this launch's phase.
-template <typename T>
-__device__ __forceinline__ bool in_phase(int32_t h, int32_t base, uint32_t size, const SgdParams<T>& p) {
-    if (p.num_phases <= 1) return true;
-    const int64_t slice = (static_cast<int64_t>(h - base) * p.num_phases) / size;
-    return slice == p.phase;
-}
 
 // Counter-based negative-sample stream of one event.
 struct NegStream {
@@ -376,6 +366,90 @@ __global__ void __launch_bounds__(SEG_BLOCK) seg_write_kernel(int64_t total, con
     }
 }
 
+// Head slices: within every epoch the segments are ordered by the slice of
+// their head -- slice b of P holds the heads [base + b size / P, base + (b+1)
+// size / P) of each instance [base, base + size) -- so that launches over
+// consecutive slot ranges take the slices in order.  seg_bucket_* count and
+// scatter each segment to order[seg_first[w] + rank] (rank among its epoch's
+// segments by slice; within a slice in no particular order).
+__device__ __forceinline__ void segment_slice(int64_t s, const int64_t* __restrict__ seg_pos,
+                                              const int2* __restrict__ ht, const int64_t* __restrict__ seg_first, int W,
+                                              const int32_t* __restrict__ inst_start, int32_t num_inst, int32_t n,
+                                              int P, int& w, int& b) {
+    int lo = 0, hi = W - 1;   // epoch: last w with seg_first[w] <= s
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (seg_first[mid] <= s) lo = mid; else hi = mid - 1;
+    }
+    w = lo;
+    const int32_t h = ht[seg_pos[s]].x;
+    int32_t base = 0, size = n;
+    if (num_inst > 1) {
+        int a = 0, c = num_inst - 1;
+        while (a < c) {
+            const int mid = (a + c + 1) >> 1;
+            if (inst_start[mid] <= h) a = mid; else c = mid - 1;
+        }
+        base = inst_start[a];
+        size = inst_start[a + 1] - base;
+    }
+    b = static_cast<int>((static_cast<int64_t>(h - base) * P) / size);
+}
+
+// One instance: the slices of an epoch are consecutive segment ranges (heads
+// ascend within an epoch); off[w][b] = first segment whose head is at least
+// b n / P (binary search), off[w][P] = the epoch's end.
+__global__ void slice_bounds_kernel(const int64_t* __restrict__ seg_pos, const int2* __restrict__ ht,
+                                    const int64_t* __restrict__ seg_first, int W, int32_t n, int P,
+                                    int64_t* __restrict__ off) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= W * (P + 1)) return;
+    const int w = i / (P + 1), b = i % (P + 1);
+    int64_t lo = seg_first[w], hi = seg_first[w + 1];
+    if (b == P) {
+        off[i] = hi;
+        return;
+    }
+    const int64_t key = (static_cast<int64_t>(b) * n + P - 1) / P;   // ceil(b n / P)
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (ht[seg_pos[mid]].x < key) lo = mid + 1; else hi = mid;
+    }
+    off[i] = lo;
+}
+
+// Several instances: block-local histograms of (epoch, slice), one global
+// atomic per block and bin to reserve ranks, then the block's segments are
+// scattered within their reservations.
+constexpr int SLICE_BLOCK = 256;
+constexpr int SLICE_MAX_BINS = 4096;
+__global__ void __launch_bounds__(SLICE_BLOCK)
+    seg_bucket_kernel(int64_t nseg, const int64_t* __restrict__ seg_pos, const int2* __restrict__ ht,
+                      const int64_t* __restrict__ seg_first, int W, const int32_t* __restrict__ inst_start,
+                      int32_t num_inst, int32_t n, int P, int* __restrict__ counts, int* __restrict__ cursor,
+                      int32_t* __restrict__ order) {
+    __shared__ int bins[SLICE_MAX_BINS];
+    const int nb = W * P;
+    for (int i = threadIdx.x; i < nb; i += SLICE_BLOCK) bins[i] = 0;
+    __syncthreads();
+    const int64_t s = blockIdx.x * int64_t(SLICE_BLOCK) + threadIdx.x;
+    int w = 0, b = 0, local = -1;
+    if (s < nseg) {
+        segment_slice(s, seg_pos, ht, seg_first, W, inst_start, num_inst, n, P, w, b);
+        local = atomicAdd(&bins[w * P + b], 1);
+    }
+    __syncthreads();
+    if (!order) {   // counting pass
+        for (int i = threadIdx.x; i < nb; i += SLICE_BLOCK)
+            if (bins[i]) atomicAdd(&counts[i], bins[i]);
+        return;
+    }
+    for (int i = threadIdx.x; i < nb; i += SLICE_BLOCK)
+        if (bins[i]) bins[i] = atomicAdd(&cursor[i], bins[i]);   // base of this block's ranks in bin i
+    __syncthreads();
+    if (s < nseg) order[seg_first[w] + bins[w * P + b] + local] = static_cast<int32_t>(s - seg_first[w]);
+}
+
 // seg_first[w] = index of the first segment of epoch w (lower bound of starts[w] in seg_pos).
 __global__ void seg_first_kernel(const int64_t* __restrict__ seg_pos, int64_t nseg, const int64_t* __restrict__ starts,
                                  int W, int64_t* __restrict__ seg_first) {
@@ -403,18 +477,19 @@ __global__ void seg_first_kernel(const int64_t* __restrict__ seg_pos, int64_t ns
 // optimize_layout.hpp:136-180.  The tail moves by a vector atomic; the head's
 // total displacement is added once at the end.
 template <int NB, int MINB>
-__global__ void __launch_bounds__(256, MINB) sgd_epoch_2d_f32(const int64_t* __restrict__ seg_first, int w,
+__global__ void __launch_bounds__(256, MINB) sgd_epoch_2d_f32(const int32_t* __restrict__ order, int64_t base,
+                                                        int64_t slot0, int64_t slot1,
                                                         const int64_t* __restrict__ seg_pos,
                                                         const int2* __restrict__ ht, const uint16_t* __restrict__ nneg,
                                                         float2* __restrict__ Y, SgdParams<float> p) {
-    const int64_t s0 = seg_first[w], s1 = seg_first[w + 1];
-    for (int64_t s = s0 + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; s < s1; s += int64_t(gridDim.x) * blockDim.x) {
+    for (int64_t slot = slot0 + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; slot < slot1;
+         slot += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t s = order ? base + order[slot] : slot;
         const int64_t e0 = seg_pos[s], e1 = seg_pos[s + 1];
         const int32_t h = ht[e0].x;
         int32_t nbase;
         uint32_t nsize;
         instance_range(h, p, nbase, nsize);
-        if (!in_phase(h, nbase, nsize, p)) continue;
         const float2 y0 = __ldcg(&Y[h]);
         float hx = y0.x, hy = y0.y;
         for (int64_t e = e0; e < e1; ++e) {
@@ -464,7 +539,8 @@ __global__ void __launch_bounds__(256, MINB) sgd_epoch_2d_f32(const int64_t* __r
 }
 
 struct Sgd2dVariant {
-    void (*kernel)(const int64_t*, int, const int64_t*, const int2*, const uint16_t*, float2*, SgdParams<float>);
+    void (*kernel)(const int32_t*, int64_t, int64_t, int64_t, const int64_t*, const int2*, const uint16_t*, float2*,
+                   SgdParams<float>);
     int neg_batch, min_blocks;
 };
 const Sgd2dVariant SGD_2D_VARIANTS[] = {
@@ -492,19 +568,20 @@ int sgd_2d_resident(int v, int block) {
 
 // Any dimension (up to MAX_GENERIC_DIM) and either precision; same per-segment order.
 template <typename T>
-__global__ void __launch_bounds__(128) sgd_epoch_generic(const int64_t* __restrict__ seg_first, int w,
+__global__ void __launch_bounds__(128) sgd_epoch_generic(const int32_t* __restrict__ order, int64_t base,
+                                                         int64_t slot0, int64_t slot1,
                                                          const int64_t* __restrict__ seg_pos,
                                                          const int2* __restrict__ ht, const uint16_t* __restrict__ nneg,
                                                          T* __restrict__ Y, int dim, SgdParams<T> p) {
-    const int64_t s0 = seg_first[w], s1 = seg_first[w + 1];
     T head[MAX_GENERIC_DIM], orig[MAX_GENERIC_DIM];
-    for (int64_t s = s0 + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; s < s1; s += int64_t(gridDim.x) * blockDim.x) {
+    for (int64_t slot = slot0 + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; slot < slot1;
+         slot += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t s = order ? base + order[slot] : slot;
         const int64_t e0 = seg_pos[s], e1 = seg_pos[s + 1];
         const int32_t h = ht[e0].x;
         int32_t nbase;
         uint32_t nsize;
         instance_range(h, p, nbase, nsize);
-        if (!in_phase(h, nbase, nsize, p)) continue;
         T* yh = Y + static_cast<size_t>(h) * dim;
         for (int d = 0; d < dim; ++d) head[d] = orig[d] = __ldcg(yh + d);
         for (int64_t e = e0; e < e1; ++e) {
@@ -656,7 +733,7 @@ void SgdEngine<T>::build_window(int first, int last_wanted, cudaStream_t s) {
     // fit the window to the memory budget
     const size_t budget = event_budget_bytes ? event_budget_bytes : window_bytes();
     // event record + (at most) one segment start per event
-    const size_t per_event = sizeof(int2) + sizeof(uint16_t) + sizeof(int64_t);
+    const size_t per_event = sizeof(int2) + sizeof(uint16_t) + sizeof(int64_t) + sizeof(int32_t);
     int Wk = W;
     while (Wk > 1 && static_cast<size_t>(h[Wk]) * per_event > budget) --Wk;
     const int64_t events = h[Wk];
@@ -709,6 +786,7 @@ void SgdEngine<T>::build_window(int first, int last_wanted, cudaStream_t s) {
                                cudaMemcpyDeviceToHost, s));
 
     host_epoch_offsets_.assign(h.begin(), h.begin() + Wk + 1);
+    build_slices(nseg, Wk, s);
     int st = 0;
     UMAPB_CUDA(cudaMemcpyAsync(&st, status.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
     UMAPB_SYNC(s);
@@ -789,8 +867,6 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
     p.n = ep_->n;
     p.inst_start = inst_start_;
     p.num_inst = num_inst_;
-    p.phase = 0;
-    p.num_phases = 1;
     const T lr = static_cast<T>(learning_rate);
 
     cudaEvent_t ev[4];
@@ -813,27 +889,29 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
         // Parallel updates read positions that the serial order would already
         // have moved; when every event of an epoch is in flight at once the
         // layouts come out measurably tighter (lower edge cross-entropy) than
-        // the reference's.  Slicing each instance's heads into at least
-        // min_phases ordered launches bounds that staleness.  One instance with
-        // more segments than resident threads is already processed in rounds
-        // by the grid-stride loop, and needs fewer explicit phases.
-        int phases = std::max(1, min_phases);
-        if (num_inst_ <= 1) {
-            const int64_t threads = static_cast<int64_t>(std::min<int64_t>(g, resident)) * blk;
-            const int64_t rounds = (nsegs + threads - 1) / threads;
-            phases = static_cast<int>(std::max<int64_t>(1, (phases + rounds - 1) / rounds));
-        }
-        p.num_phases = phases;
-        for (int ph = 0; ph < phases; ++ph) {
-            p.phase = ph;
+        // the reference's.  The epoch's segments are therefore ordered by head
+        // slice (P = min_phases slices of each instance, build_window), and
+        // taken in that order: by the grid-stride loop's rounds when the epoch
+        // holds several rounds of segments, and by consecutive launches over
+        // slot ranges (L of them, slices split evenly) to make up the rest.
+        const int P = buckets_;
+        const int64_t threads = static_cast<int64_t>(std::min<int64_t>(g, resident)) * blk;
+        const int64_t rounds = (nsegs + threads - 1) / threads;
+        const int L = static_cast<int>(std::min<int64_t>(P, std::max<int64_t>(1, (P + rounds - 1) / rounds)));
+        const int64_t* off = host_bucket_off_.data() + static_cast<size_t>(w) * (P + 1);
+        for (int l = 0; l < L; ++l) {
+            const int64_t slot0 = off[(P * l) / L], slot1 = off[(P * (l + 1)) / L];
+            if (slot1 <= slot0) continue;
+            const unsigned gl = grid_for(slot1 - slot0, blk, static_cast<unsigned>(resident * grid_multiple()));
             if (use_2d) {
                 if constexpr (std::is_same<T, float>::value) {
-                    SGD_2D_VARIANTS[variant].kernel<<<g, blk, 0, s>>>(seg_first_.get(), w, seg_pos_.get(), ht_.get(),
-                                                                      nneg_.get(), reinterpret_cast<float2*>(Yp), p);
+                    SGD_2D_VARIANTS[variant].kernel<<<gl, blk, 0, s>>>(slices_ordered_ ? seg_order_.get() : nullptr, host_seg_first_[w], slot0,
+                                                                       slot1, seg_pos_.get(), ht_.get(), nneg_.get(),
+                                                                       reinterpret_cast<float2*>(Yp), p);
                 }
             } else {
-                sgd_epoch_generic<T><<<g, 128, 0, s>>>(seg_first_.get(), w, seg_pos_.get(), ht_.get(), nneg_.get(),
-                                                       Yp, num_dim, p);
+                sgd_epoch_generic<T><<<gl, 128, 0, s>>>(slices_ordered_ ? seg_order_.get() : nullptr, host_seg_first_[w], slot0, slot1,
+                                                        seg_pos_.get(), ht_.get(), nneg_.get(), Yp, num_dim, p);
             }
             UMAPB_LAUNCH_CHECK();
         }
@@ -875,6 +953,61 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
     for (auto& x : ev) event_put(x);
     if (ms_schedule) *ms_schedule = sched_ms;
     if (ms_sgd) *ms_sgd = sgd_ms;
+}
+
+// Orders every epoch's segments of the window by head slice (see the epoch
+// kernels): counts per (epoch, slice), slot offsets on the host, scatter.
+template <typename T>
+void SgdEngine<T>::build_slices(int64_t nseg, int W, cudaStream_t s) {
+    const int P = buckets_ = std::max(1, std::min(min_phases, 64));
+    UMAPB_SYNC(s);   // host_seg_first_ (copied by the caller) is read below
+    host_bucket_off_.assign(static_cast<size_t>(W) * (P + 1), 0);
+    if (num_inst_ <= 1 || W * P > SLICE_MAX_BINS) {
+        // slices are consecutive segment ranges: identity order (with several
+        // instances and too many bins for one block, slices of the whole row range)
+        slices_ordered_ = false;
+        DevArray<int64_t> off(static_cast<size_t>(W) * (P + 1), s);
+        slice_bounds_kernel<<<grid_for(static_cast<size_t>(W) * (P + 1), 128), 128, 0, s>>>(
+            seg_pos_.get(), ht_.get(), seg_first_.get(), W, ep_->n, P, off.get());
+        UMAPB_LAUNCH_CHECK();
+        UMAPB_CUDA(cudaMemcpyAsync(host_bucket_off_.data(), off.get(), host_bucket_off_.size() * sizeof(int64_t),
+                                   cudaMemcpyDeviceToHost, s));
+        UMAPB_SYNC(s);
+        return;
+    }
+    slices_ordered_ = true;
+    seg_order_.reserve(std::max<int64_t>(nseg, 1), s);
+    DevArray<int> counts(static_cast<size_t>(W) * P, s);
+    counts.zero(s);
+    const unsigned blocks = static_cast<unsigned>((nseg + SLICE_BLOCK - 1) / SLICE_BLOCK);
+    if (nseg > 0) {
+        seg_bucket_kernel<<<blocks, SLICE_BLOCK, 0, s>>>(nseg, seg_pos_.get(), ht_.get(), seg_first_.get(), W,
+                                                         inst_start_, num_inst_, ep_->n, P, counts.get(), nullptr,
+                                                         nullptr);
+        UMAPB_LAUNCH_CHECK();
+    }
+    std::vector<int> hc(static_cast<size_t>(W) * P);
+    UMAPB_CUDA(cudaMemcpyAsync(hc.data(), counts.get(), hc.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
+    UMAPB_SYNC(s);
+    std::vector<int> cursor(static_cast<size_t>(W) * P);
+    for (int w = 0; w < W; ++w) {
+        int64_t acc = host_seg_first_[w];
+        for (int b = 0; b < P; ++b) {
+            host_bucket_off_[static_cast<size_t>(w) * (P + 1) + b] = acc;
+            cursor[static_cast<size_t>(w) * P + b] = static_cast<int>(acc - host_seg_first_[w]);
+            acc += hc[static_cast<size_t>(w) * P + b];
+        }
+        host_bucket_off_[static_cast<size_t>(w) * (P + 1) + P] = acc;
+    }
+    if (nseg > 0) {
+        DevArray<int> d_cursor(cursor.size(), s);
+        UMAPB_CUDA(cudaMemcpyAsync(d_cursor.get(), cursor.data(), cursor.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+        seg_bucket_kernel<<<blocks, SLICE_BLOCK, 0, s>>>(nseg, seg_pos_.get(), ht_.get(), seg_first_.get(), W,
+                                                         inst_start_, num_inst_, ep_->n, P, nullptr, d_cursor.get(),
+                                                         seg_order_.get());
+        UMAPB_LAUNCH_CHECK();
+        UMAPB_SYNC(s);   // the cursor vector is the copy's source
+    }
 }
 
 // Self-check of the event windows (UMAPB_CHECK_SCHEDULE=1, used by the tests):

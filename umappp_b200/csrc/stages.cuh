@@ -179,6 +179,11 @@ public:
 private:
     void build_window(int first, int last_wanted, cudaStream_t s);
     void verify_window(int first, int W, cudaStream_t s);
+    void build_slices(int64_t nseg, int W, cudaStream_t s);
+    DevArray<int32_t> seg_order_;            // per epoch: its segments by head slice (offsets from seg_first)
+    std::vector<int64_t> host_bucket_off_;   // per epoch: P + 1 slot offsets of the slices
+    int buckets_ = 8;
+    bool slices_ordered_ = false;            // seg_order_ in use (several instances)
     template <class Launch>
     void tune(T* Y, int num_dim, int first, int stop, Launch& launch, cudaStream_t s);
     static int default_variant();
