@@ -220,3 +220,20 @@ def test_trustworthiness_matches_sklearn(oracle_mod):
     X = normal_data(300, 6, seed=8)
     Y = normal_data(300, 2, seed=9)
     assert abs(oracle.trustworthiness(X, Y, 10) - sk.trustworthiness(X, Y, n_neighbors=10)) < 1e-12
+
+
+@pytest.mark.parametrize("dtype", ["float32", "float64"])
+def test_pipeline_quality_fixture_reproduces(oracle_mod, dtype):
+    # tests/golden/pipeline_quality_normal_2000.json: the serial reference runs
+    # whose mean quality the device's layouts are compared with; its first seed
+    # must come out of the oracle unchanged.
+    import json
+    import sys
+    sys.path.insert(0, GOLDEN)
+    import make_pipeline_quality as mk
+    with open(os.path.join(GOLDEN, "pipeline_quality_normal_2000.json")) as f:
+        ref = json.load(f)[dtype]
+    assert ref["seeds"][0] == 0 and len(ref["seeds"]) >= 24
+    t, ce = mk.reference_run(getattr(np, dtype), 0)
+    assert abs(t - ref["trust"][0]) < 1e-12
+    assert abs(ce - ref["cross_entropy"][0]) <= 1e-9 * abs(ce)

@@ -104,7 +104,7 @@ size_t ws_cached_bytes();
 void ws_release_cached();
 cudaEvent_t event_get();          // timing event from the pool
 void event_put(cudaEvent_t e);
-cudaStream_t stream_get();        // non-blocking stream of the current device
+cudaStream_t stream_get(bool high_priority = false);   // non-blocking stream of the current device
 void stream_put(cudaStream_t s);  // s must be idle
 
 // Stream-ordered device allocation from the workspace cache; released on the

@@ -172,7 +172,7 @@ std::vector<cudaEvent_t>& timing_events() {
     return *v;
 }
 std::mutex g_stream_mu;
-std::vector<std::pair<int, cudaStream_t>>& spare_streams() {
+std::vector<std::pair<int, cudaStream_t>>& spare_streams() {   // (device * 2 + high priority, stream)
     static auto* v = new std::vector<std::pair<int, cudaStream_t>>();
     return *v;
 }
@@ -199,29 +199,37 @@ void event_put(cudaEvent_t e) {
     timing_events().push_back(e);
 }
 
-cudaStream_t stream_get() {
+cudaStream_t stream_get(bool high_priority) {
     const int dev = current_device();
+    const int key = dev * 2 + (high_priority ? 1 : 0);
     {
         std::lock_guard<std::mutex> lock(g_stream_mu);
         auto& v = spare_streams();
         for (size_t i = 0; i < v.size(); ++i) {
-            if (v[i].first == dev) {
+            if (v[i].first == key) {
                 cudaStream_t s = v[i].second;
                 v.erase(v.begin() + static_cast<std::ptrdiff_t>(i));
                 return s;
             }
         }
     }
+    int least = 0, greatest = 0;
+    if (high_priority) UMAPB_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
     cudaStream_t s = nullptr;
-    UMAPB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    UMAPB_CUDA(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, high_priority ? greatest : least));
     return s;
 }
 
 // The stream must be idle (synchronised by the caller).
 void stream_put(cudaStream_t s) {
     if (!s) return;
+    int priority = 0, least = 0, greatest = 0;   // no throw: called from destructors
+    const bool high = cudaStreamGetPriority(s, &priority) == cudaSuccess &&
+                      cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess && greatest < least &&
+                      priority == greatest;
+    cudaGetLastError();
     std::lock_guard<std::mutex> lock(g_stream_mu);
-    spare_streams().emplace_back(current_device(), s);
+    spare_streams().emplace_back(current_device() * 2 + (high ? 1 : 0), s);
 }
 
 }  // namespace umapb

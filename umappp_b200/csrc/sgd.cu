@@ -308,36 +308,47 @@ __device__ __forceinline__ T floor_eps(T d2) {
 
 // Segments: the firing events of one head in one epoch are contiguous in the
 // event list (it follows the edges' CSR order).  A segment is a run of at most
-// SEG_MAX events of one head: runs are also cut at every SEG_MAX-aligned
+// seg_max events of one head: runs are also cut at every seg_max-aligned
 // position of the epoch, which bounds the longest sequential chain (hub heads
 // have hundreds of edges) at the cost of a few extra segments.  Segments
 // partition the window's events in order: seg_pos[s] is the first event of
 // segment s, seg_pos[S] = the event total, and the segments of epoch w are
 // [seg_first[w], seg_first[w + 1]).  Built without atomics by a count / scan /
 // write over fixed event ranges, so the list is deterministic.
+//
+// seg_max: the segments of one head run concurrently from the same starting
+// position, so a split hub takes its steps from a stale copy of itself.  When
+// an epoch holds fewer events than the epoch kernel keeps threads resident,
+// every segment is in flight at once and splitting buys no parallelism, so
+// heads are cut only every SEG_MAX_FEW events (at 2,000 points this lifts the
+// mean trustworthiness by about 0.002, to that of the serial order).  Larger
+// epochs use SEG_MAX, which keeps the kernel's rounds balanced (at 1M points,
+// 64-event segments made the SGD about 1.6x slower and moved the edge
+// cross-entropy further from the reference's).
 constexpr int SEG_MAX = 8;
+constexpr int SEG_MAX_FEW = 64;
 constexpr int SEG_BLOCK = 256;
 constexpr int SEG_ITEMS = 8;    // events per thread in the segment passes
 
 __device__ __forceinline__ bool seg_start(int64_t e, const int2* __restrict__ ht, const int64_t* __restrict__ starts,
-                                          int W) {
+                                          int W, int seg_max) {
     int lo = 0, hi = W - 1;   // epoch of e: the last w with starts[w] <= e
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
         if (starts[mid] <= e) lo = mid; else hi = mid - 1;
     }
     const int64_t s0 = starts[lo];
-    return e == s0 || ((e - s0) % SEG_MAX) == 0 || ht[e - 1].x != ht[e].x;
+    return e == s0 || ((e - s0) % seg_max) == 0 || ht[e - 1].x != ht[e].x;
 }
 
 __global__ void __launch_bounds__(SEG_BLOCK) seg_count_kernel(int64_t total, const int2* __restrict__ ht,
-                                                              const int64_t* __restrict__ starts, int W,
+                                                              const int64_t* __restrict__ starts, int W, int seg_max,
                                                               int64_t* __restrict__ block_counts) {
     const int64_t base = static_cast<int64_t>(blockIdx.x) * SEG_BLOCK * SEG_ITEMS;
     int c = 0;
     for (int i = 0; i < SEG_ITEMS; ++i) {
         const int64_t e = base + static_cast<int64_t>(i) * SEG_BLOCK + threadIdx.x;
-        if (e < total && seg_start(e, ht, starts, W)) ++c;
+        if (e < total && seg_start(e, ht, starts, W, seg_max)) ++c;
     }
     typedef cub::BlockReduce<int, SEG_BLOCK> Reduce;
     __shared__ typename Reduce::TempStorage tmp;
@@ -348,7 +359,7 @@ __global__ void __launch_bounds__(SEG_BLOCK) seg_count_kernel(int64_t total, con
 // Writes segment starts in event order: block b covers events
 // [b * SEG_BLOCK * SEG_ITEMS, ...), item-major so each pass is coalesced.
 __global__ void __launch_bounds__(SEG_BLOCK) seg_write_kernel(int64_t total, const int2* __restrict__ ht,
-                                                              const int64_t* __restrict__ starts, int W,
+                                                              const int64_t* __restrict__ starts, int W, int seg_max,
                                                               const int64_t* __restrict__ block_offsets,
                                                               int64_t* __restrict__ seg_pos) {
     typedef cub::BlockScan<int, SEG_BLOCK> Scan;
@@ -357,7 +368,7 @@ __global__ void __launch_bounds__(SEG_BLOCK) seg_write_kernel(int64_t total, con
     int64_t out = block_offsets[blockIdx.x];
     for (int i = 0; i < SEG_ITEMS; ++i) {
         const int64_t e = base + static_cast<int64_t>(i) * SEG_BLOCK + threadIdx.x;
-        const int f = (e < total && seg_start(e, ht, starts, W)) ? 1 : 0;
+        const int f = (e < total && seg_start(e, ht, starts, W, seg_max)) ? 1 : 0;
         int prefix, sum;
         Scan(tmp).ExclusiveSum(f, prefix, sum);
         if (f) seg_pos[out + prefix] = e;
@@ -663,11 +674,13 @@ void SgdEngine<T>::setup(const DeviceEpochs<T>* ep, cudaStream_t s, int base_epo
         UMAPB_CUDA(cudaMemcpyAsync(enneg_.get(), ep->enneg0.get(), ep->nnz * sizeof(T), cudaMemcpyDeviceToDevice, s));
     }
     state_epoch_ = base_epoch_;
-    window_begin_ = window_end_ = base_epoch_;
-    ht_.release();
-    nneg_.release();
-    epoch_offsets_.release();
-    host_epoch_offsets_.clear();
+    for (Window& w : win_) {
+        w.begin = w.end = base_epoch_;
+        w.ht.release();
+        w.nneg.release();
+        w.epoch_offsets.release();
+        w.host_epoch_offsets.clear();
+    }
 }
 
 template <typename T>
@@ -686,8 +699,9 @@ void SgdEngine<T>::state_at(int epoch, T* enext, T* enneg, cudaStream_t s) {
 }
 
 template <typename T>
-void SgdEngine<T>::build_window(int first, int last_wanted, cudaStream_t s) {
+void SgdEngine<T>::build_window(Window& win, int first, int last_wanted, cudaStream_t s) {
     const int64_t nnz = ep_->nnz;
+    win.begin = win.end = first;   // empty until complete
     // bring the state to 'first'
     if (state_epoch_ != first) {
         if (state_epoch_ > first) {
@@ -739,26 +753,29 @@ void SgdEngine<T>::build_window(int first, int last_wanted, cudaStream_t s) {
     const int64_t events = h[Wk];
 
     // the window buffers are kept across windows (and runs) and only grow
-    ht_.reserve(events, s);
-    nneg_.reserve(events, s);
+    win.ht.reserve(events, s);
+    win.nneg.reserve(events, s);
     DevArray<int> status(1, s);
     status.zero(s);
     if (nnz) {
         sched_write_kernel<T><<<static_cast<unsigned>(nblocks), SCHED_BLOCK, 0, s>>>(
             nnz, ep_->heads.get(), ep_->targets.get(), ep_->eps.get(), enext_.get(), enneg_.get(),
-            ep_->negative_sample_rate, first, Wk, offsets.get(), ht_.get(), nneg_.get(), status.get());
+            ep_->negative_sample_rate, first, Wk, offsets.get(), win.ht.get(), win.nneg.get(), status.get());
         UMAPB_LAUNCH_CHECK();
     }
-    epoch_offsets_.allocate(Wk + 1, s);
-    UMAPB_CUDA(cudaMemcpyAsync(epoch_offsets_.get(), h.data(), (Wk + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    win.epoch_offsets.allocate(Wk + 1, s);
+    UMAPB_CUDA(cudaMemcpyAsync(win.epoch_offsets.get(), h.data(), (Wk + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
 
     // head segments of every epoch in the window (count, scan, write, per-epoch first segment)
+    const int64_t resident_threads =
+        static_cast<int64_t>(sm_count()) * sgd_2d_resident(variant_, block_) * block_;
+    const int seg_max = events < resident_threads * Wk ? SEG_MAX_FEW : SEG_MAX;
     const int64_t seg_blocks = std::max<int64_t>((events + SEG_BLOCK * SEG_ITEMS - 1) / (SEG_BLOCK * SEG_ITEMS), 1);
     DevArray<int64_t> bcount(seg_blocks + 1, s), boff(seg_blocks + 1, s);
     bcount.zero(s);
     if (events > 0) {
-        seg_count_kernel<<<static_cast<unsigned>(seg_blocks), SEG_BLOCK, 0, s>>>(events, ht_.get(), epoch_offsets_.get(),
-                                                                               Wk, bcount.get());
+        seg_count_kernel<<<static_cast<unsigned>(seg_blocks), SEG_BLOCK, 0, s>>>(events, win.ht.get(), win.epoch_offsets.get(),
+                                                                               Wk, seg_max, bcount.get());
         UMAPB_LAUNCH_CHECK();
     }
     {
@@ -770,31 +787,31 @@ void SgdEngine<T>::build_window(int first, int last_wanted, cudaStream_t s) {
     int64_t nseg = 0;
     UMAPB_CUDA(cudaMemcpyAsync(&nseg, boff.get() + seg_blocks, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     UMAPB_SYNC(s);
-    seg_pos_.reserve(nseg + 1, s);
-    UMAPB_CUDA(cudaMemcpyAsync(seg_pos_.get() + nseg, &events, sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    win.seg_pos.reserve(nseg + 1, s);
+    UMAPB_CUDA(cudaMemcpyAsync(win.seg_pos.get() + nseg, &events, sizeof(int64_t), cudaMemcpyHostToDevice, s));
     if (events > 0) {
-        seg_write_kernel<<<static_cast<unsigned>(seg_blocks), SEG_BLOCK, 0, s>>>(events, ht_.get(), epoch_offsets_.get(),
-                                                                               Wk, boff.get(), seg_pos_.get());
+        seg_write_kernel<<<static_cast<unsigned>(seg_blocks), SEG_BLOCK, 0, s>>>(events, win.ht.get(), win.epoch_offsets.get(),
+                                                                               Wk, seg_max, boff.get(), win.seg_pos.get());
         UMAPB_LAUNCH_CHECK();
     }
-    seg_first_.allocate(Wk + 1, s);
-    seg_first_kernel<<<grid_for(Wk + 1, 128), 128, 0, s>>>(seg_pos_.get(), nseg, epoch_offsets_.get(), Wk,
-                                                            seg_first_.get());
+    win.seg_first.allocate(Wk + 1, s);
+    seg_first_kernel<<<grid_for(Wk + 1, 128), 128, 0, s>>>(win.seg_pos.get(), nseg, win.epoch_offsets.get(), Wk,
+                                                            win.seg_first.get());
     UMAPB_LAUNCH_CHECK();
-    host_seg_first_.resize(Wk + 1);
-    UMAPB_CUDA(cudaMemcpyAsync(host_seg_first_.data(), seg_first_.get(), (Wk + 1) * sizeof(int64_t),
+    win.host_seg_first.resize(Wk + 1);
+    UMAPB_CUDA(cudaMemcpyAsync(win.host_seg_first.data(), win.seg_first.get(), (Wk + 1) * sizeof(int64_t),
                                cudaMemcpyDeviceToHost, s));
 
-    host_epoch_offsets_.assign(h.begin(), h.begin() + Wk + 1);
-    build_slices(nseg, Wk, s);
+    win.host_epoch_offsets.assign(h.begin(), h.begin() + Wk + 1);
+    build_slices(win, nseg, Wk, s);
     int st = 0;
     UMAPB_CUDA(cudaMemcpyAsync(&st, status.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
     UMAPB_SYNC(s);
     require(st == DEV_OK, "a negative-sample count exceeded 65535");
-    if (check_schedule()) verify_window(first, Wk, s);
-    window_begin_ = first;
-    window_end_ = first + Wk;
-    state_epoch_ = window_end_;
+    if (check_schedule()) verify_window(win, first, Wk, s);
+    win.begin = first;
+    win.end = first + Wk;
+    state_epoch_ = win.end;
 }
 
 // Autotuner: times the 2-d epoch kernel with each candidate launch shape on a
@@ -802,16 +819,16 @@ void SgdEngine<T>::build_window(int first, int last_wanted, cudaStream_t s) {
 // fastest, and remembers it per size class (log2 of the epoch's events).
 template <typename T>
 template <class Launch>
-void SgdEngine<T>::tune(T* Y, int num_dim, int first, int stop, Launch& launch, cudaStream_t s) {
+void SgdEngine<T>::tune(T* Y, int num_dim, int first, int stop, const Window& win, Launch& launch, cudaStream_t s) {
     static std::mutex mu;
     static std::map<int, std::pair<int, int>> cache;   // size class -> (block, variant)
     int w = -1;
     for (int e = (first + stop) / 2; e < stop && w < 0; ++e) {
-        const int ww = e - window_begin_;
-        if (host_seg_first_[ww + 1] > host_seg_first_[ww]) w = ww;
+        const int ww = e - win.begin;
+        if (win.host_seg_first[ww + 1] > win.host_seg_first[ww]) w = ww;
     }
     if (w < 0) return;
-    const int64_t events = host_epoch_offsets_[w + 1] - host_epoch_offsets_[w];
+    const int64_t events = win.host_epoch_offsets[w + 1] - win.host_epoch_offsets[w];
     int key = 0;
     while ((int64_t(1) << key) < events) ++key;
     {
@@ -831,7 +848,7 @@ void SgdEngine<T>::tune(T* Y, int num_dim, int first, int stop, Launch& launch, 
         for (int blk : {128, 256}) {
             UMAPB_CUDA(cudaMemcpyAsync(scratch.get(), Y, total * sizeof(T), cudaMemcpyDeviceToDevice, s));
             UMAPB_CUDA(cudaEventRecord(a, s));
-            launch(scratch.get(), window_begin_ + w, w, blk, v);
+            launch(scratch.get(), win, win.begin + w, w, blk, v);
             UMAPB_CUDA(cudaEventRecord(b, s));
             UMAPB_CUDA(cudaEventSynchronize(b));
             float t = 0;
@@ -851,7 +868,7 @@ void SgdEngine<T>::tune(T* Y, int num_dim, int first, int stop, Launch& launch, 
 
 template <typename T>
 void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double b, double gamma, double learning_rate,
-                       uint64_t seed, cudaStream_t s, float* ms_schedule, float* ms_sgd) {
+                       uint64_t seed, cudaStream_t caller, float* ms_schedule, float* ms_sgd) {
     if (ms_schedule) *ms_schedule = 0;
     if (ms_sgd) *ms_sgd = 0;
     if (last <= first) return;
@@ -868,19 +885,16 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
     p.inst_start = inst_start_;
     p.num_inst = num_inst_;
     const T lr = static_cast<T>(learning_rate);
-
-    cudaEvent_t ev[4];
-    for (auto& e : ev) e = event_get();
-    float sched_ms = 0, sgd_ms = 0;
     const int blocks_gen = sm_count() * 8;
+    cudaStream_t s = nullptr;   // the epochs' stream (below)
 
     // One epoch launch of window slot w on Yp, with the 2-d kernel's block size and variant.
-    auto launch = [&](T* Yp, int e_abs, int w, int block, int variant) {
+    auto launch = [&](T* Yp, const Window& win, int e_abs, int w, int block, int variant) {
         const T epoch_t = static_cast<T>(e_abs);
         // alpha = lr * (1 - epoch / num_epochs) in the reference's types (optimize_layout.hpp:132-133)
         p.alpha = static_cast<T>(static_cast<double>(lr) * (1.0 - static_cast<double>(epoch_t / static_cast<T>(total))));
         p.epoch = static_cast<uint32_t>(e_abs);
-        const int64_t nsegs = host_seg_first_[w + 1] - host_seg_first_[w];
+        const int64_t nsegs = win.host_seg_first[w + 1] - win.host_seg_first[w];
         if (nsegs == 0) return;
         const bool use_2d = std::is_same<T, float>::value && num_dim == 2;
         const int blk = use_2d ? block : 128;
@@ -894,94 +908,155 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
         // taken in that order: by the grid-stride loop's rounds when the epoch
         // holds several rounds of segments, and by consecutive launches over
         // slot ranges (L of them, slices split evenly) to make up the rest.
-        const int P = buckets_;
+        const int P = win.buckets;
         const int64_t threads = static_cast<int64_t>(std::min<int64_t>(g, resident)) * blk;
         const int64_t rounds = (nsegs + threads - 1) / threads;
         const int L = static_cast<int>(std::min<int64_t>(P, std::max<int64_t>(1, (P + rounds - 1) / rounds)));
-        const int64_t* off = host_bucket_off_.data() + static_cast<size_t>(w) * (P + 1);
+        const int64_t* off = win.host_bucket_off.data() + static_cast<size_t>(w) * (P + 1);
+        const int32_t* order = win.ordered ? win.seg_order.get() : nullptr;
         for (int l = 0; l < L; ++l) {
             const int64_t slot0 = off[(P * l) / L], slot1 = off[(P * (l + 1)) / L];
             if (slot1 <= slot0) continue;
             const unsigned gl = grid_for(slot1 - slot0, blk, static_cast<unsigned>(resident * grid_multiple()));
             if (use_2d) {
                 if constexpr (std::is_same<T, float>::value) {
-                    SGD_2D_VARIANTS[variant].kernel<<<gl, blk, 0, s>>>(slices_ordered_ ? seg_order_.get() : nullptr, host_seg_first_[w], slot0,
-                                                                       slot1, seg_pos_.get(), ht_.get(), nneg_.get(),
+                    SGD_2D_VARIANTS[variant].kernel<<<gl, blk, 0, s>>>(order, win.host_seg_first[w], slot0, slot1,
+                                                                       win.seg_pos.get(), win.ht.get(), win.nneg.get(),
                                                                        reinterpret_cast<float2*>(Yp), p);
                 }
             } else {
-                sgd_epoch_generic<T><<<gl, 128, 0, s>>>(slices_ordered_ ? seg_order_.get() : nullptr, host_seg_first_[w], slot0, slot1,
-                                                        seg_pos_.get(), ht_.get(), nneg_.get(), Yp, num_dim, p);
+                sgd_epoch_generic<T><<<gl, 128, 0, s>>>(order, win.host_seg_first[w], slot0, slot1, win.seg_pos.get(),
+                                                        win.ht.get(), win.nneg.get(), Yp, num_dim, p);
             }
             UMAPB_LAUNCH_CHECK();
         }
     };
 
-    int e = first;
-    while (e < last) {
-        if (e < window_begin_ || e >= window_end_) {
-            UMAPB_CUDA(cudaEventRecord(ev[0], s));
-            build_window(e, last, s);
-            UMAPB_CUDA(cudaEventRecord(ev[1], s));
-            UMAPB_CUDA(cudaEventSynchronize(ev[1]));
+    // The epochs run on a high-priority stream s and windows are built on a
+    // default-priority stream s2 while the epochs of the previous window run:
+    // the host enqueues a window's epochs, then builds the next window (the
+    // build synchronises only its own stream), so the GPU runs both at once,
+    // the block scheduler giving the epochs first claim on the SMs.  A window
+    // buffer is rebuilt only after the epochs that read it have finished (host
+    // wait on its 'done' event), which also orders the release of any buffer
+    // the rebuild grows.  Both streams start after the caller's work on
+    // 'caller' (layout, schedule state); the host waits for the last epoch.
+    s = stream_get(true);
+    cudaStream_t s2 = stream_get();
+    cudaEvent_t start = event_get(), finish = event_get();
+    cudaEvent_t done[2] = {event_get(), event_get()};
+    bool pending[2] = {false, false};
+    std::vector<cudaEvent_t> marks;            // per window: SGD begin, SGD end (on s)
+    std::vector<cudaGraphExec_t> execs;
+    auto cleanup = [&] {
+        for (auto x : execs) cudaGraphExecDestroy(x);
+        for (auto x : marks) event_put(x);
+        event_put(start);
+        event_put(finish);
+        event_put(done[0]);
+        event_put(done[1]);
+        stream_put(s2);
+        stream_put(s);
+    };
+    try {
+        UMAPB_CUDA(cudaEventRecord(start, caller));
+        UMAPB_CUDA(cudaStreamWaitEvent(s, start, 0));
+        UMAPB_CUDA(cudaStreamWaitEvent(s2, start, 0));
+        auto find = [&](int e) {
+            for (int i = 0; i < 2; ++i)
+                if (win_[i].begin <= e && e < win_[i].end) return i;
+            return -1;
+        };
+        auto build_into = [&](int i, int e) {
+            if (pending[i]) {
+                UMAPB_CUDA(cudaEventSynchronize(done[i]));
+                pending[i] = false;
+            }
+            build_window(win_[i], e, last, s2);
+        };
+        int e = first;
+        int cur = find(e);
+        if (cur < 0) build_into(cur = 0, e);
+        while (true) {
+            const Window& win = win_[cur];
+            const int stop = std::min(last, win.end);
+            if (autotune && std::is_same<T, float>::value && num_dim == 2) tune(Y, num_dim, e, stop, win, launch, s);
+            marks.push_back(event_get());
+            marks.push_back(event_get());
+            UMAPB_CUDA(cudaEventRecord(marks[marks.size() - 2], s));
+            if (use_graphs) {
+                // this window's epoch launches as one CUDA graph
+                cudaGraph_t graph = nullptr;
+                UMAPB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+                for (int x = e; x < stop; ++x) launch(Y, win, x, x - win.begin, block_, variant_);
+                UMAPB_CUDA(cudaStreamEndCapture(s, &graph));
+                cudaGraphExec_t exec = nullptr;
+                const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+                cudaGraphDestroy(graph);
+                if (ie != cudaSuccess) cuda_fail(ie, "cudaGraphInstantiate", __FILE__, __LINE__);
+                execs.push_back(exec);
+                UMAPB_CUDA(cudaGraphLaunch(exec, s));
+            } else {
+                for (int x = e; x < stop; ++x) launch(Y, win, x, x - win.begin, block_, variant_);
+            }
+            UMAPB_CUDA(cudaEventRecord(marks.back(), s));
+            UMAPB_CUDA(cudaEventRecord(done[cur], s));
+            pending[cur] = true;
+            e = stop;
+            if (e >= last) break;
+            int next = find(e);
+            if (next < 0) build_into(next = 1 - cur, e);
+            cur = next;
+        }
+        UMAPB_CUDA(cudaEventRecord(finish, s));
+        UMAPB_CUDA(cudaEventSynchronize(finish));
+        // SGD: the windows' epoch spans on s; schedule: the rest of the span
+        // from the start to the last epoch (the first build and any wait for
+        // a build that the epochs did not hide)
+        float sgd_ms = 0, all_ms = 0;
+        for (size_t i = 0; i < marks.size(); i += 2) {
             float t = 0;
-            UMAPB_CUDA(cudaEventElapsedTime(&t, ev[0], ev[1]));
-            sched_ms += t;
+            UMAPB_CUDA(cudaEventElapsedTime(&t, marks[i], marks[i + 1]));
+            sgd_ms += t;
         }
-        const int stop = std::min(last, window_end_);
-        if (autotune && std::is_same<T, float>::value && num_dim == 2) tune(Y, num_dim, e, stop, launch, s);
-        UMAPB_CUDA(cudaEventRecord(ev[2], s));
-        // optionally record this window's epoch launches as one CUDA graph
-        cudaGraph_t graph = nullptr;
-        if (use_graphs) UMAPB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        for (; e < stop; ++e) launch(Y, e, e - window_begin_, block_, variant_);
-        if (use_graphs) {
-            UMAPB_CUDA(cudaStreamEndCapture(s, &graph));
-            cudaGraphExec_t exec = nullptr;
-            UMAPB_CUDA(cudaGraphInstantiate(&exec, graph, 0));
-            UMAPB_CUDA(cudaGraphLaunch(exec, s));
-            UMAPB_SYNC(s);
-            cudaGraphExecDestroy(exec);
-            cudaGraphDestroy(graph);
-        }
-        UMAPB_CUDA(cudaEventRecord(ev[3], s));
-        UMAPB_CUDA(cudaEventSynchronize(ev[3]));
-        float t = 0;
-        UMAPB_CUDA(cudaEventElapsedTime(&t, ev[2], ev[3]));
-        sgd_ms += t;
+        UMAPB_CUDA(cudaEventElapsedTime(&all_ms, start, finish));
+        if (ms_schedule) *ms_schedule = std::max(0.0f, all_ms - sgd_ms);
+        if (ms_sgd) *ms_sgd = sgd_ms;
+    } catch (...) {
+        cudaStreamSynchronize(s);
+        cudaStreamSynchronize(s2);
+        cleanup();
+        throw;
     }
-    for (auto& x : ev) event_put(x);
-    if (ms_schedule) *ms_schedule = sched_ms;
-    if (ms_sgd) *ms_sgd = sgd_ms;
+    cleanup();
 }
-
 // Orders every epoch's segments of the window by head slice (see the epoch
 // kernels): counts per (epoch, slice), slot offsets on the host, scatter.
 template <typename T>
-void SgdEngine<T>::build_slices(int64_t nseg, int W, cudaStream_t s) {
-    const int P = buckets_ = std::max(1, std::min(min_phases, 64));
-    UMAPB_SYNC(s);   // host_seg_first_ (copied by the caller) is read below
-    host_bucket_off_.assign(static_cast<size_t>(W) * (P + 1), 0);
+void SgdEngine<T>::build_slices(Window& win, int64_t nseg, int W, cudaStream_t s) {
+    const int P = win.buckets = std::max(1, std::min(min_phases, 64));
+    UMAPB_SYNC(s);   // win.host_seg_first (copied by the caller) is read below
+    win.host_bucket_off.assign(static_cast<size_t>(W) * (P + 1), 0);
     if (num_inst_ <= 1 || W * P > SLICE_MAX_BINS) {
         // slices are consecutive segment ranges: identity order (with several
         // instances and too many bins for one block, slices of the whole row range)
-        slices_ordered_ = false;
+        win.ordered = false;
         DevArray<int64_t> off(static_cast<size_t>(W) * (P + 1), s);
         slice_bounds_kernel<<<grid_for(static_cast<size_t>(W) * (P + 1), 128), 128, 0, s>>>(
-            seg_pos_.get(), ht_.get(), seg_first_.get(), W, ep_->n, P, off.get());
+            win.seg_pos.get(), win.ht.get(), win.seg_first.get(), W, ep_->n, P, off.get());
         UMAPB_LAUNCH_CHECK();
-        UMAPB_CUDA(cudaMemcpyAsync(host_bucket_off_.data(), off.get(), host_bucket_off_.size() * sizeof(int64_t),
+        UMAPB_CUDA(cudaMemcpyAsync(win.host_bucket_off.data(), off.get(), win.host_bucket_off.size() * sizeof(int64_t),
                                    cudaMemcpyDeviceToHost, s));
         UMAPB_SYNC(s);
         return;
     }
-    slices_ordered_ = true;
-    seg_order_.reserve(std::max<int64_t>(nseg, 1), s);
+    win.ordered = true;
+    win.seg_order.reserve(std::max<int64_t>(nseg, 1), s);
     DevArray<int> counts(static_cast<size_t>(W) * P, s);
     counts.zero(s);
     const unsigned blocks = static_cast<unsigned>((nseg + SLICE_BLOCK - 1) / SLICE_BLOCK);
     if (nseg > 0) {
-        seg_bucket_kernel<<<blocks, SLICE_BLOCK, 0, s>>>(nseg, seg_pos_.get(), ht_.get(), seg_first_.get(), W,
+        seg_bucket_kernel<<<blocks, SLICE_BLOCK, 0, s>>>(nseg, win.seg_pos.get(), win.ht.get(), win.seg_first.get(), W,
                                                          inst_start_, num_inst_, ep_->n, P, counts.get(), nullptr,
                                                          nullptr);
         UMAPB_LAUNCH_CHECK();
@@ -991,20 +1066,20 @@ void SgdEngine<T>::build_slices(int64_t nseg, int W, cudaStream_t s) {
     UMAPB_SYNC(s);
     std::vector<int> cursor(static_cast<size_t>(W) * P);
     for (int w = 0; w < W; ++w) {
-        int64_t acc = host_seg_first_[w];
+        int64_t acc = win.host_seg_first[w];
         for (int b = 0; b < P; ++b) {
-            host_bucket_off_[static_cast<size_t>(w) * (P + 1) + b] = acc;
-            cursor[static_cast<size_t>(w) * P + b] = static_cast<int>(acc - host_seg_first_[w]);
+            win.host_bucket_off[static_cast<size_t>(w) * (P + 1) + b] = acc;
+            cursor[static_cast<size_t>(w) * P + b] = static_cast<int>(acc - win.host_seg_first[w]);
             acc += hc[static_cast<size_t>(w) * P + b];
         }
-        host_bucket_off_[static_cast<size_t>(w) * (P + 1) + P] = acc;
+        win.host_bucket_off[static_cast<size_t>(w) * (P + 1) + P] = acc;
     }
     if (nseg > 0) {
         DevArray<int> d_cursor(cursor.size(), s);
         UMAPB_CUDA(cudaMemcpyAsync(d_cursor.get(), cursor.data(), cursor.size() * sizeof(int), cudaMemcpyHostToDevice, s));
-        seg_bucket_kernel<<<blocks, SLICE_BLOCK, 0, s>>>(nseg, seg_pos_.get(), ht_.get(), seg_first_.get(), W,
+        seg_bucket_kernel<<<blocks, SLICE_BLOCK, 0, s>>>(nseg, win.seg_pos.get(), win.ht.get(), win.seg_first.get(), W,
                                                          inst_start_, num_inst_, ep_->n, P, nullptr, d_cursor.get(),
-                                                         seg_order_.get());
+                                                         win.seg_order.get());
         UMAPB_LAUNCH_CHECK();
         UMAPB_SYNC(s);   // the cursor vector is the copy's source
     }
@@ -1030,7 +1105,7 @@ __global__ void window_stats_kernel(const int2* __restrict__ ht, const uint16_t*
 }
 
 template <typename T>
-void SgdEngine<T>::verify_window(int first, int W, cudaStream_t s) {
+void SgdEngine<T>::verify_window(const Window& win, int first, int W, cudaStream_t s) {
     const int64_t nnz = ep_->nnz;
     DevArray<T> en(nnz, s), enn(nnz, s);
     state_at(first, en.get(), enn.get(), s);
@@ -1044,7 +1119,7 @@ void SgdEngine<T>::verify_window(int first, int W, cudaStream_t s) {
             nnz, ep_->eps.get(), en.get(), enn.get(), ep_->negative_sample_rate, first, W, totals.get());
         UMAPB_LAUNCH_CHECK();
     }
-    window_stats_kernel<<<W, 256, 0, s>>>(ht_.get(), nneg_.get(), epoch_offsets_.get(), negs.get(), disorder.get());
+    window_stats_kernel<<<W, 256, 0, s>>>(win.ht.get(), win.nneg.get(), win.epoch_offsets.get(), negs.get(), disorder.get());
     UMAPB_LAUNCH_CHECK();
     std::vector<unsigned long long> ht_tot(2 * static_cast<size_t>(W)), hn(W), hd(W);
     UMAPB_CUDA(cudaMemcpyAsync(ht_tot.data(), totals.get(), ht_tot.size() * sizeof(unsigned long long),
@@ -1053,7 +1128,7 @@ void SgdEngine<T>::verify_window(int first, int W, cudaStream_t s) {
     UMAPB_CUDA(cudaMemcpyAsync(hd.data(), disorder.get(), W * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     UMAPB_SYNC(s);
     for (int w = 0; w < W; ++w) {
-        const unsigned long long ev = static_cast<unsigned long long>(host_epoch_offsets_[w + 1] - host_epoch_offsets_[w]);
+        const unsigned long long ev = static_cast<unsigned long long>(win.host_epoch_offsets[w + 1] - win.host_epoch_offsets[w]);
         require(ev == ht_tot[2 * w] && hn[w] == ht_tot[2 * w + 1] && hd[w] == 0,
                 "schedule window self-check failed at epoch " + std::to_string(first + w), UMAPB_ERR_CUDA);
     }

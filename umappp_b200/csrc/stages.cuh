@@ -177,15 +177,29 @@ public:
     int variant() const { return variant_; }   // 2-d kernel variant (sgd.cu, SGD_2D_VARIANTS)
 
 private:
-    void build_window(int first, int last_wanted, cudaStream_t s);
-    void verify_window(int first, int W, cudaStream_t s);
-    void build_slices(int64_t nseg, int W, cudaStream_t s);
-    DevArray<int32_t> seg_order_;            // per epoch: its segments by head slice (offsets from seg_first)
-    std::vector<int64_t> host_bucket_off_;   // per epoch: P + 1 slot offsets of the slices
-    int buckets_ = 8;
-    bool slices_ordered_ = false;            // seg_order_ in use (several instances)
+    // One window of consecutive epochs: every firing event (head, tail) with
+    // its negative-sample count, grouped by epoch and head segment, and each
+    // epoch's segments ordered by head slice.  The engine keeps two, so that
+    // the next window is built (on a second stream) while the epochs of the
+    // current one run.
+    struct Window {
+        int begin = 0, end = 0;                   // epochs [begin, end)
+        DevArray<int2> ht;
+        DevArray<uint16_t> nneg;
+        DevArray<int64_t> seg_pos;                // first event of every head segment, plus the event total (see sgd.cu)
+        DevArray<int64_t> seg_first;              // per epoch: index of its first segment (end - begin + 1)
+        DevArray<int64_t> epoch_offsets;          // end - begin + 1 entries
+        DevArray<int32_t> seg_order;              // per epoch: its segments by head slice (offsets from seg_first)
+        std::vector<int64_t> host_seg_first, host_epoch_offsets;
+        std::vector<int64_t> host_bucket_off;     // per epoch: buckets + 1 slot offsets of the slices
+        int buckets = 8;
+        bool ordered = false;                     // seg_order in use (several instances)
+    };
+    void build_window(Window& win, int first, int last_wanted, cudaStream_t s);
+    void verify_window(const Window& win, int first, int W, cudaStream_t s);
+    void build_slices(Window& win, int64_t nseg, int W, cudaStream_t s);
     template <class Launch>
-    void tune(T* Y, int num_dim, int first, int stop, Launch& launch, cudaStream_t s);
+    void tune(T* Y, int num_dim, int first, int stop, const Window& win, Launch& launch, cudaStream_t s);
     static int default_variant();
     int block_ = 256, variant_ = default_variant();
     const DeviceEpochs<T>* ep_ = nullptr;
@@ -194,14 +208,7 @@ private:
     int base_epoch_ = 0;
     DevArray<T> enext_, enneg_;    // schedule state at state_epoch_
     int state_epoch_ = 0;          // epoch the state arrays describe
-    int window_begin_ = 0, window_end_ = 0;
-    DevArray<int2> ht_;
-    DevArray<uint16_t> nneg_;
-    DevArray<int64_t> seg_pos_;         // first event of every head segment, plus the event total (see sgd.cu)
-    DevArray<int64_t> seg_first_;       // per epoch: index of its first segment (window_end_ - window_begin_ + 1)
-    std::vector<int64_t> host_seg_first_;
-    DevArray<int64_t> epoch_offsets_;   // window_end_ - window_begin_ + 1 entries
-    std::vector<int64_t> host_epoch_offsets_;
+    Window win_[2];
 };
 
 // ---- adjoint (adjoint.cu) ----------------------------------------------------
