@@ -173,7 +173,8 @@ def test_partial_runs_follow_the_same_schedule(umap):
 @pytest.mark.parametrize("n,epochs", [(3000, 500), (20000, 200)])
 def test_event_windows_self_check(umap, monkeypatch, n, epochs):
     # every window's event lists are checked on the device against the
-    # schedule recomputed from the initial state (counts, negatives, head order)
+    # schedule recomputed from the initial state (counts, negatives, head order),
+    # and its head segments (in order, one head each, at most the cap long)
     monkeypatch.setenv("UMAPB_CHECK_SCHEDULE", "1")
     X = oracle.gaussian_mixture(n, 12, 5, 4.0, seed=n, dtype=np.float32)
     Y = np.zeros((n, 2), np.float32)

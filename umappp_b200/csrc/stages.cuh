@@ -193,6 +193,7 @@ private:
         std::vector<int64_t> host_seg_first, host_epoch_offsets;
         std::vector<int64_t> host_bucket_off;     // per epoch: buckets + 1 slot offsets of the slices
         int buckets = 8;
+        int seg_max = 8;                          // longest segment
         bool ordered = false;                     // seg_order in use (several instances)
     };
     void build_window(Window& win, int first, int last_wanted, cudaStream_t s);
