@@ -46,8 +46,8 @@ CONFIGS = {
 }
 METRIC = "end-to-end s & SGD edge-updates/s, 1M pts; FP32/batched vs plain at equal trust"
 # DRAM bytes (read + write) per launch of the dominant kernels, from one ncu
-# capture each (profiles/knn_tc16_kernel.md, profiles/sgd_epoch_2d_f32.md).
-TRAFFIC = {"mixture_1m": {"knn_tc16_kernel": 3.94e9 + 0.22e9, "sgd_epoch_2d_f32": 95.9e6 + 0.8e6}}
+# capture (profiles/launches_mixture_1m.md; knn_tc16_kernel.md, sgd_epoch_2d_f32.md).
+TRAFFIC = {"mixture_1m": {"knn_tc16_kernel": 4.116e9 + 0.216e9, "sgd_epoch_2d_f32": 91.3e6 + 0.2e6}}
 # Batched workload: 64 independent instances, sizes log-uniform in [500, 50000],
 # 30 dims, float32 5-cluster mixtures, k = 15, 200 epochs.
 BATCH = {"instances": 64, "min": 500, "max": 50_000, "dim": 30, "clusters": 5, "k": 15, "epochs": 200}
