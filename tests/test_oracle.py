@@ -237,3 +237,60 @@ def test_pipeline_quality_fixture_reproduces(oracle_mod, dtype):
     t, ce = mk.reference_run(getattr(np, dtype), 0)
     assert abs(t - ref["trust"][0]) < 1e-12
     assert abs(ce - ref["cross_entropy"][0]) <= 1e-9 * abs(ce)
+
+
+def test_adjoint_matches_finite_differences(oracle_mod):
+    # The adjoint (loss and gradient of the fuzzy cross-entropy with respect to
+    # the embedding and to a, b) against FP64 central differences, h = 1e-6, on
+    # a 20,000 x 30 FP64 mixture of 10 clusters, k = 15, 2-d layout.  The device
+    # kernel is compared with this restatement in test_gpu_stages.py.  The loss
+    # sums ~490,000 edge terms of ~1 each, so a difference quotient carries
+    # ~1e-4 of rounding noise: bars 1e-3 absolute for coordinates (gradients up
+    # to ~20 here) and 1e-6 relative for a and b.
+    X = oracle.gaussian_mixture(20000, 30, 10, 4.0, seed=20000, dtype=np.float64)
+    nl = neighbors_of(X, 15)
+    w, _, _ = oracle.neighbor_similarities(nl)
+    g = oracle.combine_neighbor_sets(w, 1.0)
+    rng = np.random.default_rng(3)
+    Y = rng.normal(size=(20000, 2)) * 3
+    a, b = oracle.find_ab(1.0, 0.1)
+    loss, gY, gab = oracle.loss_grad(g, Y, a, b)
+    # the loss is the cross-entropy without its w-only constant sum w log w + (1 - w) log(1 - w)
+    wv = g.val.astype(np.float64)
+    const = float(np.sum(np.where(wv > 0, wv * np.log(np.where(wv > 0, wv, 1.0)), 0.0)) +
+                  np.sum(np.where(wv < 1, (1 - wv) * np.log(np.where(wv < 1, 1 - wv, 1.0)), 0.0)))
+    assert abs(loss + const - oracle.cross_entropy(g, Y, a, b)) <= 1e-9 * abs(loss)
+    h = 1e-6
+    for _ in range(24):
+        i, d = int(rng.integers(20000)), int(rng.integers(2))
+        Yp, Ym = Y.copy(), Y.copy()
+        Yp[i, d] += h
+        Ym[i, d] -= h
+        fd = (oracle.loss_grad(g, Yp, a, b)[0] - oracle.loss_grad(g, Ym, a, b)[0]) / (2 * h)
+        assert abs(fd - gY[i, d]) <= 1e-3, (i, d, fd, gY[i, d])
+    for k, (lo, hi) in enumerate([((a - h, b), (a + h, b)), ((a, b - h), (a, b + h))]):
+        fd = (oracle.loss_grad(g, Y, *hi)[0] - oracle.loss_grad(g, Y, *lo)[0]) / (2 * h)
+        assert abs(fd - gab[k]) <= 1e-6 * abs(gab[k]), (k, fd, gab[k])
+
+
+def test_adjoint_matches_reference_step_formulas(oracle_mod):
+    # One edge: the gradient of w (-log q) is minus the reference's attractive
+    # step coefficient times (y_i - y_j) (optimize_layout.hpp:147-149), and the
+    # gradient of (1 - w)(-log(1 - q)) with 1/d2 softened to 1/(d2 + 0.001) is
+    # minus its repulsive one with gamma = 1 (optimize_layout.hpp:170-171).
+    a, b = oracle.find_ab(1.0, 0.1)
+    rng = np.random.default_rng(12)
+    for _ in range(20):
+        Y = rng.normal(size=(2, 2)) * rng.uniform(0.05, 5.0)
+        diff = Y[0] - Y[1]
+        d2 = float(diff @ diff)
+        pd2b = d2 ** b
+        attract = (-2 * a * b * pd2b) / (d2 * (a * pd2b + 1.0))
+        repulse = 2 * 1.0 * b / ((0.001 + d2) * (a * pd2b + 1.0))
+        one = oracle.CSR(np.array([0, 1, 1], np.int64), np.array([1], np.int32), np.array([1.0]))
+        _, gY, _ = oracle.loss_grad(one, Y, a, b)
+        assert np.allclose(gY[0], -attract * diff, rtol=1e-12, atol=0)
+        assert np.allclose(gY[1], attract * diff, rtol=1e-12, atol=0)
+        zero = oracle.CSR(np.array([0, 1, 1], np.int64), np.array([1], np.int32), np.array([0.0]))
+        _, gY, _ = oracle.loss_grad(zero, Y, a, b, eps_rep=0.001)
+        assert np.allclose(gY[0], -repulse * diff, rtol=1e-12, atol=0)
