@@ -184,6 +184,30 @@ def test_event_windows_self_check(umap, monkeypatch, n, epochs):
     assert st.epoch() == epochs and np.all(np.isfinite(Y))
 
 
+def test_many_small_windows(umap, monkeypatch):
+    # window buffers capped at 2 MiB: about four epochs per window at 3000
+    # points, so the two buffers alternate dozens of times (each window built
+    # while the previous one's epochs run) and partial runs pick up a window
+    # left by the last call; every window is checked on the device against the
+    # recomputed schedule
+    monkeypatch.setenv("UMAPB_SGD_WINDOW_BYTES", str(2 << 20))
+    monkeypatch.setenv("UMAPB_CHECK_SCHEDULE", "1")
+    n, epochs = 3000, 300
+    X = oracle.gaussian_mixture(n, 12, 5, 4.0, seed=77, dtype=np.float32)
+    Y = np.zeros((n, 2), np.float32)
+    st = umap.initialize_from_data(X, 2, Y, umap.Options(num_epochs=epochs))
+    for limit in (1, 37, 150, epochs):
+        st.run(Y, limit)
+        assert st.epoch() == limit
+    assert np.all(np.isfinite(Y))
+    monkeypatch.delenv("UMAPB_SGD_WINDOW_BYTES")
+    Z = np.zeros((n, 2), np.float32)
+    one = umap.initialize_from_data(X, 2, Z, umap.Options(num_epochs=epochs))
+    one.run(Z)
+    t_many, t_one = oracle.trustworthiness(X, Y, 15), oracle.trustworthiness(X, Z, 15)
+    assert abs(t_many - t_one) < 0.02, (t_many, t_one)
+
+
 def test_initialize_method_semantics(umap):
     # tests/src/umappp.cpp:209-313
     nn = mock_neighbors(87, 5, seed=87)

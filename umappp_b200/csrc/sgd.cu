@@ -56,6 +56,12 @@ size_t window_bytes() {
     }();
     return v;
 }
+// UMAPB_SGD_WINDOW_BYTES caps the window buffers (read at every build; 0 or
+// unset: window_bytes()).
+size_t window_bytes_override() {
+    const char* e = std::getenv("UMAPB_SGD_WINDOW_BYTES");
+    return e ? static_cast<size_t>(std::strtoull(e, nullptr, 10)) : 0;
+}
 constexpr int MAX_GENERIC_DIM = 64;
 
 template <typename T>
@@ -779,7 +785,8 @@ void SgdEngine<T>::build_window(Window& win, int first, int last_wanted, cudaStr
     UMAPB_SYNC(s);
 
     // fit the window to the memory budget
-    const size_t budget = event_budget_bytes ? event_budget_bytes : window_bytes();
+    const size_t env_budget = window_bytes_override();
+    const size_t budget = event_budget_bytes ? event_budget_bytes : env_budget ? env_budget : window_bytes();
     // event record + (at most) one segment start per event
     const size_t per_event = sizeof(int2) + sizeof(uint16_t) + sizeof(int64_t) + sizeof(int32_t);
     int Wk = W;
