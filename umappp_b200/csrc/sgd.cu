@@ -1065,6 +1065,14 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
         if (ms_schedule) *ms_schedule = std::max(0.0f, all_ms - sgd_ms);
         if (ms_sgd) *ms_sgd = sgd_ms;
     } catch (...) {
+        // an error inside a graph capture leaves s capturing: end and drop it
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(s, &g);
+            if (g) cudaGraphDestroy(g);
+        }
+        cudaGetLastError();
         cudaStreamSynchronize(s);
         cudaStreamSynchronize(s2);
         cleanup();
