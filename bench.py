@@ -74,12 +74,14 @@ def load_peaks() -> dict:
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled during the timed region
+    (raw samples kept in $UMAPB_CLOCKS_DIR/clocks_rank<i>.csv when that is set)."""
 
     def __init__(self, index: int):
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv") if os.path.isdir(
-            os.path.join(ROOT, "gpurun_out")) else f"/tmp/umapb_clocks_{os.getpid()}.csv"
+        out_dir = os.environ.get("UMAPB_CLOCKS_DIR")
+        self.path = (os.path.join(out_dir, f"clocks_rank{index}.csv") if out_dir and os.path.isdir(out_dir)
+                     else f"/tmp/umapb_clocks_{os.getpid()}.csv")
         self.index = index
 
     def __enter__(self):

@@ -1,8 +1,9 @@
 // C entry points over the reference's own headers (include/umappp/*.hpp),
 // compiled unmodified against the project-written stand-ins in ref_shim/ for
 // its absent dependencies.  Built by oracle/Makefile into
-// oracle/_ref/libumappp_ref.so.  Used only as a checker (parity pinning of the
-// C restatement and of the CUDA path) and as the timed CPU baseline.
+// oracle/_ref/libumappp_ref.so.  Test infrastructure: used only to pin the C
+// restatement and the CUDA path to the reference, and as the timed CPU
+// baseline.
 //
 // Layout conventions of every entry point: neighbour lists are CSR
 // (row_ptr[n + 1] as int64, indices as int32, values as the float type);

@@ -3,7 +3,8 @@
 // their textbook definitions; the streams therefore differ from upstream
 // aarand, which is why layouts are compared by quality metrics rather than
 // bit-for-bit against upstream umappp.  oracle/oracle.c draws from the same
-// definitions so that the C restatement and this build agree exactly.
+// definitions so that the C restatement and the compiled reference agree
+// exactly.
 //
 // Test infrastructure only.
 #ifndef ORACLE_SHIM_AARAND_HPP
