@@ -94,32 +94,40 @@ __global__ void prepare16_kernel(const float* __restrict__ data, int32_t n, int3
                                  float s, __half* __restrict__ a_hi, __half* __restrict__ a_lo,
                                  __half* __restrict__ b_hi, __half* __restrict__ b_lo, float* __restrict__ norms,
                                  const int32_t* __restrict__ pad_src) {
+    // one warp per operand row: the data row is read and the four operand rows
+    // written by consecutive lanes; the FP64 norm is a warp reduction
     const double s2 = static_cast<double>(s) * s;
-    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n_pad; i += int64_t(gridDim.x) * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n_pad;
+         i += warps) {
         const int64_t src = pad_src ? pad_src[i] : (i < n ? i : -1);
-        const bool real = src >= 0;
+        const bool real = src >= 0;   // the same for the whole warp
         double nrm = 0;
         if (real) {
-            for (int d = 0; d < dim; ++d) {
+            for (int d = lane; d < dim; d += 32) {
                 const double v = data[src * dim + d];
                 nrm += v * v;
             }
         }
-        norms[i] = real ? static_cast<float>(nrm) : CUDART_INF_F;
+        for (int o = 16; o > 0; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
+        if (lane == 0) norms[i] = real ? static_cast<float>(nrm) : CUDART_INF_F;
         const int64_t row = i * k_pad;
-        for (int d = 0; d < k_pad; ++d) {
+        for (int d = lane; d < k_pad; d += 32) {
             __half h = __float2half_rn(0.0f), l = h;
             if (real && d < dim) split_f16(data[src * dim + d] * s, h, l);
-            a_hi[row + d] = h;
-            a_lo[row + d] = l;
+            __half ah = h;
+            const __half al = l;
             if (d == dim) {
                 if (real) {
-                    a_hi[row + d] = __float2half_rn(1.0f);
+                    ah = __float2half_rn(1.0f);
                     split_f16(static_cast<float>(-0.5 * nrm * s2), h, l);
                 } else {
                     h = __float2half_rn(-60000.0f);   // padding reference: d2 beyond any candidate
                 }
             }
+            a_hi[row + d] = ah;
+            a_lo[row + d] = al;
             b_hi[row + d] = h;
             b_lo[row + d] = l;
         }
@@ -502,7 +510,7 @@ void knn_tc16_run_tasks(const float* data, int32_t dim, int kcap, float scale, c
     const size_t elems = static_cast<size_t>(n_pad) * k_pad;
     DevArray<__half> ahi(elems, s), alo(elems, s), bhi(elems, s), blo(elems, s);
     DevArray<float> onorm(n_pad, s);
-    prepare16_kernel<<<grid_for(n_pad, 256), 256, 0, s>>>(data, 0, dim, n_pad, k_pad, scale, ahi.get(), alo.get(),
+    prepare16_kernel<<<grid_for(n_pad, 256 / 32), 256, 0, s>>>(data, 0, dim, n_pad, k_pad, scale, ahi.get(), alo.get(),
                                                            bhi.get(), blo.get(), onorm.get(), tiles.row_map.get());
     UMAPB_LAUNCH_CHECK();
     Maps16 m;
