@@ -129,6 +129,16 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def max_over_ranks(value: float, world: int, device=None) -> float:
+    """The largest of the ranks' values; every rank calls it (one rank: the value)."""
+    if world <= 1:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 # ------------------------------------------------------------ our arm ---
 
 def run_ours(args, rank: int, world: int) -> dict | None:
@@ -172,11 +182,7 @@ def run_ours(args, rank: int, world: int) -> dict | None:
             last = fn()
         e1.record()
         barrier()
-        ms = e0.elapsed_time(e1) / steps
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(e0.elapsed_time(e1) / steps, world, dev)
         return ms, last, U.lib().umapb_launch_count() - l0
 
     for _ in range(args.warmup):
@@ -287,11 +293,7 @@ def run_batch(args, rank: int, world: int) -> dict | None:
             last = fn()
         e1.record()
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / steps
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(e0.elapsed_time(e1) / steps, world, dev)
         return ms, last, (U.lib().umapb_launch_count() - l0) // max(steps, 1)
 
     for _ in range(args.warmup):
@@ -359,8 +361,7 @@ def run_reference(args, rank: int) -> dict | None:
     n, dim, _, _, _, k, epochs = CONFIGS[args.config]
     vals = []
     cb = None
-    for _ in range(args.warmup and 1 or 0):
-        pass
+    # the host-core reference needs no warm-up: every step is a fresh bounded sample
     for _ in range(max(args.steps, 1)):
         cb = cpu_sample(args.config)
         vals.append(cb["value"])
