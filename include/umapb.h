@@ -3,7 +3,8 @@
  *
  * Every entry point is plain C: pointers, sizes and an int status.  Pointer
  * arguments may be host memory (pageable or pinned) or device memory on the
- * current CUDA device; the library detects which and copies as needed.
+ * current CUDA device; the library detects which and copies as needed.  Device
+ * memory of another GPU is rejected with UMAPB_ERR_INVALID.
  * Layouts follow the reference (libscran/umappp v3.3.2):
  *   - data and embeddings are column-major with observations as columns,
  *     i.e. observation i occupies [i * dim, (i + 1) * dim)
@@ -301,7 +302,10 @@ int umapb_batch_run(int dtype, int32_t num_instances, const int32_t* sizes, size
  * With eps_rep > 0 the repulsive derivative uses 1 / (d^2 + eps_rep) in place
  * of 1 / d^2, as the reference's step does (eps 0.001).  Outputs: *loss,
  * grad_embedding (num_obs x num_dim, may be NULL), grad_ab[2] = dL/da, dL/db
- * (may be NULL).  Accumulation is FP64 for both dtypes.
+ * (may be NULL).  Accumulation is FP64 for both dtypes.  A row_ptr that does
+ * not run upwards within [0, row_ptr[num_obs]], or an index outside
+ * [0, num_obs), is reported as UMAPB_ERR_INVALID (detected on the device; the
+ * bad edges are not read).
  */
 int umapb_loss_grad(int dtype, size_t num_dim, const void* embedding, int32_t num_obs, const int64_t* row_ptr,
                     const int32_t* indices, const void* weights, double a, double b, double eps_rep,
@@ -317,15 +321,19 @@ int umapb_loss_grad(int dtype, size_t num_dim, const void* embedding, int32_t nu
  * allocator, which also synchronises the device.  Same arguments and results as
  * umapb_loss_grad, with these differences:
  *   - embedding, row_ptr, indices, weights and grad_embedding must be device
- *     memory (host pointers are rejected with UMAPB_ERR_INVALID); loss and
- *     grad_ab are host memory;
+ *     memory of the current device (host pointers and other devices' memory
+ *     are rejected with UMAPB_ERR_INVALID); loss and grad_ab are host memory;
+ *     with num_obs == 0 no pointer is read (NULL is accepted) and the results
+ *     are zero;
  *   - the work runs on the calling thread's per-thread default stream;
  *   - its scratch is a fixed array in the library's device memory (32 MB on
  *     every device that loads the library, held until exit); for UMAPB_F32 a
  *     gradient of more than 4,194,304 elements (num_obs * num_dim) is rejected
  *     with UMAPB_ERR_INVALID;
  *   - the first call on a device looks up the scratch's device address
- *     (cudaGetSymbolAddress); make that first call before any stream capture;
+ *     (cudaGetSymbolAddress) and keeps it for the life of the process; make
+ *     that first call before any stream capture, and make no call after a
+ *     cudaDeviceReset of that device;
  *   - every call shares the one scratch array, so calls that overlap on the
  *     GPU (other threads, other streams) race; serialise them.
  */

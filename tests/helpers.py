@@ -87,3 +87,42 @@ def eigen_check(g: oracle.CSR, Y: np.ndarray, tol: float = 1e-4) -> bool:
     ref = Y.astype(np.float64)
     cmp = out * res_scale / copy_scale
     return bool(np.all(np.abs(ref - cmp) < tol * (np.abs(ref) + np.abs(cmp)) / 2 + 1e-12))
+
+
+def trustworthiness_torch(X: np.ndarray, Y: np.ndarray, k: int = 15, queries: np.ndarray | None = None,
+                          device: str = "cuda", batch: int = 8) -> float:
+    """Trustworthiness(k) of embedding Y for data X, as oracle.trustworthiness
+    computes it (FP64 squared distances, ranks with ties broken by index,
+    queries optionally a sample of rows; sklearn.manifold.trustworthiness's
+    formula), evaluated with torch on 'device' so that 10^4 queries against
+    10^6 points take seconds.  Test infrastructure: a quality measure of
+    layouts, not a stage of the product."""
+    import torch
+
+    n = X.shape[0]
+    q = np.arange(n) if queries is None else np.asarray(queries)
+    Xd = torch.as_tensor(np.ascontiguousarray(X), device=device).to(torch.float64)
+    Yd = torch.as_tensor(np.ascontiguousarray(Y), device=device).to(torch.float64)
+    ar = torch.arange(n, device=device)
+    total = 0.0
+    for s in range(0, len(q), batch):
+        qi = torch.as_tensor(q[s:s + batch], device=device, dtype=torch.long)
+        rows = torch.arange(len(qi), device=device)
+        dX = ((Xd[None, :, :] - Xd[qi][:, None, :]) ** 2).sum(-1)          # (b, n)
+        dY = ((Yd[None, :, :] - Yd[qi][:, None, :]) ** 2).sum(-1)
+        dY[rows, qi] = float("inf")
+        # k nearest in Y, ties by index: among the k + 8 smallest, sort by (distance, index)
+        cand = torch.topk(dY, min(k + 8, n - 1), dim=1, largest=False).indices
+        cand = torch.sort(cand, dim=1).values
+        cd = torch.gather(dY, 1, cand)
+        order = torch.argsort(cd, dim=1, stable=True)
+        nb = torch.gather(cand, 1, order)[:, :k]                            # (b, k)
+        dj = torch.gather(dX, 1, nb)                                        # (b, k)
+        for t in range(k):
+            d = dj[:, t:t + 1]
+            j = nb[:, t:t + 1]
+            closer = (dX < d) | ((dX == d) & (ar[None, :] < j))
+            closer[rows, qi] = False
+            rank = closer.sum(1) + 1                                        # j itself is never 'closer'
+            total += float(torch.clamp(rank - k, min=0).sum())
+    return 1.0 - 2.0 / (len(q) * k * (2.0 * n - 3.0 * k - 1.0)) * total

@@ -330,3 +330,19 @@ def test_loss_grad_matches_oracle(umap, dtype):
     assert abs(loss - rl) <= tol * abs(rl)
     assert np.max(np.abs(gY - rgY)) <= tol * np.max(np.abs(rgY))
     assert np.max(np.abs(np.array(gab) - rgab)) <= 1e-9 * np.max(np.abs(rgab))
+
+
+def test_loss_grad_rejects_out_of_range_indices(umap):
+    """A neighbour index outside [0, num_obs) is skipped on the device and
+    reported as an invalid argument instead of being read."""
+    nl = neighbors_of(normal_data(200, 6, seed=6), 10)
+    w, _, _ = oracle.neighbor_similarities(nl)
+    g = oracle.combine_neighbor_sets(w, 1.0)
+    Y = np.random.default_rng(2).normal(size=(200, 2))
+    a, b = oracle.find_ab(1.0, 0.1)
+    idx = g.idx.copy()
+    idx[3] = 200
+    with pytest.raises(umap.UmapbError, match="out of range"):
+        umap.loss_grad((g.ptr, idx, g.val), Y, a, b)
+    loss, _, _ = umap.loss_grad(csr_tuple(g), Y, a, b)   # the next call is unaffected
+    assert np.isfinite(loss)

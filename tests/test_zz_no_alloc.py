@@ -88,3 +88,38 @@ def test_noalloc_rejects_host_pointers_and_oversize(umap):
     rc = fn(0, 2, d_Y.data_ptr(), 3_000_000, d_ptr.data_ptr(), d_idx.data_ptr(), d_w.data_ptr(), 1.5, 0.9, 0.0, 0,
             ctypes.byref(loss), d_g.data_ptr(), None)
     assert rc == 1 and "scratch" in umap._lib.lib().umapb_last_error().decode()
+
+
+def test_noalloc_rejects_bad_indices_and_accepts_empty(umap):
+    """An index outside [0, num_obs) or a row_ptr running backwards is found on
+    the device (the bad edges are skipped, never read) and reported as
+    UMAPB_ERR_INVALID; a following valid call succeeds.  num_obs == 0 reads
+    no pointer at all."""
+    torch = pytest.importorskip("torch")
+    fn = _noalloc_fn(umap)
+    g, Y = _problem(np.float64)
+    a, b = oracle.find_ab(1.0, 0.1)
+    dev = torch.device("cuda", 0)
+    d_Y = torch.from_numpy(Y).to(dev)
+    d_w = torch.from_numpy(g.val).to(dev)
+    loss = ctypes.c_double()
+    bad_idx = g.idx.copy()
+    bad_idx[len(bad_idx) // 2] = g.n          # one neighbour out of range
+    bad_ptr = g.ptr.copy()
+    bad_ptr[5] = bad_ptr[7]                   # row 5 runs backwards
+    for ptr, idx in ((g.ptr, bad_idx), (bad_ptr, g.idx)):
+        d_ptr = torch.from_numpy(ptr).to(dev)
+        d_idx = torch.from_numpy(idx).to(dev)
+        rc = fn(1, 2, d_Y.data_ptr(), g.n, d_ptr.data_ptr(), d_idx.data_ptr(), d_w.data_ptr(), a, b, 0.001, 0,
+                ctypes.byref(loss), None, None)
+        assert rc == 1 and "out of range" in umap._lib.lib().umapb_last_error().decode()
+    d_ptr = torch.from_numpy(g.ptr).to(dev)
+    d_idx = torch.from_numpy(g.idx).to(dev)
+    rc = fn(1, 2, d_Y.data_ptr(), g.n, d_ptr.data_ptr(), d_idx.data_ptr(), d_w.data_ptr(), a, b, 0.001, 0,
+            ctypes.byref(loss), None, None)
+    assert rc == 0
+    ref_loss, _, _ = umap.loss_grad(csr_tuple(g), Y, a, b, eps_rep=0.001)
+    assert abs(loss.value - ref_loss) <= 1e-10 * abs(ref_loss)
+    gab = np.full(2, np.nan)
+    rc = fn(1, 2, None, 0, None, None, None, a, b, 0.001, 0, ctypes.byref(loss), None, gab.ctypes.data)
+    assert rc == 0 and loss.value == 0 and np.all(gab == 0)

@@ -40,10 +40,18 @@ __global__ void __launch_bounds__(ADJ_BLOCK) loss_grad_kernel(int32_t n, int dim
     double loss = 0, ga = 0, gb = 0;
     const double log_a = log(a);
     const int32_t i = blockIdx.x * ADJ_BLOCK + threadIdx.x;
+    bool bad = false;
     if (i < n) {
         const T* yi = Y + static_cast<size_t>(i) * dim;
-        for (int64_t p = ptr[i]; p < ptr[i + 1]; ++p) {
+        // a row outside [0, ptr[n]] or running backwards is skipped and flagged
+        const int64_t p0 = ptr[i], p1 = ptr[i + 1], nnz = ptr[n];
+        if (p0 < 0 || p1 < p0 || p1 > nnz) bad = true;
+        for (int64_t p = p0; !bad && p < p1; ++p) {
             const int32_t j = idx[p];
+            if (j < 0 || j >= n) {   // out-of-range neighbour: skipped and flagged
+                bad = true;
+                continue;
+            }
             const T* yj = Y + static_cast<size_t>(j) * dim;
             double d2 = 0;
             for (int d = 0; d < dim; ++d) {
@@ -84,6 +92,7 @@ __global__ void __launch_bounds__(ADJ_BLOCK) loss_grad_kernel(int32_t n, int dim
         atomicAdd(acc + 1, ga);
         atomicAdd(acc + 2, gb);
     }
+    if (bad) acc[3] = 1.0;   // invalid row_ptr or indices
 }
 
 template <typename T>
@@ -99,7 +108,7 @@ void loss_grad(int32_t n, int num_dim, const T* Y, const int64_t* ptr, const int
                double b, double eps_rep, bool with_constant, double* loss_out, T* grad_Y, double* grad_ab,
                cudaStream_t s) {
     require(a > 0 && b > 0, "a and b must be positive");
-    DevArray<double> acc(3, s);
+    DevArray<double> acc(4, s);
     acc.zero(s);
     const size_t total = static_cast<size_t>(n) * num_dim;
     DevArray<double> g64;
@@ -122,9 +131,10 @@ void loss_grad(int32_t n, int num_dim, const T* Y, const int64_t* ptr, const int
         cast_grad_kernel<T><<<grid_for(total, 256), 256, 0, s>>>(total, gptr, grad_Y);
         UMAPB_LAUNCH_CHECK();
     }
-    double h[3];
+    double h[4];
     UMAPB_CUDA(cudaMemcpyAsync(h, acc.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
     UMAPB_SYNC(s);
+    require(h[3] == 0, "row_ptr or indices out of range (row_ptr must run from 0 upwards, indices in [0, num_obs))");
     if (loss_out) *loss_out = h[0];
     if (grad_ab) {
         grad_ab[0] = h[1];
@@ -140,9 +150,10 @@ template void loss_grad<double>(int32_t, int, const double*, const int64_t*, con
 // ------------------------------------------------- allocation-free variant --
 //
 // Scratch for umapb_loss_grad_noalloc, resident on every device that loads the
-// library: [0, 3) the loss and dL/da, dL/db accumulators, [4, 4 + max) the FP64
-// accumulation of a float gradient.  Its host-side name is only a stand-in;
-// kernels get the device address from cudaGetSymbolAddress.
+// library: [0, 3) the loss and dL/da, dL/db accumulators, [3] the invalid-input
+// flag, [4, 4 + max) the FP64 accumulation of a float gradient.  Its host-side
+// name is only a stand-in; kernels get the device address from
+// cudaGetSymbolAddress.
 constexpr size_t NOALLOC_GRAD_MAX = size_t(1) << 22;   // gradient elements (n * num_dim) for float data
 constexpr size_t NOALLOC_ACC_OFFSET = 0;
 constexpr size_t NOALLOC_GRAD_OFFSET = 4;
@@ -154,7 +165,10 @@ constexpr int MAX_DEVICES = 64;
 std::mutex g_noalloc_mutex;
 double* g_noalloc_ptr[MAX_DEVICES] = {nullptr};
 
-// Device address of the scratch on the current device, looked up once per device.
+// Device address of the scratch on the current device, looked up on the first
+// call on that device and cached for the life of the process (a
+// cudaDeviceReset of that device invalidates it; the library does not support
+// calls after a reset).
 double* noalloc_scratch(int dev) {
     require(dev >= 0 && dev < MAX_DEVICES, "device ordinal out of range");
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
@@ -164,16 +178,6 @@ double* noalloc_scratch(int dev) {
         g_noalloc_ptr[dev] = static_cast<double*>(p);
     }
     return g_noalloc_ptr[dev];
-}
-
-bool device_pointer(const void* p) {
-    if (!p) return false;
-    cudaPointerAttributes attr;
-    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
 }
 
 template <typename T>
@@ -186,15 +190,21 @@ void loss_grad_noalloc(int32_t n, int num_dim, const T* Y, const int64_t* ptr, c
         require(total <= NOALLOC_GRAD_MAX,
                 "num_obs * num_dim exceeds the allocation-free scratch (4194304 gradient elements for float data)");
     }
-    require(device_pointer(Y) && device_pointer(ptr) && device_pointer(idx) && device_pointer(w),
+    if (n == 0) {   // nothing to read: no pointer is looked at, the results are zero
+        if (loss_out) *loss_out = 0;
+        if (grad_ab) grad_ab[0] = grad_ab[1] = 0;
+        return;
+    }
+    // pointers of another device are rejected inside is_device_pointer
+    require(is_device_pointer(Y) && is_device_pointer(ptr) && is_device_pointer(idx) && is_device_pointer(w),
             "the allocation-free entry point takes device pointers for embedding, row_ptr, indices and weights");
-    require(!grad_Y || device_pointer(grad_Y), "grad_embedding must be a device pointer (or NULL)");
+    require(!grad_Y || is_device_pointer(grad_Y), "grad_embedding must be a device pointer (or NULL)");
     int dev = 0;
     UMAPB_CUDA(cudaGetDevice(&dev));
     double* scratch = noalloc_scratch(dev);
     double* acc = scratch + NOALLOC_ACC_OFFSET;
     const cudaStream_t s = cudaStreamPerThread;
-    UMAPB_CUDA(cudaMemsetAsync(acc, 0, 3 * sizeof(double), s));
+    UMAPB_CUDA(cudaMemsetAsync(acc, 0, 4 * sizeof(double), s));
     double* gptr = nullptr;
     if (grad_Y) {
         if constexpr (std::is_same<T, double>::value) {
@@ -204,18 +214,17 @@ void loss_grad_noalloc(int32_t n, int num_dim, const T* Y, const int64_t* ptr, c
         }
         UMAPB_CUDA(cudaMemsetAsync(gptr, 0, total * sizeof(double), s));
     }
-    if (n > 0) {
-        loss_grad_kernel<T><<<(n + ADJ_BLOCK - 1) / ADJ_BLOCK, ADJ_BLOCK, 0, s>>>(
-            n, num_dim, Y, ptr, idx, w, a, b, eps_rep, with_constant ? 1 : 0, gptr, acc);
-        UMAPB_LAUNCH_CHECK();
-    }
+    loss_grad_kernel<T><<<(n + ADJ_BLOCK - 1) / ADJ_BLOCK, ADJ_BLOCK, 0, s>>>(
+        n, num_dim, Y, ptr, idx, w, a, b, eps_rep, with_constant ? 1 : 0, gptr, acc);
+    UMAPB_LAUNCH_CHECK();
     if (grad_Y && !std::is_same<T, double>::value) {
         cast_grad_kernel<T><<<grid_for(total, 256), 256, 0, s>>>(total, gptr, grad_Y);
         UMAPB_LAUNCH_CHECK();
     }
-    double h[3];
+    double h[4];
     UMAPB_CUDA(cudaMemcpyAsync(h, acc, sizeof(h), cudaMemcpyDeviceToHost, s));
     UMAPB_SYNC(s);
+    require(h[3] == 0, "row_ptr or indices out of range (row_ptr must run from 0 upwards, indices in [0, num_obs))");
     if (loss_out) *loss_out = h[0];
     if (grad_ab) {
         grad_ab[0] = h[1];

@@ -158,6 +158,9 @@ private:
 };
 
 // True when p is device (or managed) memory usable by kernels on this device.
+// Device memory of another GPU is rejected (UMAPB_ERR_INVALID): without peer
+// access a kernel reading it would fault, and every buffer of a call must
+// belong to the current device.
 inline bool is_device_pointer(const void* p) {
     if (!p) return false;
     cudaPointerAttributes attr;
@@ -166,7 +169,18 @@ inline bool is_device_pointer(const void* p) {
         cudaGetLastError();
         return false;
     }
-    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+    if (attr.type == cudaMemoryTypeDevice) {
+        int dev = -1;
+        if (cudaGetDevice(&dev) != cudaSuccess) {
+            cudaGetLastError();
+            dev = -1;
+        }
+        if (attr.device != dev)
+            fail(UMAPB_ERR_INVALID, "a device pointer belongs to device " + std::to_string(attr.device) +
+                                        ", not to the current device " + std::to_string(dev));
+        return true;
+    }
+    return attr.type == cudaMemoryTypeManaged;
 }
 
 // Read-only view of a caller array on the device: the caller's pointer when it

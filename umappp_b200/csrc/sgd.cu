@@ -306,6 +306,16 @@ __device__ __forceinline__ float repulse_coef_fast(float d2, const SgdParams<flo
     return __fdividef(p.gamma2b, (0.001f + d2) * __fmaf_rn(p.a, pow_b(d2, p.b), 1.0f));
 }
 
+// The same coefficients with libm's powf and IEEE division (a kernel variant
+// that measures what the approximations above cost in layout quality).
+__device__ __forceinline__ float attract_coef_precise(float d2, const SgdParams<float>& p) {
+    const float pd2b = powf(d2, p.b);
+    return (p.neg2ab * pd2b) / (d2 * (p.a * pd2b + 1.0f));
+}
+__device__ __forceinline__ float repulse_coef_precise(float d2, const SgdParams<float>& p) {
+    return p.gamma2b / ((0.001f + d2) * (p.a * powf(d2, p.b) + 1.0f));
+}
+
 template <typename T>
 __device__ __forceinline__ T floor_eps(T d2) {
     const T e = FloatLimits<T>::epsilon();
@@ -527,7 +537,7 @@ __global__ void seg_first_kernel(const int64_t* __restrict__ seg_pos, int64_t ns
 // followed by its negative samples -- the per-row sequence of
 // optimize_layout.hpp:136-180.  The tail moves by a vector atomic; the head's
 // total displacement is added once at the end.
-template <int NB, int MINB>
+template <int NB, int MINB, bool PRECISE = false>
 __global__ void __launch_bounds__(256, MINB) sgd_epoch_2d_f32(const int32_t* __restrict__ order, int64_t base,
                                                         int64_t slot0, int64_t slot1,
                                                         const int64_t* __restrict__ seg_pos,
@@ -564,7 +574,7 @@ __global__ void __launch_bounds__(256, MINB) sgd_epoch_2d_f32(const int32_t* __r
                 if (attract) {
                     const float dx = hx - yt.x, dy = hy - yt.y;
                     const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
-                    const float cf = attract_coef_fast(d2, p);
+                    const float cf = PRECISE ? attract_coef_precise(d2, p) : attract_coef_fast(d2, p);
                     const float gx = p.alpha * clamp4(cf * dx);
                     const float gy = p.alpha * clamp4(cf * dy);
                     hx += gx;
@@ -577,7 +587,7 @@ __global__ void __launch_bounds__(256, MINB) sgd_epoch_2d_f32(const int32_t* __r
                     if (i < m && ks[i] != h) {
                         const float dx = hx - yk[i].x, dy = hy - yk[i].y;
                         const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
-                        const float cf = repulse_coef_fast(d2, p);
+                        const float cf = PRECISE ? repulse_coef_precise(d2, p) : repulse_coef_fast(d2, p);
                         hx = __fmaf_rn(p.alpha, clamp4(cf * dx), hx);
                         hy = __fmaf_rn(p.alpha, clamp4(cf * dy), hy);
                     }
@@ -599,6 +609,7 @@ const Sgd2dVariant SGD_2D_VARIANTS[] = {
     {sgd_epoch_2d_f32<12, 4>, 12, 4},   // 64 registers
     {sgd_epoch_2d_f32<8, 4>, 8, 4},     // default
     {sgd_epoch_2d_f32<6, 6>, 6, 6},     // 40 registers
+    {sgd_epoch_2d_f32<8, 4, true>, 8, 4},   // libm powf and IEEE division (precision check)
 };
 constexpr int NUM_SGD_2D_VARIANTS = sizeof(SGD_2D_VARIANTS) / sizeof(SGD_2D_VARIANTS[0]);
 
@@ -810,7 +821,11 @@ void SgdEngine<T>::build_window(Window& win, int first, int last_wanted, cudaStr
     // head segments of every epoch in the window (count, scan, write, per-epoch first segment)
     const int64_t resident_threads =
         static_cast<int64_t>(sm_count()) * sgd_2d_resident(variant_, block_) * block_;
-    const int seg_max = events < resident_threads * Wk ? SEG_MAX_FEW : SEG_MAX;
+    int seg_max = events < resident_threads * Wk ? SEG_MAX_FEW : SEG_MAX;
+    if (const char* e = std::getenv("UMAPB_SGD_SEG_MAX")) {   // override of the segment cap
+        const int x = std::atoi(e);
+        if (x >= 1 && x <= 4096) seg_max = x;
+    }
     win.seg_max = seg_max;
     const int64_t seg_blocks = std::max<int64_t>((events + SEG_BLOCK * SEG_ITEMS - 1) / (SEG_BLOCK * SEG_ITEMS), 1);
     DevArray<int64_t> bcount(seg_blocks + 1, s), boff(seg_blocks + 1, s);
@@ -953,7 +968,10 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
         const int P = win.buckets;
         const int64_t threads = static_cast<int64_t>(std::min<int64_t>(g, resident)) * blk;
         const int64_t rounds = (nsegs + threads - 1) / threads;
-        const int L = static_cast<int>(std::min<int64_t>(P, std::max<int64_t>(1, (P + rounds - 1) / rounds)));
+        int L = static_cast<int>(std::min<int64_t>(P, std::max<int64_t>(1, (P + rounds - 1) / rounds)));
+        if (const char* he = std::getenv("UMAPB_SGD_HARD_SLICES")) {   // one launch per slice
+            if (*he && *he != '0') L = P;
+        }
         const int64_t* off = win.host_bucket_off.data() + static_cast<size_t>(w) * (P + 1);
         const int32_t* order = win.ordered ? win.seg_order.get() : nullptr;
         for (int l = 0; l < L; ++l) {
@@ -1232,12 +1250,9 @@ void SgdEngine<T>::counts(int first, int last, int64_t* out, cudaStream_t s) {
 // UMAPB_SGD_PHASES overrides it (1 = every event of an epoch in one launch).
 template <typename T>
 int SgdEngine<T>::default_min_phases() {
-    static const int v = [] {
-        const char* e = std::getenv("UMAPB_SGD_PHASES");
-        const int x = e ? std::atoi(e) : 0;
-        return (x >= 1 && x <= 64) ? x : 8;
-    }();
-    return v;
+    const char* e = std::getenv("UMAPB_SGD_PHASES");
+    const int x = e ? std::atoi(e) : 0;
+    return (x >= 1 && x <= 64) ? x : 8;
 }
 
 // UMAPB_SGD_VARIANT selects the 2-d kernel variant (index into
