@@ -537,7 +537,23 @@ __global__ void seg_first_kernel(const int64_t* __restrict__ seg_pos, int64_t ns
 // followed by its negative samples -- the per-row sequence of
 // optimize_layout.hpp:136-180.  The tail moves by a vector atomic; the head's
 // total displacement is added once at the end.
-template <int NB, int MINB, bool PRECISE = false>
+// Head publication modes of the 2-d kernel: HEAD_AT_END adds the head's total
+// displacement once at the segment's end; HEAD_PER_EVENT adds each event's
+// displacement as soon as it is computed; HEAD_FRESH also re-reads the head
+// at the start of every event (seeing the pulls of other threads' attractive
+// steps, which move it as a tail), so no event works from a copy of the head
+// older than one event.
+enum HeadMode { HEAD_AT_END = 0, HEAD_PER_EVENT = 1, HEAD_FRESH = 2 };
+
+// Coherent device-scope load: ordered after this thread's own earlier atomic
+// adds to the same address.
+__device__ __forceinline__ float2 ld_relaxed_f2(const float2* p) {
+    float2 v;
+    asm volatile("ld.relaxed.gpu.global.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p) : "memory");
+    return v;
+}
+
+template <int NB, int MINB, bool PRECISE = false, int MODE = HEAD_AT_END>
 __global__ void __launch_bounds__(256, MINB) sgd_epoch_2d_f32(const int32_t* __restrict__ order, int64_t base,
                                                         int64_t slot0, int64_t slot1,
                                                         const int64_t* __restrict__ seg_pos,
@@ -551,12 +567,18 @@ __global__ void __launch_bounds__(256, MINB) sgd_epoch_2d_f32(const int32_t* __r
         int32_t nbase;
         uint32_t nsize;
         instance_range(h, p, nbase, nsize);
-        const float2 y0 = __ldcg(&Y[h]);
+        const float2 y0 = MODE == HEAD_FRESH ? ld_relaxed_f2(&Y[h]) : __ldcg(&Y[h]);
         float hx = y0.x, hy = y0.y;
         for (int64_t e = e0; e < e1; ++e) {
             const int2 pr = ht[e];
             int remaining = nneg[e];
             const float2 yt = __ldcg(&Y[pr.y]);
+            if (MODE == HEAD_FRESH && e != e0) {
+                const float2 yh = ld_relaxed_f2(&Y[h]);
+                hx = yh.x;
+                hy = yh.y;
+            }
+            const float ex = hx, ey = hy;   // head at the event's start
             NegStream rng(static_cast<uint32_t>(h), static_cast<uint32_t>(pr.y), p.epoch, p.k0, p.k1);
             bool attract = true;
             do {
@@ -594,8 +616,9 @@ __global__ void __launch_bounds__(256, MINB) sgd_epoch_2d_f32(const int32_t* __r
                 }
                 remaining -= m;
             } while (remaining > 0);
+            if (MODE != HEAD_AT_END) atomicAdd(&Y[h], make_float2(hx - ex, hy - ey));
         }
-        atomicAdd(&Y[h], make_float2(hx - y0.x, hy - y0.y));
+        if (MODE == HEAD_AT_END) atomicAdd(&Y[h], make_float2(hx - y0.x, hy - y0.y));
     }
 }
 
@@ -610,8 +633,11 @@ const Sgd2dVariant SGD_2D_VARIANTS[] = {
     {sgd_epoch_2d_f32<8, 4>, 8, 4},     // default
     {sgd_epoch_2d_f32<6, 6>, 6, 6},     // 40 registers
     {sgd_epoch_2d_f32<8, 4, true>, 8, 4},   // libm powf and IEEE division (precision check)
+    {sgd_epoch_2d_f32<8, 4, false, HEAD_PER_EVENT>, 8, 4},
+    {sgd_epoch_2d_f32<8, 4, false, HEAD_FRESH>, 8, 4},
 };
 constexpr int NUM_SGD_2D_VARIANTS = sizeof(SGD_2D_VARIANTS) / sizeof(SGD_2D_VARIANTS[0]);
+constexpr int NUM_TUNED_VARIANTS = 4;   // the tuner picks among launch shapes of one arithmetic
 
 // Resident blocks per SM of variant v at 'block' threads (occupancy query, cached).
 int sgd_2d_resident(int v, int block) {
@@ -901,7 +927,7 @@ void SgdEngine<T>::tune(T* Y, int num_dim, int first, int stop, const Window& wi
     DevArray<T> scratch(total, s);
     cudaEvent_t a = event_get(), b = event_get();
     float best = 1e30f;
-    for (int v = 0; v < NUM_SGD_2D_VARIANTS; ++v) {
+    for (int v = 0; v < NUM_TUNED_VARIANTS; ++v) {
         for (int blk : {128, 256}) {
             UMAPB_CUDA(cudaMemcpyAsync(scratch.get(), Y, total * sizeof(T), cudaMemcpyDeviceToDevice, s));
             UMAPB_CUDA(cudaEventRecord(a, s));
