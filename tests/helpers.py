@@ -61,6 +61,47 @@ def mock_neighbors(n: int, k: int, seed: int) -> oracle.CSR:
     return oracle.CSR.from_lists(rows)
 
 
+def same_neighbors(idx_a, idx_b, dist_ref, rel_tie=1e-6) -> int:
+    """Number of neighbour positions where idx_a differs from idx_b other than
+    by an exchange of (near-)tied reference distances (within rel_tie)."""
+    bad = 0
+    for i in range(idx_a.shape[0]):
+        if np.array_equal(idx_a[i], idx_b[i]):
+            continue
+        d = dist_ref[i]
+        for c in np.nonzero(idx_a[i] != idx_b[i])[0]:
+            lo = max(c - 1, 0)
+            hi = min(c + 1, len(d) - 1)
+            near = np.abs(d[lo:hi + 1] - d[c]) <= rel_tie * max(d[c], 1e-300)
+            if near.sum() < 2:
+                bad += 1
+    return bad
+
+
+def sampled_rows(n: int, blocks: int, block_len: int, seed: int) -> np.ndarray:
+    """blocks non-overlapping runs of block_len consecutive rows at seeded
+    random offsets (sorted)."""
+    rng = np.random.default_rng(seed)
+    span = n // blocks
+    starts = [b * span + int(rng.integers(0, max(span - block_len, 1))) for b in range(blocks)]
+    return np.concatenate([np.arange(s, min(s + block_len, n)) for s in starts])
+
+
+def oracle_knn_rows(X: np.ndarray, k: int, rows: np.ndarray, block_len: int, threads: int = 0):
+    """The oracle's exact FP64 kNN (oracle.knn) of the given rows, which come
+    in runs of block_len consecutive rows (sampled_rows); the runs are searched
+    in parallel host threads (the C search releases the GIL)."""
+    import concurrent.futures
+    import os
+
+    X64 = np.ascontiguousarray(X, dtype=np.float64)   # what oracle_knn_f32 would convert to
+    starts = rows[::block_len]
+    threads = threads or min(len(starts), os.cpu_count() or 1)
+    with concurrent.futures.ThreadPoolExecutor(threads) as ex:
+        parts = list(ex.map(lambda s: oracle.knn(X64, k, int(s), int(min(block_len, X.shape[0] - s))), starts))
+    return np.concatenate([p[0] for p in parts]), np.concatenate([p[1] for p in parts])
+
+
 def csr_tuple(g: oracle.CSR):
     return g.ptr, g.idx, g.val
 

@@ -1,0 +1,37 @@
+"""Exactness of the device kNN at the benchmark's sizes.
+
+The tensor-core search prunes reference tiles with FP32 bounds carrying
+relative safety margins and recomputes in FP64 only the queries whose
+candidate list is not provably complete; a wrong bound would drop true
+neighbours silently, and most visibly on large, clustered inputs.  Here the
+device searches the benchmark data sets in full (100,000 x 50 and
+1,000,000 x 50 Gaussian mixtures, k = 15) and 1,000 sampled query rows are
+checked against the oracle's exact FP64 brute force over all points: the
+neighbour indices must be equal except where reference distances tie within
+1e-6 (relative), and the distances must be the FP64 values rounded to float
+(1e-6 relative).
+"""
+import numpy as np
+import pytest
+
+import bench
+from helpers import oracle_knn_rows, rel_err, same_neighbors, sampled_rows
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("workload", ["mixture_100k", "mixture_1m"])
+def test_knn_exact_on_benchmark_data(umap, workload):
+    X = bench.make_data(workload)
+    k = bench.CONFIGS[workload][5]
+    idx, dist = umap.knn(X, k)
+    L = umap.lib()
+    rows = sampled_rows(X.shape[0], 8, 125, seed=2024)
+    ridx, rdist = oracle_knn_rows(X, k, rows, 125)
+    bad = same_neighbors(idx[rows], ridx, rdist)
+    err = rel_err(dist[rows], rdist)
+    print(f"{workload}: {len(rows)} sampled queries, non-tie mismatches {bad}, max distance rel. error {err:.2e}, "
+          f"FP64-recomputed queries {L.umapb_knn_last_fp64_recomputed()}, tile pairs {L.umapb_knn_last_tile_pairs()}, "
+          f"largest tensor-core distance error {L.umapb_knn_last_tc_error():.2e}")
+    assert bad == 0
+    assert err <= 1e-6

@@ -9,28 +9,12 @@ import pytest
 
 import oracle
 from helpers import (csr_tuple, eigen_check, mock_probabilities, neighbors_of, normal_data, rel_err,
-                     two_populations)
+                     same_neighbors, two_populations)
 
 pytestmark = pytest.mark.gpu
 
 
 # ------------------------------------------------------------------ kNN ---
-
-def _same_neighbors(idx_a, idx_b, dist_ref, rel_tie=1e-6):
-    """Indices equal except where the reference distances tie within rel_tie."""
-    bad = 0
-    for i in range(idx_a.shape[0]):
-        if np.array_equal(idx_a[i], idx_b[i]):
-            continue
-        d = dist_ref[i]
-        for c in np.nonzero(idx_a[i] != idx_b[i])[0]:
-            lo = max(c - 1, 0)
-            hi = min(c + 1, len(d) - 1)
-            near = np.abs(d[lo:hi + 1] - d[c]) <= rel_tie * max(d[c], 1e-300)
-            if near.sum() < 2:
-                bad += 1
-    return bad
-
 
 # (12, 4, 5), (20, 3, 10): fewer other points than the candidate list holds, so
 # padding columns of the tensor-core tile must never become candidates
@@ -40,7 +24,7 @@ def test_knn_f32_matches_fp64_bruteforce(umap, n, dim, k):
     X = oracle.gaussian_mixture(n, dim, 6, 4.0, seed=n + dim, dtype=np.float32)
     idx, dist = umap.knn(X, k)
     ridx, rdist = oracle.knn(X, k)
-    assert _same_neighbors(idx, ridx, rdist) == 0
+    assert same_neighbors(idx, ridx, rdist) == 0
     # distances are FP64 results rounded to float
     assert rel_err(dist, rdist) <= 1e-6
 
@@ -64,7 +48,7 @@ def test_knn_tensor_core_operands(umap, monkeypatch, kind, n, dim, k):
     X *= np.float32(37.5)   # not a power of two: the FP16 scaling must stay exact
     idx, dist = umap.knn(X, k)
     ridx, rdist = oracle.knn(X, k)
-    assert _same_neighbors(idx, ridx, rdist) == 0
+    assert same_neighbors(idx, ridx, rdist) == 0
     assert rel_err(dist, rdist) <= 1e-6
     err = umap.lib().umapb_knn_last_tc_error()
     if kind == "tf32" and dim + 1 > 64:
@@ -82,7 +66,7 @@ def test_knn_tile_pruning_is_exact(umap, monkeypatch, prune):
     X = oracle.gaussian_mixture(n, 30, 8, 10.0, seed=11, dtype=np.float32)
     idx, dist = umap.knn(X, 15)
     ridx, rdist = oracle.knn(X, 15)
-    assert _same_neighbors(idx, ridx, rdist) == 0
+    assert same_neighbors(idx, ridx, rdist) == 0
     assert rel_err(dist, rdist) <= 1e-6
     pairs = umap.lib().umapb_knn_last_tile_pairs()
     tiles = (n + 127) // 128
@@ -99,7 +83,7 @@ def test_knn_duplicates_and_ties(umap):
     idx, dist = umap.knn(X, 6)
     ridx, rdist = oracle.knn(X, 6)
     assert np.array_equal(dist.astype(np.float64) == 0, rdist == 0)
-    assert _same_neighbors(idx, ridx, rdist) == 0
+    assert same_neighbors(idx, ridx, rdist) == 0
 
 
 def test_knn_rejects_bad_k(umap):

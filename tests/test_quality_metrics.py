@@ -25,3 +25,15 @@ def test_trustworthiness_torch_equals_oracle(n, dim, sample):
     a = oracle.trustworthiness(X, Y, 15, queries=q)
     b = trustworthiness_torch(X, Y, 15, queries=q, device="cpu", batch=64)
     assert a == b, (a, b)
+
+
+def test_oracle_knn_rows_equals_full_search():
+    """The threaded, row-sampled oracle search used at the benchmark sizes
+    returns exactly the full search's rows."""
+    from helpers import oracle_knn_rows, sampled_rows
+
+    X = oracle.gaussian_mixture(3000, 12, 5, 3.0, seed=4, dtype=np.float32)
+    rows = sampled_rows(3000, 4, 50, seed=1)
+    idx, dist = oracle_knn_rows(X, 10, rows, 50)
+    fidx, fdist = oracle.knn(X, 10)
+    assert np.array_equal(idx, fidx[rows]) and np.array_equal(dist, fdist[rows])
