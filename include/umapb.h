@@ -100,6 +100,27 @@ size_t umapb_options_size(void);
 /* Number of kernels this library has launched in this process (all threads). */
 int64_t umapb_launch_count(void);
 
+/*
+ * Poll limit of the bounded device-side waits of the tensor-core kNN kernels
+ * (an extension; the reference has no device code).  A role of the kernel
+ * that waits longer than this for another role gives up: the kernel stops
+ * all roles, waits for its copies and MMAs in flight, frees its tensor memory
+ * and the call returns UMAPB_ERR_DEVICE_TIMEOUT, leaving the device usable.
+ * polls <= 0 restores the default (2^26 polls, seconds).  Process-wide; read
+ * at each launch.  Returns the previous limit.  Meant for failure testing.
+ */
+int64_t umapb_set_device_wait_limit(int64_t polls);
+
+/*
+ * Caps the device memory the library holds at once (blocks in use plus its
+ * cache of freed blocks; process-wide, all devices): an allocation beyond the
+ * cap first returns the cache to the device and then fails with UMAPB_ERR_OOM,
+ * as a real out-of-memory does.  0 removes the cap (the default).  Returns the
+ * previous cap.  An extension (the reference allocates host memory only): for
+ * callers that share a GPU, and for testing the out-of-memory path.
+ */
+size_t umapb_set_workspace_limit(size_t bytes);
+
 /* ------------------------------------------------------------------ Status */
 
 typedef struct umapb_status umapb_status;

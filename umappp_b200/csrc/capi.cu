@@ -17,6 +17,7 @@
 namespace umapb {
 
 std::atomic<long long> g_launches{0};
+std::atomic<long long> g_wait_limit{1ll << 26};
 
 namespace {
 
@@ -507,6 +508,12 @@ int umapb_version(void) { return UMAPB_VERSION; }
 size_t umapb_options_size(void) { return sizeof(umapb_options); }
 
 int64_t umapb_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+size_t umapb_set_workspace_limit(size_t bytes) { return umapb::ws_set_limit(bytes); }
+
+int64_t umapb_set_device_wait_limit(int64_t polls) {
+    return g_wait_limit.exchange(polls > 0 ? polls : (1ll << 26), std::memory_order_relaxed);
+}
 
 int umapb_initialize_neighbors(int dtype, int32_t num_obs, const int64_t* row_ptr, const int32_t* indices,
                                const void* distances, size_t num_dim, void* embedding, const umapb_options* opt,

@@ -21,6 +21,10 @@
 namespace umapb {
 
 extern std::atomic<long long> g_launches;   // defined in capi.cu
+// Poll limit of the tensor-core kernels' bounded mbarrier waits
+// (umapb_set_device_wait_limit; defined in capi.cu).
+extern std::atomic<long long> g_wait_limit;
+inline long long device_wait_limit() { return g_wait_limit.load(std::memory_order_relaxed); }
 
 // ---------------------------------------------------------------- errors ---
 
@@ -102,6 +106,7 @@ void* ws_alloc(size_t bytes, cudaStream_t s);
 void ws_free(void* p, cudaStream_t s);
 size_t ws_cached_bytes();
 void ws_release_cached();
+size_t ws_set_limit(size_t bytes);   // cap on bytes held (in use + cached), 0: none; returns the previous cap
 cudaEvent_t event_get();          // timing event from the pool
 void event_put(cudaEvent_t e);
 cudaStream_t stream_get(bool high_priority = false);   // non-blocking stream of the current device

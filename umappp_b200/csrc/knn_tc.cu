@@ -137,6 +137,7 @@ struct TcSmem {
     uint64_t tmem_full[2];
     uint64_t tmem_empty[2];
     uint64_t a_full;
+    uint64_t mma_done;   // drain after an abort (mma_drain)
     uint32_t tmem_base;
     int abort_flag;
 };
@@ -151,7 +152,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_tc_kernel(const __grid_cons
                                                                int32_t* __restrict__ cand_idx,
                                                                float* __restrict__ cand_d2, int* __restrict__ err,
                                                                const int4* __restrict__ tasks,
-                                                               const int32_t* __restrict__ shifts) {
+                                                               const int32_t* __restrict__ shifts,
+                                                               long long wait_limit) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // the dynamic window is only guaranteed 16-byte aligned: round up to 1024
     TcSmem<KC>& sm = *reinterpret_cast<TcSmem<KC>*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -187,6 +189,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_tc_kernel(const __grid_cons
             mbar_init(&sm.tmem_empty[b], 32 * TC_EPI_WARPS);
         }
         mbar_init(&sm.a_full, 1);
+        mbar_init(&sm.mma_done, 1);
         sm.abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -215,7 +218,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_tc_kernel(const __grid_cons
             for (int it = 0; it < n_tiles; ++it) {
                 const int s = it % TC_STAGES;
                 const uint32_t round = it / TC_STAGES;
-                if (!mbar_wait(&sm.empty[s], (round & 1) ^ 1, abort_flag, err)) break;
+                if (!mbar_wait(&sm.empty[s], (round & 1) ^ 1, abort_flag, err, wait_limit)) break;
                 mbar_arrive_expect_tx(&sm.full[s], B_BYTES);
                 for (int c = 0; c < KC; ++c) {
                     tma_load_2d(sm.b_hi[s][c], &map_bhi, &sm.full[s], c * TC_KCHUNK, (ref_tile0 + it) * TC_N);
@@ -226,12 +229,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_tc_kernel(const __grid_cons
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            if (mbar_wait(&sm.a_full, 0, abort_flag, err)) {
+            if (mbar_wait(&sm.a_full, 0, abort_flag, err, wait_limit)) {
                 for (int it = 0; it < n_tiles; ++it) {
                     const int s = it % TC_STAGES;
                     const int buf = it & 1;
-                    if (!mbar_wait(&sm.full[s], (it / TC_STAGES) & 1, abort_flag, err)) break;
-                    if (!mbar_wait(&sm.tmem_empty[buf], ((it >> 1) & 1) ^ 1, abort_flag, err)) break;
+                    if (!mbar_wait(&sm.full[s], (it / TC_STAGES) & 1, abort_flag, err, wait_limit)) break;
+                    if (!mbar_wait(&sm.tmem_empty[buf], ((it >> 1) & 1) ^ 1, abort_flag, err, wait_limit)) break;
                     tc_fence_after();
                     const uint32_t d = tmem_base + buf * TC_N;
                     uint32_t acc = 0;
@@ -277,7 +280,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_tc_kernel(const __grid_cons
         float athr = -CUDART_INF_F;
         for (int it = 0; it < n_tiles; ++it) {
             const int buf = it & 1;
-            if (!mbar_wait(&sm.tmem_full[buf], (it >> 1) & 1, abort_flag, err)) break;
+            if (!mbar_wait(&sm.tmem_full[buf], (it >> 1) & 1, abort_flag, err, wait_limit)) break;
             tc_fence_after();
             const uint32_t taddr = tmem_base + (uint32_t(quarter * 32) << 16) + buf * TC_N + half * (TC_N / 2);
             const int col0 = (ref_tile0 + it) * TC_N + half * (TC_N / 2);   // operand row of column 0
@@ -352,6 +355,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) knn_tc_kernel(const __grid_cons
     __syncthreads();
     tc_fence_after();
     if (warp == 1) {
+        // after an abort, MMAs issued by lane 0 may still read shared memory and
+        // write the accumulators: wait for them before freeing TMEM
+        if (lane == 0 && *abort_flag) mma_drain(&sm.mma_done);
+        __syncwarp();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TC_TMEM_COLS));
     }
 }
@@ -405,7 +412,8 @@ void launch_tc(const Maps& m, const float* norms, int32_t n, int32_t n_pad, int3
     }
     const int n_tiles = n_pad / TC_N;
     knn_tc_kernel<KC, KCAP><<<ctas, TC_THREADS, smem, s>>>(m.ahi, m.alo, m.bhi, m.blo, norms, n, n_tiles, m.ksteps,
-                                                           cand_idx, cand_d2, err, tasks, shifts);
+                                                           cand_idx, cand_d2, err, tasks, shifts,
+                                                           device_wait_limit());
     UMAPB_LAUNCH_CHECK();
 }
 

@@ -24,8 +24,8 @@
 //               register list of the KCAP best (distance, index) pairs.
 // No cluster multicast.  Every mbarrier wait is bounded (tc_ptx.cuh): on
 // expiry the kernel records an error, raises a CTA-wide abort flag so the
-// other roles stop waiting, waits for its loads in flight, frees TMEM and
-// returns.
+// other roles stop waiting, waits for its loads and MMAs in flight, frees
+// TMEM and returns.
 #include <cuda.h>
 #include <cuda_fp16.h>
 #include <cudaTypedefs.h>
@@ -147,6 +147,7 @@ struct H16Smem {
     uint64_t tmem_full[QT][2];
     uint64_t tmem_empty[QT][2];
     uint64_t a_full;
+    uint64_t mma_done;   // drain after an abort (mma_drain)
     uint32_t tmem_base;
     int abort_flag;
 };
@@ -220,7 +221,7 @@ __global__ void __launch_bounds__(h16_threads<QT>(), 1)
                     int32_t* __restrict__ cand_idx, float* __restrict__ cand_d2, int* __restrict__ err,
                     const int4* __restrict__ tasks, const int64_t* __restrict__ qlist_off,
                     const int32_t* __restrict__ qlist_len, const int32_t* __restrict__ tile_list,
-                    const int32_t* __restrict__ row_map) {
+                    const int32_t* __restrict__ row_map, long long wait_limit) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     using Smem = H16Smem<KC, QT, NS>;
     Smem& sm = *reinterpret_cast<Smem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -249,6 +250,7 @@ __global__ void __launch_bounds__(h16_threads<QT>(), 1)
             }
         }
         mbar_init(&sm.a_full, 1);
+        mbar_init(&sm.mma_done, 1);
         sm.abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -279,7 +281,7 @@ __global__ void __launch_bounds__(h16_threads<QT>(), 1)
             unsigned mask;
             for (int u = 0; walk.next(tile, mask); ++u) {
                 const int s = u % NS;
-                if (!mbar_wait(&sm.empty[s], ((u / NS) & 1) ^ 1, abort_flag, err)) break;
+                if (!mbar_wait(&sm.empty[s], ((u / NS) & 1) ^ 1, abort_flag, err, wait_limit)) break;
                 mbar_arrive_expect_tx(&sm.full[s], B_BYTES);
                 for (int c = 0; c < KC; ++c) {
                     tma_load_2d(sm.b_hi[s][c], &map_bhi, &sm.full[s], c * H_KCHUNK, tile * H_N);
@@ -289,7 +291,7 @@ __global__ void __launch_bounds__(h16_threads<QT>(), 1)
             }
         }
     } else if (warp == 1) {
-        if (lane == 0 && mbar_wait(&sm.a_full, 0, abort_flag, err)) {
+        if (lane == 0 && mbar_wait(&sm.a_full, 0, abort_flag, err, wait_limit)) {
             bool ok = true;
             int32_t used[QT];   // accumulator rounds of each query tile so far
 #pragma unroll
@@ -298,12 +300,12 @@ __global__ void __launch_bounds__(h16_threads<QT>(), 1)
             unsigned mask;
             for (int u = 0; ok && walk.next(tile, mask); ++u) {
                 const int s = u % NS;
-                if (!mbar_wait(&sm.full[s], (u / NS) & 1, abort_flag, err)) break;
+                if (!mbar_wait(&sm.full[s], (u / NS) & 1, abort_flag, err, wait_limit)) break;
                 for (int t = 0; t < QT; ++t) {
                     if (!(mask & (1u << t))) continue;
                     const int c_t = used[t]++;
                     const int buf = c_t & 1;
-                    if (!mbar_wait(&sm.tmem_empty[t][buf], ((c_t >> 1) & 1) ^ 1, abort_flag, err)) {
+                    if (!mbar_wait(&sm.tmem_empty[t][buf], ((c_t >> 1) & 1) ^ 1, abort_flag, err, wait_limit)) {
                         ok = false;
                         break;
                     }
@@ -354,7 +356,7 @@ __global__ void __launch_bounds__(h16_threads<QT>(), 1)
         const int32_t my_len = walk.len[t];
         for (int c_t = 0; c_t < my_len; ++c_t) {
             const int buf = c_t & 1;
-            if (!mbar_wait(&sm.tmem_full[t][buf], (c_t >> 1) & 1, abort_flag, err)) break;
+            if (!mbar_wait(&sm.tmem_full[t][buf], (c_t >> 1) & 1, abort_flag, err, wait_limit)) break;
             tc_fence_after();
             const uint32_t taddr = tmem_base + (uint32_t(quarter * 32) << 16) + (t * 2 + buf) * H_N;
             const int col0 = my_list[c_t] * H_N;   // operand row of column 0
@@ -399,6 +401,10 @@ __global__ void __launch_bounds__(h16_threads<QT>(), 1)
     __syncthreads();
     tc_fence_after();
     if (warp == 1) {
+        // after an abort, MMAs issued by lane 0 may still read shared memory and
+        // write the accumulators: wait for them before freeing TMEM
+        if (lane == 0 && *abort_flag) mma_drain(&sm.mma_done);
+        __syncwarp();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
     }
 }
@@ -451,7 +457,7 @@ void launch16(const Maps16& m, const float* norms, float s2, float inv_s2, int32
     });
     knn_tc16_kernel<KC, QT, NS, KCAP><<<ctas, h16_threads<QT>(), smem, s>>>(
         m.ahi, m.alo, m.bhi, m.blo, norms, s2, inv_s2, m.ksteps, cand_idx, cand_d2, err, tk.tasks.get(),
-        tk.qlist_off.get(), tk.qlist_len.get(), tk.tile_list.get(), row_map);
+        tk.qlist_off.get(), tk.qlist_len.get(), tk.tile_list.get(), row_map, device_wait_limit());
     UMAPB_LAUNCH_CHECK();
 }
 

@@ -13,6 +13,10 @@
 // of 2 MiB.  A request takes a cached block of its own bucket or one up to a
 // quarter larger.  When the device reports out-of-memory the cache hands its
 // blocks back to the device pool and the allocation is retried once.
+//
+// umapb_set_workspace_limit caps the bytes the library holds on a device (in
+// use plus cached): a request beyond it first flushes the cache and then fails
+// with UMAPB_ERR_OOM, as a real out-of-memory does.
 #include <map>
 #include <mutex>
 #include <unordered_map>
@@ -38,6 +42,8 @@ struct Cache {
     std::unordered_map<void*, Block> in_use;            // by pointer
     std::vector<cudaEvent_t> spare_events;               // timing disabled
     size_t cached_bytes = 0;
+    size_t in_use_bytes = 0;
+    size_t limit = 0;                                    // 0: no limit
 };
 
 Cache& cache() {
@@ -98,7 +104,14 @@ void* ws_alloc(size_t bytes, cudaStream_t s) {
             c.spare_events.push_back(b.ready);
             b.ready = nullptr;
             c.in_use.emplace(b.ptr, b);
+            c.in_use_bytes += b.bytes;
             return b.ptr;
+        }
+        if (c.limit && c.in_use_bytes + c.cached_bytes + want > c.limit) {
+            flush_locked(c);
+            if (c.in_use_bytes + want > c.limit)
+                fail(UMAPB_ERR_OOM, "device workspace limit reached (" + std::to_string(c.limit) + " bytes; " +
+                                        std::to_string(want) + " more requested)");
         }
     }
     const double t0 = trace_enabled() ? host_ms() : 0.0;
@@ -116,6 +129,7 @@ void* ws_alloc(size_t bytes, cudaStream_t s) {
     if (trace_enabled()) trace_wait("device allocation", t0, want, __FILE__, __LINE__);
     std::lock_guard<std::mutex> lock(c.mu);
     c.in_use.emplace(p, Block{p, want, dev, s, nullptr});
+    c.in_use_bytes += want;
     return p;
 }
 
@@ -130,6 +144,7 @@ void ws_free(void* p, cudaStream_t s) {
     }
     Block b = it->second;
     c.in_use.erase(it);
+    c.in_use_bytes -= b.bytes;
     cudaEvent_t ev = nullptr;
     if (!c.spare_events.empty()) {
         ev = c.spare_events.back();
@@ -161,6 +176,14 @@ void ws_release_cached() {
     Cache& c = cache();
     std::lock_guard<std::mutex> lock(c.mu);
     flush_locked(c);
+}
+
+size_t ws_set_limit(size_t bytes) {
+    Cache& c = cache();
+    std::lock_guard<std::mutex> lock(c.mu);
+    const size_t prev = c.limit;
+    c.limit = bytes;
+    return prev;
 }
 
 // ------------------------------------------------------------ event pool --

@@ -14,6 +14,10 @@
 namespace umapb {
 namespace tc {
 
+// Polls of a bounded mbarrier wait: the default limit of the role waits (the
+// kernels take the limit as an argument, umapb_set_device_wait_limit), and the
+// fixed limit of the drain waits at exit, which wait for copies and MMAs
+// already issued and must not give up early.
 constexpr long long WAIT_LIMIT = 1ll << 26;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -45,8 +49,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Bounded wait; returns false (and raises the abort flag) on expiry or abort.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* err) {
-    for (long long i = 0; i < WAIT_LIMIT; ++i) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* err,
+                                          long long limit) {
+    for (long long i = 0; i < limit; ++i) {
         if (mbar_try_wait(bar, parity)) return true;
         if (*abort_flag) return false;
         if (i > 64) __nanosleep(32);
@@ -82,6 +87,15 @@ __device__ __forceinline__ uint64_t smem_desc(const void* p) {
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                  : "memory");
+}
+
+// After an abort: the MMAs this thread has issued (tcgen05.mma is
+// asynchronous) must finish before their shared-memory operands go away and
+// before the accumulators are freed.  A commit to 'bar' (fresh, count 1)
+// arrives once all of them are done; waited for with the drain limit.
+__device__ __forceinline__ void mma_drain(uint64_t* bar) {
+    mma_commit(bar);
+    for (long long i = 0; i < WAIT_LIMIT && !mbar_try_wait(bar, 0); ++i) __nanosleep(64);
 }
 
 __device__ __forceinline__ void tmem_load32(uint32_t taddr, uint32_t (&r)[32]) {
