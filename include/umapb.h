@@ -112,10 +112,10 @@ int64_t umapb_launch_count(void);
 int64_t umapb_set_device_wait_limit(int64_t polls);
 
 /*
- * Caps the device memory the library holds at once (blocks in use plus its
- * cache of freed blocks; process-wide, all devices): an allocation beyond the
- * cap first returns the cache to the device and then fails with UMAPB_ERR_OOM,
- * as a real out-of-memory does.  0 removes the cap (the default).  Returns the
+ * Caps the device memory the library has in use at once (process-wide, all
+ * devices): an allocation beyond the cap fails with UMAPB_ERR_OOM, as a real
+ * out-of-memory does, and the library's cache of freed blocks is returned to
+ * the device before in-use plus cached bytes would exceed it.  0 removes the cap (the default).  Returns the
  * previous cap.  An extension (the reference allocates host memory only): for
  * callers that share a GPU, and for testing the out-of-memory path.
  */

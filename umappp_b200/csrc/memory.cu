@@ -14,9 +14,9 @@
 // quarter larger.  When the device reports out-of-memory the cache hands its
 // blocks back to the device pool and the allocation is retried once.
 //
-// umapb_set_workspace_limit caps the bytes the library holds on a device (in
-// use plus cached): a request beyond it first flushes the cache and then fails
-// with UMAPB_ERR_OOM, as a real out-of-memory does.
+// umapb_set_workspace_limit caps the bytes in use: a request beyond it fails
+// with UMAPB_ERR_OOM, as a real out-of-memory does; new device memory that
+// would take in-use plus cached bytes past the cap first flushes the cache.
 #include <map>
 #include <mutex>
 #include <unordered_map>
@@ -87,6 +87,9 @@ void* ws_alloc(size_t bytes, cudaStream_t s) {
     Cache& c = cache();
     {
         std::lock_guard<std::mutex> lock(c.mu);
+        if (c.limit && c.in_use_bytes + want > c.limit)
+            fail(UMAPB_ERR_OOM, "device workspace limit reached (" + std::to_string(c.limit) + " bytes; " +
+                                    std::to_string(want) + " more requested)");
         for (auto it = c.free_blocks.lower_bound(want); it != c.free_blocks.end() && it->first <= want + want / 4;
              ++it) {
             if (it->second.device != dev) continue;
@@ -107,12 +110,7 @@ void* ws_alloc(size_t bytes, cudaStream_t s) {
             c.in_use_bytes += b.bytes;
             return b.ptr;
         }
-        if (c.limit && c.in_use_bytes + c.cached_bytes + want > c.limit) {
-            flush_locked(c);
-            if (c.in_use_bytes + want > c.limit)
-                fail(UMAPB_ERR_OOM, "device workspace limit reached (" + std::to_string(c.limit) + " bytes; " +
-                                        std::to_string(want) + " more requested)");
-        }
+        if (c.limit && c.in_use_bytes + c.cached_bytes + want > c.limit) flush_locked(c);
     }
     const double t0 = trace_enabled() ? host_ms() : 0.0;
     void* p = nullptr;

@@ -544,6 +544,11 @@ __global__ void seg_first_kernel(const int64_t* __restrict__ seg_pos, int64_t ns
 // steps, which move it as a tail), so no event works from a copy of the head
 // older than one event.
 enum HeadMode { HEAD_AT_END = 0, HEAD_PER_EVENT = 1, HEAD_FRESH = 2 };
+// PAIR: an undirected edge fires in both directions in the same epochs (the
+// union gives both directions the same weight, hence the same schedule); the
+// event whose head is the smaller index takes both attractive steps, the
+// second one (head and tail exchanged) from the positions the first one left,
+// and the event of the larger head takes only its negative samples.
 
 // Coherent device-scope load: ordered after this thread's own earlier atomic
 // adds to the same address.
@@ -553,7 +558,7 @@ __device__ __forceinline__ float2 ld_relaxed_f2(const float2* p) {
     return v;
 }
 
-template <int NB, int MINB, bool PRECISE = false, int MODE = HEAD_AT_END>
+template <int NB, int MINB, bool PRECISE = false, int MODE = HEAD_AT_END, bool PAIR = false>
 __global__ void __launch_bounds__(256, MINB) sgd_epoch_2d_f32(const int32_t* __restrict__ order, int64_t base,
                                                         int64_t slot0, int64_t slot1,
                                                         const int64_t* __restrict__ seg_pos,
@@ -593,17 +598,29 @@ __global__ void __launch_bounds__(256, MINB) sgd_epoch_2d_f32(const int32_t* __r
                         yk[i] = __ldcg(&Y[ks[i]]);
                     }
                 }
-                if (attract) {
+                if (attract && (!PAIR || pr.y > h)) {
                     const float dx = hx - yt.x, dy = hy - yt.y;
                     const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
                     const float cf = PRECISE ? attract_coef_precise(d2, p) : attract_coef_fast(d2, p);
-                    const float gx = p.alpha * clamp4(cf * dx);
-                    const float gy = p.alpha * clamp4(cf * dy);
+                    float gx = p.alpha * clamp4(cf * dx);
+                    float gy = p.alpha * clamp4(cf * dy);
                     hx += gx;
                     hy += gy;
+                    if (PAIR) {   // the reverse edge's step: head = tail, from the moved positions
+                        const float tx = yt.x - gx, ty = yt.y - gy;
+                        const float ex2 = tx - hx, ey2 = ty - hy;
+                        const float e2 = floor_eps(__fmaf_rn(ex2, ex2, ey2 * ey2));
+                        const float cf2 = PRECISE ? attract_coef_precise(e2, p) : attract_coef_fast(e2, p);
+                        const float g2x = p.alpha * clamp4(cf2 * ex2);
+                        const float g2y = p.alpha * clamp4(cf2 * ey2);
+                        hx -= g2x;
+                        hy -= g2y;
+                        gx -= g2x;   // the tail's total move is -(g - g2)
+                        gy -= g2y;
+                    }
                     atomicAdd(&Y[pr.y], make_float2(-gx, -gy));
-                    attract = false;
                 }
+                attract = false;
 #pragma unroll
                 for (int i = 0; i < NB; ++i) {
                     if (i < m && ks[i] != h) {
@@ -635,6 +652,8 @@ const Sgd2dVariant SGD_2D_VARIANTS[] = {
     {sgd_epoch_2d_f32<8, 4, true>, 8, 4},   // libm powf and IEEE division (precision check)
     {sgd_epoch_2d_f32<8, 4, false, HEAD_PER_EVENT>, 8, 4},
     {sgd_epoch_2d_f32<8, 4, false, HEAD_FRESH>, 8, 4},
+    {sgd_epoch_2d_f32<8, 4, false, HEAD_AT_END, true>, 8, 4},   // 7: PAIR
+    {sgd_epoch_2d_f32<8, 4, false, HEAD_FRESH, true>, 8, 4},    // 8: PAIR, fresh head
 };
 constexpr int NUM_SGD_2D_VARIANTS = sizeof(SGD_2D_VARIANTS) / sizeof(SGD_2D_VARIANTS[0]);
 constexpr int NUM_TUNED_VARIANTS = 4;   // the tuner picks among launch shapes of one arithmetic
@@ -982,7 +1001,12 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
         const bool use_2d = std::is_same<T, float>::value && num_dim == 2;
         const int blk = use_2d ? block : 128;
         const int resident = use_2d ? sm_count() * sgd_2d_resident(variant, block) : blocks_gen;
-        const unsigned g = grid_for(nsegs, blk, static_cast<unsigned>(resident * grid_multiple()));
+        unsigned cap_blocks = static_cast<unsigned>(resident * grid_multiple());
+        if (const char* e = std::getenv("UMAPB_SGD_MAX_BLOCKS")) {   // cap on the blocks in flight
+            const int x = std::atoi(e);
+            if (x >= 1) cap_blocks = std::min<unsigned>(cap_blocks, static_cast<unsigned>(x));
+        }
+        const unsigned g = grid_for(nsegs, blk, cap_blocks);
         // Parallel updates read positions that the serial order would already
         // have moved; when every event of an epoch is in flight at once the
         // layouts come out measurably tighter (lower edge cross-entropy) than
@@ -1003,7 +1027,7 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
         for (int l = 0; l < L; ++l) {
             const int64_t slot0 = off[(P * l) / L], slot1 = off[(P * (l + 1)) / L];
             if (slot1 <= slot0) continue;
-            const unsigned gl = grid_for(slot1 - slot0, blk, static_cast<unsigned>(resident * grid_multiple()));
+            const unsigned gl = grid_for(slot1 - slot0, blk, cap_blocks);
             if (use_2d) {
                 if constexpr (std::is_same<T, float>::value) {
                     SGD_2D_VARIANTS[variant].kernel<<<gl, blk, 0, s>>>(order, win.host_seg_first[w], slot0, slot1,
