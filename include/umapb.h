@@ -112,6 +112,16 @@ int64_t umapb_launch_count(void);
 int64_t umapb_set_device_wait_limit(int64_t polls);
 
 /*
+ * Roofline probe (an extension): the rate of uniformly random float2 accesses
+ * to an array of num_points float2 values in device memory, with nothing else
+ * to do -- mode 0: loads through L2 (ld.global.cg), mode 1: atomic adds
+ * (red.global.add.v2.f32) -- measured with CUDA events over 'reps' launches of
+ * about 'accesses' accesses each.  At 10^6 points the array (8 MB) stays in
+ * L2, which is where the SGD epochs' gathers and atomics land.
+ */
+int umapb_measure_random_access(int64_t num_points, int64_t accesses, int mode, int reps, double* per_second);
+
+/*
  * Caps the device memory the library has in use at once (process-wide, all
  * devices): an allocation beyond the cap fails with UMAPB_ERR_OOM, as a real
  * out-of-memory does, and the library's cache of freed blocks is returned to

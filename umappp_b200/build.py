@@ -26,7 +26,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
                  "-I" + os.path.join(ROOT, "include"), "-I" + CSRC, "--expt-relaxed-constexpr"]
 NO_FMAD = {"similarities.cu", "graph.cu", "sgd.cu"}
-SOURCES = ["capi.cu", "memory.cu", "knn.cu", "knn_tc.cu", "knn_tc16.cu", "knn_tree.cu", "similarities.cu", "graph.cu", "spectral.cu", "sgd.cu", "adjoint.cu",
+SOURCES = ["capi.cu", "memory.cu", "knn.cu", "knn_tc.cu", "knn_tc16.cu", "knn_tree.cu", "similarities.cu", "graph.cu", "spectral.cu", "sgd.cu", "adjoint.cu", "probe.cu",
            "find_ab.cpp"]
 
 

@@ -622,6 +622,15 @@ int64_t umapb_knn_last_tile_pairs(void) { return last_knn_tiles_scanned(); }
 
 double umapb_knn_last_kernel_ms(void) { return last_knn_kernel_ms(); }
 
+int umapb_measure_random_access(int64_t num_points, int64_t accesses, int mode, int reps, double* per_second) {
+    return guarded([&] {
+        require_device();
+        require(per_second != nullptr, "per_second must not be NULL");
+        Context& c = thread_context();
+        *per_second = measure_random_access(num_points, accesses, mode, reps, c.stream);
+    });
+}
+
 int umapb_neighbor_similarities(int dtype, int32_t num_obs, const int64_t* row_ptr, void* distances,
                                 double local_connectivity, double bandwidth, double min_k_dist_scale, int use_newton,
                                 double* rho_out, double* sigma_out) {

@@ -143,73 +143,50 @@ template <typename T>
 void random_init(int32_t n, int num_dim, T* Y, uint64_t seed, double scale, cudaStream_t s);
 
 // ---- SGD (sgd.cu) -----------------------------------------------------------
-// Per-epoch event lists of the deterministic schedule, precomputed for a
-// window of epochs: event e of epoch w is (head, tail, negative-sample count),
-// stored in CSR order of the edges.
+// Epochs of the reference's SGD: one thread per head row, the schedule
+// advanced in place in the reference's Float_ arithmetic (see sgd.cu).
 template <typename T>
 class SgdEngine {
 public:
     // ep->enext0 / enneg0 describe the schedule at epoch 'base_epoch'.
     void setup(const DeviceEpochs<T>* ep, cudaStream_t s, int base_epoch = 0);
-    // Runs epochs [first, last) on Y (n x num_dim, device).
+    // Runs epochs [first, last) on Y (n x num_dim, device).  ms_schedule is
+    // always 0 (no schedule stage); ms_sgd is the epochs' device time.
     void run(T* Y, int num_dim, int first, int last, double a, double b, double gamma, double learning_rate,
              uint64_t seed, cudaStream_t s, float* ms_schedule, float* ms_sgd);
     // Exact per-epoch [firing, negatives] counts over [first, last) (host output).
     void counts(int first, int last, int64_t* out, cudaStream_t s);
     // Schedule state (enext, enneg) at 'epoch' into device arrays.
     void state_at(int epoch, T* enext, T* enneg, cudaStream_t s);
-    size_t event_budget_bytes = 0;  // window buffer cap; 0: 4 GiB or 1/16 of device memory (sgd.cu)
     // Batched runs: instance i owns observations [inst_start[i], inst_start[i+1])
     // (device array of num_inst + 1 entries); negative samples stay inside it.
     void set_instances(const int32_t* inst_start, int32_t num_inst) {
         inst_start_ = inst_start;
         num_inst_ = num_inst;
     }
-    // Record each window's epochs as one CUDA graph and launch that.
+    // Record the epochs of each run() call as one CUDA graph and launch that.
     bool use_graphs = false;
-    // Minimum number of ordered head slices per epoch (sgd.cu, run()).
-    int min_phases = default_min_phases();
-    static int default_min_phases();
     // Pick the 2-d epoch kernel's block size and variant by timing the
-    // candidates on a scratch copy of the layout (sgd.cu, tune()).
+    // candidates on scratch copies (sgd.cu, tune()).
     bool autotune = false;
+    // Firing edges between publications of a row's head (sgd.cu).
+    int publish_every = default_publish_every();
     int block_size() const { return block_; }
     int variant() const { return variant_; }   // 2-d kernel variant (sgd.cu, SGD_2D_VARIANTS)
 
 private:
-    // One window of consecutive epochs: every firing event (head, tail) with
-    // its negative-sample count, grouped by epoch and head segment, and each
-    // epoch's segments ordered by head slice.  The engine keeps two, so that
-    // the next window is built (on a second stream) while the epochs of the
-    // current one run.
-    struct Window {
-        int begin = 0, end = 0;                   // epochs [begin, end)
-        DevArray<int2> ht;
-        DevArray<uint16_t> nneg;
-        DevArray<int64_t> seg_pos;                // first event of every head segment, plus the event total (see sgd.cu)
-        DevArray<int64_t> seg_first;              // per epoch: index of its first segment (end - begin + 1)
-        DevArray<int64_t> epoch_offsets;          // end - begin + 1 entries
-        DevArray<int32_t> seg_order;              // per epoch: its segments by head slice (offsets from seg_first)
-        std::vector<int64_t> host_seg_first, host_epoch_offsets;
-        std::vector<int64_t> host_bucket_off;     // per epoch: buckets + 1 slot offsets of the slices
-        int buckets = 8;
-        int seg_max = 8;                          // longest segment
-        bool ordered = false;                     // seg_order in use (several instances)
-    };
-    void build_window(Window& win, int first, int last_wanted, cudaStream_t s);
-    void verify_window(const Window& win, int first, int W, cudaStream_t s);
-    void build_slices(Window& win, int64_t nseg, int W, cudaStream_t s);
     template <class Launch>
-    void tune(T* Y, int num_dim, int first, int stop, const Window& win, Launch& launch, cudaStream_t s);
+    void tune(T* Y, int num_dim, int epoch, Launch& launch, cudaStream_t s);
     static int default_variant();
+    static int default_publish_every();
     int block_ = 256, variant_ = default_variant();
     const DeviceEpochs<T>* ep_ = nullptr;
     const int32_t* inst_start_ = nullptr;
     int32_t num_inst_ = 1;
     int base_epoch_ = 0;
     DevArray<T> enext_, enneg_;    // schedule state at state_epoch_
+    DevArray<int32_t> order_;      // rows by descending firing rate
     int state_epoch_ = 0;          // epoch the state arrays describe
-    Window win_[2];
 };
 
 // ---- adjoint (adjoint.cu) ----------------------------------------------------
@@ -217,6 +194,11 @@ template <typename T>
 void loss_grad(int32_t n, int num_dim, const T* Y, const int64_t* ptr, const int32_t* idx, const T* w, double a,
                double b, double eps_rep, bool with_constant, double* loss_out, T* grad_Y, double* grad_ab,
                cudaStream_t s);
+
+// ---- roofline probes (probe.cu) ----------------------------------------------
+// Random float2 accesses per second over an n-point array (mode 0: L2 gathers,
+// 1: atomic adds).
+double measure_random_access(int64_t n, int64_t accesses, int mode, int reps, cudaStream_t s);
 
 // ---- host (find_ab.cpp) -------------------------------------------------------
 void find_ab(double spread, double min_dist, double* a, double* b);
