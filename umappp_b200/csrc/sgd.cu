@@ -284,12 +284,24 @@ __device__ __forceinline__ void add_totals(unsigned long long* totals, unsigned 
     }
 }
 
-// 2-d FP32 rows.  Negative samples are gathered NB at a time: their indices
-// do not depend on the layout, so all loads of a batch (and the tail's) are
-// in flight together, and the head then takes the updates in sequence.  NB
-// and the minimum number of resident 256-thread blocks (which caps the
-// registers per thread) are the variants in SGD_2D_VARIANTS.
-template <int NB, int MINB>
+// Coherent device-scope load: ordered after this thread's own earlier atomic
+// adds to the same address (per-location coherence), so a head re-read after
+// its own publication sees it, plus whatever other threads have added.
+__device__ __forceinline__ float2 ld_relaxed_f2(const float2* q) {
+    float2 v;
+    asm volatile("ld.relaxed.gpu.global.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(q) : "memory");
+    return v;
+}
+
+// 2-d FP32 rows.  Per firing edge: the head (FRESH: re-read, so that the pulls
+// of other rows' attractive steps on it are seen), the tail and the first NB
+// negative samples are gathered together -- the negative-sample indices do
+// not depend on the layout -- and, while they are in flight, the row is
+// scanned for its next firing edge, whose target and schedule state are
+// loaded.  Then the updates are applied in the reference's order.  NB and
+// the minimum number of resident 256-thread blocks (which caps the registers
+// per thread) are the variants in SGD_2D_VARIANTS.
+template <int NB, int MINB, bool FRESH>
 __global__ void __launch_bounds__(256, MINB) sgd_rows_2d_f32(RowArgs<float> r, float2* __restrict__ Y,
                                                              SgdParams<float> p) {
     unsigned long long fired = 0, drawn = 0;
@@ -306,48 +318,71 @@ __global__ void __launch_bounds__(256, MINB) sgd_rows_2d_f32(RowArgs<float> r, f
                 int32_t nbase;
                 uint32_t nsize;
                 instance_range(h, p, nbase, nsize);
-                const float2 y0 = __ldcg(&Y[h]);
-                float hx = y0.x, hy = y0.y;
-                float px = hx, py = hy;   // head as last published
+                float hx, hy;
+                if (!FRESH) {
+                    const float2 y0 = __ldcg(&Y[h]);
+                    hx = y0.x;
+                    hy = y0.y;
+                }
+                // the current firing edge: target, schedule state
+                int32_t t = r.targets[j];
+                float ep = r.eps[j], en = r.enext[j], enn = r.enneg[j];
+                float px = 0.0f, py = 0.0f;   // head as last published
                 int since = 0;
+                bool first = true;
                 do {
-                    // the schedule step of edge j (optimize_layout.hpp:160-161,178-179)
-                    const float ep = r.eps[j];
-                    const float epns = ep / p.rate;
-                    const float enn = r.enneg[j];
+                    // gathers of this edge: head, tail, first batch of negatives
+                    float2 yh;
+                    if (FRESH) yh = ld_relaxed_f2(&Y[h]);
+                    const float2 yt = __ldcg(&Y[t]);
+                    const float epns = ep / p.rate;   // optimize_layout.hpp:160-161
                     const int nn = static_cast<int>((ef - enn) / epns);
-                    r.enext[j] = r.enext[j] + ep;
-                    r.enneg[j] = enn + static_cast<float>(nn) * epns;
-                    const int32_t t = r.targets[j];
                     int remaining = nn > 0 ? nn : 0;   // a negative count draws nothing, as in the reference's loop
+                    NegStream rng(static_cast<uint32_t>(h), static_cast<uint32_t>(t), p.epoch_u, p.k0, p.k1);
+                    int m = remaining < NB ? remaining : NB;
+                    int32_t ks[NB];
+                    float2 yk[NB];
+#pragma unroll
+                    for (int q = 0; q < NB; ++q) {
+                        if (q < m) {
+                            ks[q] = nbase + rng.bounded(nsize);
+                            yk[q] = __ldcg(&Y[ks[q]]);
+                        }
+                    }
+                    // the schedule step (:178-179) and the next firing edge, while the gathers fly
+                    r.enext[j] = en + ep;
+                    r.enneg[j] = enn + static_cast<float>(nn) * epns;
                     ++fired;
                     drawn += remaining;
-                    const float2 yt = __ldcg(&Y[t]);
-                    NegStream rng(static_cast<uint32_t>(h), static_cast<uint32_t>(t), p.epoch_u, p.k0, p.k1);
-                    bool attract = true;
-                    do {
-                        // issue this batch's gathers, then apply the updates in order
-                        const int m = remaining < NB ? remaining : NB;
-                        int32_t ks[NB];
-                        float2 yk[NB];
-#pragma unroll
-                        for (int q = 0; q < NB; ++q) {
-                            if (q < m) {
-                                ks[q] = nbase + rng.bounded(nsize);
-                                yk[q] = __ldcg(&Y[ks[q]]);
-                            }
-                        }
-                        if (attract) {
-                            const float dx = hx - yt.x, dy = hy - yt.y;
-                            const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
-                            const float cf = attract_coef_fast(d2, p);
-                            const float gx = p.alpha * clamp4(cf * dx);
-                            const float gy = p.alpha * clamp4(cf * dy);
-                            hx += gx;
-                            hy += gy;
-                            atomicAdd(&Y[t], make_float2(-gx, -gy));
-                            attract = false;
-                        }
+                    const int64_t j2 = next_firing(r.enext, j + 1, r1, ef);
+                    int32_t t2 = 0;
+                    float ep2 = 0.0f, en2 = 0.0f, enn2 = 0.0f;
+                    if (j2 < r1) {
+                        t2 = r.targets[j2];
+                        ep2 = r.eps[j2];
+                        en2 = r.enext[j2];
+                        enn2 = r.enneg[j2];
+                    }
+                    if (FRESH) {
+                        hx = yh.x;
+                        hy = yh.y;
+                    }
+                    if (first || FRESH) {
+                        px = hx;
+                        py = hy;
+                        first = false;
+                    }
+                    {   // attractive step (:145-155)
+                        const float dx = hx - yt.x, dy = hy - yt.y;
+                        const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
+                        const float cf = attract_coef_fast(d2, p);
+                        const float gx = p.alpha * clamp4(cf * dx);
+                        const float gy = p.alpha * clamp4(cf * dy);
+                        hx += gx;
+                        hy += gy;
+                        atomicAdd(&Y[t], make_float2(-gx, -gy));
+                    }
+                    while (true) {   // negative samples (:157-176)
 #pragma unroll
                         for (int q = 0; q < NB; ++q) {
                             if (q < m && ks[q] != h) {
@@ -359,14 +394,27 @@ __global__ void __launch_bounds__(256, MINB) sgd_rows_2d_f32(RowArgs<float> r, f
                             }
                         }
                         remaining -= m;
-                    } while (remaining > 0);
-                    j = next_firing(r.enext, j + 1, r1, ef);
-                    if (++since >= p.publish_every || j >= r1) {
+                        if (remaining <= 0) break;
+                        m = remaining < NB ? remaining : NB;
+#pragma unroll
+                        for (int q = 0; q < NB; ++q) {
+                            if (q < m) {
+                                ks[q] = nbase + rng.bounded(nsize);
+                                yk[q] = __ldcg(&Y[ks[q]]);
+                            }
+                        }
+                    }
+                    j = j2;
+                    if (FRESH || ++since >= p.publish_every || j >= r1) {
                         atomicAdd(&Y[h], make_float2(hx - px, hy - py));
                         px = hx;
                         py = hy;
                         since = 0;
                     }
+                    t = t2;
+                    ep = ep2;
+                    en = en2;
+                    enn = enn2;
                 } while (j < r1);
             }
         }
@@ -380,10 +428,10 @@ struct Sgd2dVariant {
     int neg_batch, min_blocks;
 };
 const Sgd2dVariant SGD_2D_VARIANTS[] = {
-    {sgd_rows_2d_f32<8, 4>, 8, 4},     // default: 64 registers
-    {sgd_rows_2d_f32<12, 3>, 12, 3},
-    {sgd_rows_2d_f32<6, 6>, 6, 6},     // 40 registers
-    {sgd_rows_2d_f32<8, 2>, 8, 2},
+    {sgd_rows_2d_f32<8, 4, true>, 8, 4},     // default
+    {sgd_rows_2d_f32<8, 2, true>, 8, 2},
+    {sgd_rows_2d_f32<6, 5, true>, 6, 5},
+    {sgd_rows_2d_f32<8, 4, false>, 8, 4},    // head kept in registers, published every publish_every edges
 };
 constexpr int NUM_SGD_2D_VARIANTS = sizeof(SGD_2D_VARIANTS) / sizeof(SGD_2D_VARIANTS[0]);
 
@@ -628,6 +676,8 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
     const bool use_2d = std::is_same<T, float>::value && num_dim == 2;
     const bool check = check_schedule();
     cudaStream_t s = caller;
+    int max_blocks = 0;   // UMAPB_SGD_MAX_BLOCKS: cap on the blocks of an epoch launch (0: all resident)
+    if (const char* e = std::getenv("UMAPB_SGD_MAX_BLOCKS")) max_blocks = std::max(0, std::atoi(e));
 
     // One epoch launch on (Yp, schedule state en/enn), claiming rows from 'counter'.
     auto launch = [&](T* Yp, T* en, T* enn, int* counter, unsigned long long* totals, int e_abs, int block,
@@ -649,7 +699,8 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
         r.totals = totals;
         if (use_2d) {
             if constexpr (std::is_same<T, float>::value) {
-                const unsigned g = static_cast<unsigned>(sm_count() * sgd_2d_resident(variant, block) * 256 / block);
+                unsigned g = static_cast<unsigned>(sm_count() * sgd_2d_resident(variant, block));
+                if (max_blocks > 0) g = std::min<unsigned>(g, static_cast<unsigned>(max_blocks));
                 SGD_2D_VARIANTS[variant].kernel<<<g, block, 0, s>>>(r, reinterpret_cast<float2*>(Yp), p);
             }
         } else {
