@@ -33,6 +33,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cstdlib>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <type_traits>
@@ -131,6 +132,14 @@ __global__ void row_rate_kernel(int32_t n, const int64_t* __restrict__ ptr, cons
     }
 }
 
+__global__ void count_at_least_kernel(int32_t n, const uint32_t* __restrict__ key, uint32_t threshold,
+                                      int* __restrict__ count) {
+    int c = 0;
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) c += key[i] >= threshold;
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
+}
+
 // ---------------------------------------------------------- epoch kernels --
 
 template <typename T>
@@ -162,8 +171,9 @@ struct RowArgs {
     const T* eps;
     T* enext;
     T* enneg;
-    int* counter;              // rows claimed so far in this epoch
+    int* counter;              // work units claimed so far in this epoch
     unsigned long long* totals;   // optional: [firing edges, negative samples drawn] of this epoch
+    int32_t nhub;              // 2-d kernel: order[0, nhub) are hub rows, one warp each
 };
 
 // Observation range [base, base + size) of the instance that owns h.
@@ -293,130 +303,258 @@ __device__ __forceinline__ float2 ld_relaxed_f2(const float2* q) {
     return v;
 }
 
-// 2-d FP32 rows.  Per firing edge: the head (FRESH: re-read, so that the pulls
-// of other rows' attractive steps on it are seen), the tail and the first NB
-// negative samples are gathered together -- the negative-sample indices do
-// not depend on the layout -- and, while they are in flight, the row is
-// scanned for its next firing edge, whose target and schedule state are
-// loaded.  Then the updates are applied in the reference's order.  NB and
-// the minimum number of resident 256-thread blocks (which caps the registers
-// per thread) are the variants in SGD_2D_VARIANTS.
-template <int NB, int MINB, bool FRESH>
+// 2-d FP32 rows.  Work units, claimed by warps in order: first the hub rows
+// (expected to fire at least HUB_RATE edges per epoch; one row per warp),
+// then the other rows, 32 per warp (one per lane).
+constexpr int HUB_RATE = 32;
+constexpr int BULK_CHUNK = 8;    // edges of a row whose schedule state a lane loads at once
+
+// A lane's row.  Its schedule state is read BULK_CHUNK edges at a time, the
+// next chunk's loads in flight while the current chunk's firing edges are
+// processed.  Per firing edge the head (re-read: it sees the pulls of other
+// rows' attractive steps), the tail and the first NB negative samples are
+// gathered together -- the negative-sample indices do not depend on the
+// layout -- and the updates are then applied in the reference's order; the
+// head's move is published after each firing edge.
+template <int NB>
+__device__ __forceinline__ void bulk_row(int32_t h, const RowArgs<float>& r, float2* __restrict__ Y,
+                                         const SgdParams<float>& p, unsigned long long& fired,
+                                         unsigned long long& drawn) {
+    const float ef = p.epoch;
+    const int64_t j0 = r.ptr[h], r1 = r.ptr[h + 1];
+    if (j0 >= r1) return;
+    int32_t nbase;
+    uint32_t nsize;
+    instance_range(h, p, nbase, nsize);
+    float en[BULK_CHUNK];
+#pragma unroll
+    for (int q = 0; q < BULK_CHUNK; ++q) en[q] = (j0 + q < r1) ? r.enext[j0 + q] : CUDART_INF_F;
+    for (int64_t c = j0; c < r1; c += BULK_CHUNK) {
+        float en_next[BULK_CHUNK];
+#pragma unroll
+        for (int q = 0; q < BULK_CHUNK; ++q) {
+            const int64_t jn = c + BULK_CHUNK + q;
+            en_next[q] = (jn < r1) ? r.enext[jn] : CUDART_INF_F;
+        }
+        unsigned mask = 0;
+#pragma unroll
+        for (int q = 0; q < BULK_CHUNK; ++q) mask |= (en[q] <= ef ? 1u : 0u) << q;
+        if (mask) {
+            int32_t tq[BULK_CHUNK];
+            float epq[BULK_CHUNK], ennq[BULK_CHUNK];
+#pragma unroll
+            for (int q = 0; q < BULK_CHUNK; ++q) {
+                if (mask & (1u << q)) {
+                    tq[q] = r.targets[c + q];
+                    epq[q] = r.eps[c + q];
+                    ennq[q] = r.enneg[c + q];
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < BULK_CHUNK; ++q) {
+                if (!(mask & (1u << q))) continue;
+                const int32_t t = tq[q];
+                const float epns = epq[q] / p.rate;   // optimize_layout.hpp:160-161
+                const int nn = static_cast<int>((ef - ennq[q]) / epns);
+                r.enext[c + q] = en[q] + epq[q];       // :178-179
+                r.enneg[c + q] = ennq[q] + static_cast<float>(nn) * epns;
+                int remaining = nn > 0 ? nn : 0;       // a negative count draws nothing, as in the reference's loop
+                ++fired;
+                drawn += remaining;
+                const float2 yh = ld_relaxed_f2(&Y[h]);
+                const float2 yt = __ldcg(&Y[t]);
+                NegStream rng(static_cast<uint32_t>(h), static_cast<uint32_t>(t), p.epoch_u, p.k0, p.k1);
+                int m = remaining < NB ? remaining : NB;
+                int32_t ks[NB];
+                float2 yk[NB];
+#pragma unroll
+                for (int b = 0; b < NB; ++b) {
+                    if (b < m) {
+                        ks[b] = nbase + rng.bounded(nsize);
+                        yk[b] = __ldcg(&Y[ks[b]]);
+                    }
+                }
+                float hx = yh.x, hy = yh.y;
+                {   // attractive step (:145-155)
+                    const float dx = hx - yt.x, dy = hy - yt.y;
+                    const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
+                    const float cf = attract_coef_fast(d2, p);
+                    const float gx = p.alpha * clamp4(cf * dx);
+                    const float gy = p.alpha * clamp4(cf * dy);
+                    hx += gx;
+                    hy += gy;
+                    atomicAdd(&Y[t], make_float2(-gx, -gy));
+                }
+                while (true) {   // negative samples (:157-176)
+#pragma unroll
+                    for (int b = 0; b < NB; ++b) {
+                        if (b < m && ks[b] != h) {
+                            const float dx = hx - yk[b].x, dy = hy - yk[b].y;
+                            const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
+                            const float cf = repulse_coef_fast(d2, p);
+                            hx = __fmaf_rn(p.alpha, clamp4(cf * dx), hx);
+                            hy = __fmaf_rn(p.alpha, clamp4(cf * dy), hy);
+                        }
+                    }
+                    remaining -= m;
+                    if (remaining <= 0) break;
+                    m = remaining < NB ? remaining : NB;
+#pragma unroll
+                    for (int b = 0; b < NB; ++b) {
+                        if (b < m) {
+                            ks[b] = nbase + rng.bounded(nsize);
+                            yk[b] = __ldcg(&Y[ks[b]]);
+                        }
+                    }
+                }
+                atomicAdd(&Y[h], make_float2(hx - yh.x, hy - yh.y));
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < BULK_CHUNK; ++q) en[q] = en_next[q];
+    }
+}
+
+// Gathered operands of one firing edge of a hub row (shared memory).
+template <int NB>
+struct HubEvent {
+    float2 yt;
+    float2 yk[NB];
+    int32_t ks[NB];
+    int32_t t;
+    int32_t nn;
+};
+
+// A hub row, by a whole warp: the lanes take 32 edges at a time -- schedule
+// step, tail and first NB negative samples gathered into shared memory, all
+// in parallel -- and lane 0 then applies the chunk's firing edges in order.
+// Lane 0 keeps the head; it re-reads it once per firing edge (the value
+// arrives while the previous edge is computed) and publishes each edge's move.
+template <int NB>
+__device__ __forceinline__ void hub_row(int32_t h, const RowArgs<float>& r, float2* __restrict__ Y,
+                                        const SgdParams<float>& p, HubEvent<NB>* __restrict__ ev,
+                                        unsigned long long& fired, unsigned long long& drawn) {
+    const int lane = threadIdx.x & 31;
+    const float ef = p.epoch;
+    const int64_t j0 = r.ptr[h], r1 = r.ptr[h + 1];
+    int32_t nbase;
+    uint32_t nsize;
+    instance_range(h, p, nbase, nsize);
+    float hx = 0.0f, hy = 0.0f;     // lane 0: the head
+    float2 seen = make_float2(0.0f, 0.0f);   // lane 0: the head as last read
+    bool have = false;
+    for (int64_t c = j0; c < r1; c += 32) {
+        const int64_t j = c + lane;
+        bool fire = false;
+        if (j < r1) {
+            const float en = r.enext[j];
+            fire = en <= ef;
+            if (fire) {
+                const float ep = r.eps[j], enn = r.enneg[j];
+                const int32_t t = r.targets[j];
+                const float epns = ep / p.rate;
+                const int nn = static_cast<int>((ef - enn) / epns);
+                r.enext[j] = en + ep;
+                r.enneg[j] = enn + static_cast<float>(nn) * epns;
+                const int draws = nn > 0 ? nn : 0;
+                ++fired;
+                drawn += draws;
+                HubEvent<NB>& e = ev[lane];
+                e.t = t;
+                e.nn = draws;
+                e.yt = __ldcg(&Y[t]);
+                NegStream rng(static_cast<uint32_t>(h), static_cast<uint32_t>(t), p.epoch_u, p.k0, p.k1);
+                const int m = draws < NB ? draws : NB;
+#pragma unroll
+                for (int b = 0; b < NB; ++b) {
+                    if (b < m) {
+                        const int32_t k = nbase + rng.bounded(nsize);
+                        e.ks[b] = k;
+                        e.yk[b] = __ldcg(&Y[k]);
+                    }
+                }
+            }
+        }
+        unsigned mask = __ballot_sync(0xffffffffu, fire);
+        __syncwarp();
+        if (lane == 0) {
+            while (mask) {
+                const int q = __ffs(mask) - 1;
+                mask &= mask - 1;
+                const HubEvent<NB>& e = ev[q];
+                if (!have) {
+                    seen = ld_relaxed_f2(&Y[h]);
+                    hx = seen.x;
+                    hy = seen.y;
+                    have = true;
+                }
+                const float2 next_seen = ld_relaxed_f2(&Y[h]);   // for the next edge (others' pulls so far)
+                const float sx = hx, sy = hy;
+                {
+                    const float dx = hx - e.yt.x, dy = hy - e.yt.y;
+                    const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
+                    const float cf = attract_coef_fast(d2, p);
+                    const float gx = p.alpha * clamp4(cf * dx);
+                    const float gy = p.alpha * clamp4(cf * dy);
+                    hx += gx;
+                    hy += gy;
+                    atomicAdd(&Y[e.t], make_float2(-gx, -gy));
+                }
+                const int nn = e.nn;
+                const int m = nn < NB ? nn : NB;
+#pragma unroll
+                for (int b = 0; b < NB; ++b) {
+                    if (b < m && e.ks[b] != h) {
+                        const float dx = hx - e.yk[b].x, dy = hy - e.yk[b].y;
+                        const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
+                        const float cf = repulse_coef_fast(d2, p);
+                        hx = __fmaf_rn(p.alpha, clamp4(cf * dx), hx);
+                        hy = __fmaf_rn(p.alpha, clamp4(cf * dy), hy);
+                    }
+                }
+                if (nn > NB) {   // rare: the rest of this edge's negative samples, from the same stream
+                    NegStream rng(static_cast<uint32_t>(h), static_cast<uint32_t>(e.t), p.epoch_u, p.k0, p.k1);
+                    for (int b = 0; b < nn; ++b) {
+                        const int32_t k = nbase + rng.bounded(nsize);
+                        if (b < NB || k == h) continue;
+                        const float2 y = __ldcg(&Y[k]);
+                        const float dx = hx - y.x, dy = hy - y.y;
+                        const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
+                        const float cf = repulse_coef_fast(d2, p);
+                        hx = __fmaf_rn(p.alpha, clamp4(cf * dx), hx);
+                        hy = __fmaf_rn(p.alpha, clamp4(cf * dy), hy);
+                    }
+                }
+                const float mx = hx - sx, my = hy - sy;
+                atomicAdd(&Y[h], make_float2(mx, my));
+                // the next edge starts from the head as read above (which
+                // includes this lane's earlier publications) plus this move
+                hx = next_seen.x + mx;
+                hy = next_seen.y + my;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+template <int NB, int MINB>
 __global__ void __launch_bounds__(256, MINB) sgd_rows_2d_f32(RowArgs<float> r, float2* __restrict__ Y,
                                                              SgdParams<float> p) {
+    __shared__ HubEvent<NB> hub_ev[256 / 32][32];
     unsigned long long fired = 0, drawn = 0;
-    const float ef = p.epoch;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int32_t nbulk_units = (r.nrows - r.nhub + 31) / 32;
+    const int32_t units = r.nhub + nbulk_units;
     while (true) {
-        const int32_t base = claim_rows(r.counter);
-        if (base >= r.nrows) break;
-        const int32_t i = base + (threadIdx.x & 31);
-        if (i < r.nrows) {
-            const int32_t h = r.order[i];
-            const int64_t r1 = r.ptr[h + 1];
-            int64_t j = next_firing(r.enext, r.ptr[h], r1, ef);
-            if (j < r1) {
-                int32_t nbase;
-                uint32_t nsize;
-                instance_range(h, p, nbase, nsize);
-                float hx, hy;
-                if (!FRESH) {
-                    const float2 y0 = __ldcg(&Y[h]);
-                    hx = y0.x;
-                    hy = y0.y;
-                }
-                // the current firing edge: target, schedule state
-                int32_t t = r.targets[j];
-                float ep = r.eps[j], en = r.enext[j], enn = r.enneg[j];
-                float px = 0.0f, py = 0.0f;   // head as last published
-                int since = 0;
-                bool first = true;
-                do {
-                    // gathers of this edge: head, tail, first batch of negatives
-                    float2 yh;
-                    if (FRESH) yh = ld_relaxed_f2(&Y[h]);
-                    const float2 yt = __ldcg(&Y[t]);
-                    const float epns = ep / p.rate;   // optimize_layout.hpp:160-161
-                    const int nn = static_cast<int>((ef - enn) / epns);
-                    int remaining = nn > 0 ? nn : 0;   // a negative count draws nothing, as in the reference's loop
-                    NegStream rng(static_cast<uint32_t>(h), static_cast<uint32_t>(t), p.epoch_u, p.k0, p.k1);
-                    int m = remaining < NB ? remaining : NB;
-                    int32_t ks[NB];
-                    float2 yk[NB];
-#pragma unroll
-                    for (int q = 0; q < NB; ++q) {
-                        if (q < m) {
-                            ks[q] = nbase + rng.bounded(nsize);
-                            yk[q] = __ldcg(&Y[ks[q]]);
-                        }
-                    }
-                    // the schedule step (:178-179) and the next firing edge, while the gathers fly
-                    r.enext[j] = en + ep;
-                    r.enneg[j] = enn + static_cast<float>(nn) * epns;
-                    ++fired;
-                    drawn += remaining;
-                    const int64_t j2 = next_firing(r.enext, j + 1, r1, ef);
-                    int32_t t2 = 0;
-                    float ep2 = 0.0f, en2 = 0.0f, enn2 = 0.0f;
-                    if (j2 < r1) {
-                        t2 = r.targets[j2];
-                        ep2 = r.eps[j2];
-                        en2 = r.enext[j2];
-                        enn2 = r.enneg[j2];
-                    }
-                    if (FRESH) {
-                        hx = yh.x;
-                        hy = yh.y;
-                    }
-                    if (first || FRESH) {
-                        px = hx;
-                        py = hy;
-                        first = false;
-                    }
-                    {   // attractive step (:145-155)
-                        const float dx = hx - yt.x, dy = hy - yt.y;
-                        const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
-                        const float cf = attract_coef_fast(d2, p);
-                        const float gx = p.alpha * clamp4(cf * dx);
-                        const float gy = p.alpha * clamp4(cf * dy);
-                        hx += gx;
-                        hy += gy;
-                        atomicAdd(&Y[t], make_float2(-gx, -gy));
-                    }
-                    while (true) {   // negative samples (:157-176)
-#pragma unroll
-                        for (int q = 0; q < NB; ++q) {
-                            if (q < m && ks[q] != h) {
-                                const float dx = hx - yk[q].x, dy = hy - yk[q].y;
-                                const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
-                                const float cf = repulse_coef_fast(d2, p);
-                                hx = __fmaf_rn(p.alpha, clamp4(cf * dx), hx);
-                                hy = __fmaf_rn(p.alpha, clamp4(cf * dy), hy);
-                            }
-                        }
-                        remaining -= m;
-                        if (remaining <= 0) break;
-                        m = remaining < NB ? remaining : NB;
-#pragma unroll
-                        for (int q = 0; q < NB; ++q) {
-                            if (q < m) {
-                                ks[q] = nbase + rng.bounded(nsize);
-                                yk[q] = __ldcg(&Y[ks[q]]);
-                            }
-                        }
-                    }
-                    j = j2;
-                    if (FRESH || ++since >= p.publish_every || j >= r1) {
-                        atomicAdd(&Y[h], make_float2(hx - px, hy - py));
-                        px = hx;
-                        py = hy;
-                        since = 0;
-                    }
-                    t = t2;
-                    ep = ep2;
-                    en = en2;
-                    enn = enn2;
-                } while (j < r1);
-            }
+        int32_t u = 0;
+        if (lane == 0) u = atomicAdd(r.counter, 1);
+        u = __shfl_sync(0xffffffffu, u, 0);
+        if (u >= units) break;
+        if (u < r.nhub) {
+            hub_row<NB>(r.order[u], r, Y, p, hub_ev[warp], fired, drawn);
+        } else {
+            const int32_t i = r.nhub + (u - r.nhub) * 32 + lane;
+            if (i < r.nrows) bulk_row<NB>(r.order[i], r, Y, p, fired, drawn);
         }
         __syncwarp();
     }
@@ -428,10 +566,10 @@ struct Sgd2dVariant {
     int neg_batch, min_blocks;
 };
 const Sgd2dVariant SGD_2D_VARIANTS[] = {
-    {sgd_rows_2d_f32<8, 4, true>, 8, 4},     // default
-    {sgd_rows_2d_f32<8, 2, true>, 8, 2},
-    {sgd_rows_2d_f32<6, 5, true>, 6, 5},
-    {sgd_rows_2d_f32<8, 4, false>, 8, 4},    // head kept in registers, published every publish_every edges
+    {sgd_rows_2d_f32<8, 3>, 8, 3},     // default
+    {sgd_rows_2d_f32<8, 2>, 8, 2},
+    {sgd_rows_2d_f32<6, 4>, 6, 4},
+    {sgd_rows_2d_f32<8, 4>, 8, 4},
 };
 constexpr int NUM_SGD_2D_VARIANTS = sizeof(SGD_2D_VARIANTS) / sizeof(SGD_2D_VARIANTS[0]);
 
@@ -584,6 +722,18 @@ void SgdEngine<T>::setup(const DeviceEpochs<T>* ep, cudaStream_t s, int base_epo
         DevArray<unsigned char> temp(tb, s);
         UMAPB_CUDA(cub::DeviceRadixSort::SortPairsDescending(temp.get(), tb, key.get(), key_sorted.get(), row.get(),
                                                              order_.get(), n, 0, 32, s));
+        // hub rows (expected to fire at least HUB_RATE edges per epoch) lead the order
+        DevArray<int> cnt(1, s);
+        cnt.zero(s);
+        const float thr = static_cast<float>(HUB_RATE);
+        uint32_t thr_bits;
+        std::memcpy(&thr_bits, &thr, sizeof(thr_bits));
+        count_at_least_kernel<<<grid_for(n, 256, 1024), 256, 0, s>>>(n, key_sorted.get(), thr_bits, cnt.get());
+        UMAPB_LAUNCH_CHECK();
+        UMAPB_CUDA(cudaMemcpyAsync(&nhub_, cnt.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        UMAPB_SYNC(s);
+    } else {
+        nhub_ = 0;
     }
 }
 
@@ -697,6 +847,7 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
         r.enneg = enn;
         r.counter = counter;
         r.totals = totals;
+        r.nhub = use_2d ? nhub_ : 0;
         if (use_2d) {
             if constexpr (std::is_same<T, float>::value) {
                 unsigned g = static_cast<unsigned>(sm_count() * sgd_2d_resident(variant, block));

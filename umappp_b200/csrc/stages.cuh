@@ -186,6 +186,7 @@ private:
     int base_epoch_ = 0;
     DevArray<T> enext_, enneg_;    // schedule state at state_epoch_
     DevArray<int32_t> order_;      // rows by descending firing rate
+    int nhub_ = 0;                 // leading rows of order_ taken by a whole warp (2-d kernel)
     int state_epoch_ = 0;          // epoch the state arrays describe
 };
 
