@@ -119,15 +119,21 @@ __global__ void __launch_bounds__(SCHED_BLOCK) sched_totals_kernel(int64_t nnz, 
 
 // ------------------------------------------------------------ row order --
 
-// Firing rate of each row: sum of 1 / epochs_per_sample over its edges (the
-// expected number of firing edges per epoch), as an order-preserving key.
+// Hub rows: expected to fire at least HUB_RATE edges per epoch.
+constexpr int HUB_RATE = 32;
+
+// Order key of each row: its firing rate (sum of 1 / epochs_per_sample over
+// its edges, the expected number of firing edges per epoch) for hub rows, 0
+// for the others, as an order-preserving integer; a stable descending sort
+// then puts the hubs first, heaviest first, and keeps the other rows in index
+// order.
 template <typename T>
 __global__ void row_rate_kernel(int32_t n, const int64_t* __restrict__ ptr, const T* __restrict__ eps,
                                 uint32_t* __restrict__ key, int32_t* __restrict__ row) {
     for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float r = 0.0f;
         for (int64_t j = ptr[i]; j < ptr[i + 1]; ++j) r += 1.0f / static_cast<float>(eps[j]);
-        key[i] = __float_as_uint(r);   // r >= 0: the bit pattern orders as the value
+        key[i] = r >= static_cast<float>(HUB_RATE) ? __float_as_uint(r) : 0u;   // r >= 0: bits order as values
         row[i] = i;
     }
 }
@@ -304,18 +310,69 @@ __device__ __forceinline__ float2 ld_relaxed_f2(const float2* q) {
 }
 
 // 2-d FP32 rows.  Work units, claimed by warps in order: first the hub rows
-// (expected to fire at least HUB_RATE edges per epoch; one row per warp),
-// then the other rows, 32 per warp (one per lane).
-constexpr int HUB_RATE = 32;
+// (one row per warp), then the other rows, 32 per warp (one per lane).
 constexpr int BULK_CHUNK = 8;    // edges of a row whose schedule state a lane loads at once
 
-// A lane's row.  Its schedule state is read BULK_CHUNK edges at a time, the
-// next chunk's loads in flight while the current chunk's firing edges are
-// processed.  Per firing edge the head (re-read: it sees the pulls of other
-// rows' attractive steps), the tail and the first NB negative samples are
-// gathered together -- the negative-sample indices do not depend on the
-// layout -- and the updates are then applied in the reference's order; the
-// head's move is published after each firing edge.
+// Value q of an 8-entry register window.
+__device__ __forceinline__ float pick8(const float (&w)[BULK_CHUNK], int q) {
+    float v = w[0];
+#pragma unroll
+    for (int k = 1; k < BULK_CHUNK; ++k) v = (q == k) ? w[k] : v;
+    return v;
+}
+
+// A row's schedule state, read BULK_CHUNK edges at a time into registers
+// (the next window's loads in flight while the current one is used), and the
+// row's firing edges found in it in order.
+struct RowScan {
+    int64_t cb, nb, r1;        // current window's first edge, next window's first edge, row end
+    float cw[BULK_CHUNK], nw[BULK_CHUNK];
+    unsigned cm;               // firing edges of the current window not yet taken
+    __device__ __forceinline__ void load(float (&w)[BULK_CHUNK], const float* __restrict__ enext, int64_t b) {
+#pragma unroll
+        for (int q = 0; q < BULK_CHUNK; ++q) w[q] = (b + q < r1) ? enext[b + q] : CUDART_INF_F;
+    }
+    __device__ __forceinline__ unsigned fire_mask(const float (&w)[BULK_CHUNK], float ef) {
+        unsigned m = 0;
+#pragma unroll
+        for (int q = 0; q < BULK_CHUNK; ++q) m |= (w[q] <= ef ? 1u : 0u) << q;
+        return m;
+    }
+    __device__ __forceinline__ void start(const float* __restrict__ enext, int64_t j0, int64_t end, float ef) {
+        r1 = end;
+        cb = j0;
+        nb = j0 + BULK_CHUNK;
+        load(cw, enext, cb);
+        load(nw, enext, nb);
+        cm = fire_mask(cw, ef);
+    }
+    // Next firing edge (false: none left); en = its epoch_of_next_sample.
+    __device__ __forceinline__ bool next(const float* __restrict__ enext, float ef, int64_t& j, float& en) {
+        while (cm == 0) {
+            if (nb >= r1) return false;
+            cb = nb;
+#pragma unroll
+            for (int q = 0; q < BULK_CHUNK; ++q) cw[q] = nw[q];
+            nb += BULK_CHUNK;
+            load(nw, enext, nb);
+            cm = fire_mask(cw, ef);
+        }
+        const int q = __ffs(cm) - 1;
+        cm &= cm - 1;
+        j = cb + q;
+        en = pick8(cw, q);
+        return true;
+    }
+};
+
+// A lane's row.  Per firing edge the head (re-read: it sees the pulls of
+// other rows' attractive steps), the tail and the first NB negative samples
+// are gathered together -- the negative-sample indices do not depend on the
+// layout; while they are in flight the schedule step is written and the
+// row's next firing edge found and its target and state loaded; then the
+// updates are applied in the reference's order and the head's move is
+// published.  Every lane of a warp works on its own row's next firing edge
+// in the same iteration.
 template <int NB>
 __device__ __forceinline__ void bulk_row(int32_t h, const RowArgs<float>& r, float2* __restrict__ Y,
                                          const SgdParams<float>& p, unsigned long long& fired,
@@ -323,95 +380,87 @@ __device__ __forceinline__ void bulk_row(int32_t h, const RowArgs<float>& r, flo
     const float ef = p.epoch;
     const int64_t j0 = r.ptr[h], r1 = r.ptr[h + 1];
     if (j0 >= r1) return;
+    RowScan sc;
+    sc.start(r.enext, j0, r1, ef);
+    int64_t j;
+    float en;
+    if (!sc.next(r.enext, ef, j, en)) return;
     int32_t nbase;
     uint32_t nsize;
     instance_range(h, p, nbase, nsize);
-    float en[BULK_CHUNK];
+    int32_t t = r.targets[j];
+    float ep = r.eps[j], enn = r.enneg[j];
+    while (true) {
+        const float2 yh = ld_relaxed_f2(&Y[h]);
+        const float2 yt = __ldcg(&Y[t]);
+        const float epns = ep / p.rate;   // optimize_layout.hpp:160-161
+        const int nn = static_cast<int>((ef - enn) / epns);
+        int remaining = nn > 0 ? nn : 0;   // a negative count draws nothing, as in the reference's loop
+        NegStream rng(static_cast<uint32_t>(h), static_cast<uint32_t>(t), p.epoch_u, p.k0, p.k1);
+        int m = remaining < NB ? remaining : NB;
+        int32_t ks[NB];
+        float2 yk[NB];
 #pragma unroll
-    for (int q = 0; q < BULK_CHUNK; ++q) en[q] = (j0 + q < r1) ? r.enext[j0 + q] : CUDART_INF_F;
-    for (int64_t c = j0; c < r1; c += BULK_CHUNK) {
-        float en_next[BULK_CHUNK];
-#pragma unroll
-        for (int q = 0; q < BULK_CHUNK; ++q) {
-            const int64_t jn = c + BULK_CHUNK + q;
-            en_next[q] = (jn < r1) ? r.enext[jn] : CUDART_INF_F;
-        }
-        unsigned mask = 0;
-#pragma unroll
-        for (int q = 0; q < BULK_CHUNK; ++q) mask |= (en[q] <= ef ? 1u : 0u) << q;
-        if (mask) {
-            int32_t tq[BULK_CHUNK];
-            float epq[BULK_CHUNK], ennq[BULK_CHUNK];
-#pragma unroll
-            for (int q = 0; q < BULK_CHUNK; ++q) {
-                if (mask & (1u << q)) {
-                    tq[q] = r.targets[c + q];
-                    epq[q] = r.eps[c + q];
-                    ennq[q] = r.enneg[c + q];
-                }
+        for (int b = 0; b < NB; ++b) {
+            if (b < m) {
+                ks[b] = nbase + rng.bounded(nsize);
+                yk[b] = __ldcg(&Y[ks[b]]);
             }
+        }
+        r.enext[j] = en + ep;                          // :178-179
+        r.enneg[j] = enn + static_cast<float>(nn) * epns;
+        ++fired;
+        drawn += remaining;
+        int64_t j2;
+        float en2;
+        const bool more = sc.next(r.enext, ef, j2, en2);
+        int32_t t2 = 0;
+        float ep2 = 0.0f, enn2 = 0.0f;
+        if (more) {
+            t2 = r.targets[j2];
+            ep2 = r.eps[j2];
+            enn2 = r.enneg[j2];
+        }
+        float hx = yh.x, hy = yh.y;
+        {   // attractive step (:145-155)
+            const float dx = hx - yt.x, dy = hy - yt.y;
+            const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
+            const float cf = attract_coef_fast(d2, p);
+            const float gx = p.alpha * clamp4(cf * dx);
+            const float gy = p.alpha * clamp4(cf * dy);
+            hx += gx;
+            hy += gy;
+            atomicAdd(&Y[t], make_float2(-gx, -gy));
+        }
+        while (true) {   // negative samples (:157-176)
 #pragma unroll
-            for (int q = 0; q < BULK_CHUNK; ++q) {
-                if (!(mask & (1u << q))) continue;
-                const int32_t t = tq[q];
-                const float epns = epq[q] / p.rate;   // optimize_layout.hpp:160-161
-                const int nn = static_cast<int>((ef - ennq[q]) / epns);
-                r.enext[c + q] = en[q] + epq[q];       // :178-179
-                r.enneg[c + q] = ennq[q] + static_cast<float>(nn) * epns;
-                int remaining = nn > 0 ? nn : 0;       // a negative count draws nothing, as in the reference's loop
-                ++fired;
-                drawn += remaining;
-                const float2 yh = ld_relaxed_f2(&Y[h]);
-                const float2 yt = __ldcg(&Y[t]);
-                NegStream rng(static_cast<uint32_t>(h), static_cast<uint32_t>(t), p.epoch_u, p.k0, p.k1);
-                int m = remaining < NB ? remaining : NB;
-                int32_t ks[NB];
-                float2 yk[NB];
-#pragma unroll
-                for (int b = 0; b < NB; ++b) {
-                    if (b < m) {
-                        ks[b] = nbase + rng.bounded(nsize);
-                        yk[b] = __ldcg(&Y[ks[b]]);
-                    }
-                }
-                float hx = yh.x, hy = yh.y;
-                {   // attractive step (:145-155)
-                    const float dx = hx - yt.x, dy = hy - yt.y;
+            for (int b = 0; b < NB; ++b) {
+                if (b < m && ks[b] != h) {
+                    const float dx = hx - yk[b].x, dy = hy - yk[b].y;
                     const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
-                    const float cf = attract_coef_fast(d2, p);
-                    const float gx = p.alpha * clamp4(cf * dx);
-                    const float gy = p.alpha * clamp4(cf * dy);
-                    hx += gx;
-                    hy += gy;
-                    atomicAdd(&Y[t], make_float2(-gx, -gy));
+                    const float cf = repulse_coef_fast(d2, p);
+                    hx = __fmaf_rn(p.alpha, clamp4(cf * dx), hx);
+                    hy = __fmaf_rn(p.alpha, clamp4(cf * dy), hy);
                 }
-                while (true) {   // negative samples (:157-176)
+            }
+            remaining -= m;
+            if (remaining <= 0) break;
+            m = remaining < NB ? remaining : NB;
 #pragma unroll
-                    for (int b = 0; b < NB; ++b) {
-                        if (b < m && ks[b] != h) {
-                            const float dx = hx - yk[b].x, dy = hy - yk[b].y;
-                            const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
-                            const float cf = repulse_coef_fast(d2, p);
-                            hx = __fmaf_rn(p.alpha, clamp4(cf * dx), hx);
-                            hy = __fmaf_rn(p.alpha, clamp4(cf * dy), hy);
-                        }
-                    }
-                    remaining -= m;
-                    if (remaining <= 0) break;
-                    m = remaining < NB ? remaining : NB;
-#pragma unroll
-                    for (int b = 0; b < NB; ++b) {
-                        if (b < m) {
-                            ks[b] = nbase + rng.bounded(nsize);
-                            yk[b] = __ldcg(&Y[ks[b]]);
-                        }
-                    }
+            for (int b = 0; b < NB; ++b) {
+                if (b < m) {
+                    ks[b] = nbase + rng.bounded(nsize);
+                    yk[b] = __ldcg(&Y[ks[b]]);
                 }
-                atomicAdd(&Y[h], make_float2(hx - yh.x, hy - yh.y));
             }
         }
-#pragma unroll
-        for (int q = 0; q < BULK_CHUNK; ++q) en[q] = en_next[q];
+        atomicAdd(&Y[h], make_float2(hx - yh.x, hy - yh.y));
+        if (!more) break;
+        j = j2;
+        en = en2;
+        t = t2;
+        ep = ep2;
+        enn = enn2;
     }
 }
 
@@ -427,9 +476,8 @@ struct HubEvent {
 
 // A hub row, by a whole warp: the lanes take 32 edges at a time -- schedule
 // step, tail and first NB negative samples gathered into shared memory, all
-// in parallel -- and lane 0 then applies the chunk's firing edges in order.
-// Lane 0 keeps the head; it re-reads it once per firing edge (the value
-// arrives while the previous edge is computed) and publishes each edge's move.
+// in parallel -- and lane 0 then applies the chunk's firing edges in order,
+// keeping the head in registers and publishing its move after each edge.
 template <int NB>
 __device__ __forceinline__ void hub_row(int32_t h, const RowArgs<float>& r, float2* __restrict__ Y,
                                         const SgdParams<float>& p, HubEvent<NB>* __restrict__ ev,
@@ -440,8 +488,7 @@ __device__ __forceinline__ void hub_row(int32_t h, const RowArgs<float>& r, floa
     int32_t nbase;
     uint32_t nsize;
     instance_range(h, p, nbase, nsize);
-    float hx = 0.0f, hy = 0.0f;     // lane 0: the head
-    float2 seen = make_float2(0.0f, 0.0f);   // lane 0: the head as last read
+    float hx = 0.0f, hy = 0.0f;   // lane 0: the head
     bool have = false;
     for (int64_t c = j0; c < r1; c += 32) {
         const int64_t j = c + lane;
@@ -478,17 +525,16 @@ __device__ __forceinline__ void hub_row(int32_t h, const RowArgs<float>& r, floa
         unsigned mask = __ballot_sync(0xffffffffu, fire);
         __syncwarp();
         if (lane == 0) {
+            if (mask && !have) {
+                const float2 y0 = ld_relaxed_f2(&Y[h]);
+                hx = y0.x;
+                hy = y0.y;
+                have = true;
+            }
             while (mask) {
                 const int q = __ffs(mask) - 1;
                 mask &= mask - 1;
                 const HubEvent<NB>& e = ev[q];
-                if (!have) {
-                    seen = ld_relaxed_f2(&Y[h]);
-                    hx = seen.x;
-                    hy = seen.y;
-                    have = true;
-                }
-                const float2 next_seen = ld_relaxed_f2(&Y[h]);   // for the next edge (others' pulls so far)
                 const float sx = hx, sy = hy;
                 {
                     const float dx = hx - e.yt.x, dy = hy - e.yt.y;
@@ -525,12 +571,7 @@ __device__ __forceinline__ void hub_row(int32_t h, const RowArgs<float>& r, floa
                         hy = __fmaf_rn(p.alpha, clamp4(cf * dy), hy);
                     }
                 }
-                const float mx = hx - sx, my = hy - sy;
-                atomicAdd(&Y[h], make_float2(mx, my));
-                // the next edge starts from the head as read above (which
-                // includes this lane's earlier publications) plus this move
-                hx = next_seen.x + mx;
-                hy = next_seen.y + my;
+                atomicAdd(&Y[h], make_float2(hx - sx, hy - sy));
             }
         }
         __syncwarp();
@@ -826,8 +867,14 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
     const bool use_2d = std::is_same<T, float>::value && num_dim == 2;
     const bool check = check_schedule();
     cudaStream_t s = caller;
-    int max_blocks = 0;   // UMAPB_SGD_MAX_BLOCKS: cap on the blocks of an epoch launch (0: all resident)
+    // Rows in flight at once: at most n / window_div (a sliding window over
+    // the claim order), so that few rows run beside their neighbours with
+    // positions read before those neighbours' updates; at a million points
+    // that is still enough rows to keep L2 saturated.
+    // UMAPB_SGD_MAX_BLOCKS overrides the block count (0: from the window).
+    int max_blocks = 0;
     if (const char* e = std::getenv("UMAPB_SGD_MAX_BLOCKS")) max_blocks = std::max(0, std::atoi(e));
+    const int64_t window_rows = window_div > 0 ? std::max<int64_t>(1, ep_->n / window_div) : int64_t(1) << 40;
 
     // One epoch launch on (Yp, schedule state en/enn), claiming rows from 'counter'.
     auto launch = [&](T* Yp, T* en, T* enn, int* counter, unsigned long long* totals, int e_abs, int block,
@@ -850,13 +897,17 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
         r.nhub = use_2d ? nhub_ : 0;
         if (use_2d) {
             if constexpr (std::is_same<T, float>::value) {
-                unsigned g = static_cast<unsigned>(sm_count() * sgd_2d_resident(variant, block));
-                if (max_blocks > 0) g = std::min<unsigned>(g, static_cast<unsigned>(max_blocks));
-                SGD_2D_VARIANTS[variant].kernel<<<g, block, 0, s>>>(r, reinterpret_cast<float2*>(Yp), p);
+                int64_t g = static_cast<int64_t>(sm_count()) * sgd_2d_resident(variant, block);
+                g = std::min<int64_t>(g, std::max<int64_t>(1, (window_rows + block - 1) / block));
+                if (max_blocks > 0) g = std::min<int64_t>(g, max_blocks);
+                SGD_2D_VARIANTS[variant].kernel<<<static_cast<unsigned>(g), block, 0, s>>>(
+                    r, reinterpret_cast<float2*>(Yp), p);
             }
         } else {
-            const unsigned g = static_cast<unsigned>(sm_count() * generic_resident());
-            sgd_rows_generic<T><<<g, 128, 0, s>>>(r, Yp, num_dim, p);
+            int64_t g = static_cast<int64_t>(sm_count()) * generic_resident();
+            g = std::min<int64_t>(g, std::max<int64_t>(1, (window_rows + 127) / 128));
+            if (max_blocks > 0) g = std::min<int64_t>(g, max_blocks);
+            sgd_rows_generic<T><<<static_cast<unsigned>(g), 128, 0, s>>>(r, Yp, num_dim, p);
         }
         UMAPB_LAUNCH_CHECK();
     };
@@ -958,6 +1009,14 @@ int SgdEngine<T>::default_variant() {
     const char* e = std::getenv("UMAPB_SGD_VARIANT");
     const int x = e ? std::atoi(e) : -1;
     return (x >= 0 && x < NUM_SGD_2D_VARIANTS) ? x : 0;
+}
+
+// UMAPB_SGD_WINDOW_DIV: rows in flight at most n / this (default 16; 0: no cap).
+template <typename T>
+int SgdEngine<T>::default_window_div() {
+    const char* e = std::getenv("UMAPB_SGD_WINDOW_DIV");
+    const int x = e ? std::atoi(e) : -1;
+    return (x >= 0 && x <= 1 << 20) ? x : 16;
 }
 
 // UMAPB_SGD_PUBLISH_EVERY: firing edges between publications of a row's head

@@ -171,6 +171,8 @@ public:
     bool autotune = false;
     // Firing edges between publications of a row's head (sgd.cu).
     int publish_every = default_publish_every();
+    // Rows in flight at most n / window_div (sgd.cu, run(); 0: no cap).
+    int window_div = default_window_div();
     int block_size() const { return block_; }
     int variant() const { return variant_; }   // 2-d kernel variant (sgd.cu, SGD_2D_VARIANTS)
 
@@ -179,6 +181,7 @@ private:
     void tune(T* Y, int num_dim, int epoch, Launch& launch, cudaStream_t s);
     static int default_variant();
     static int default_publish_every();
+    static int default_window_div();
     int block_ = 256, variant_ = default_variant();
     const DeviceEpochs<T>* ep_ = nullptr;
     const int32_t* inst_start_ = nullptr;
