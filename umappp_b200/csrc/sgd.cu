@@ -128,12 +128,12 @@ constexpr int HUB_RATE = 32;
 // then puts the hubs first, heaviest first, and keeps the other rows in index
 // order.
 template <typename T>
-__global__ void row_rate_kernel(int32_t n, const int64_t* __restrict__ ptr, const T* __restrict__ eps,
+__global__ void row_rate_kernel(int32_t n, const int64_t* __restrict__ ptr, const T* __restrict__ eps, float hub_rate,
                                 uint32_t* __restrict__ key, int32_t* __restrict__ row) {
     for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float r = 0.0f;
         for (int64_t j = ptr[i]; j < ptr[i + 1]; ++j) r += 1.0f / static_cast<float>(eps[j]);
-        key[i] = r >= static_cast<float>(HUB_RATE) ? __float_as_uint(r) : 0u;   // r >= 0: bits order as values
+        key[i] = r >= hub_rate ? __float_as_uint(r) : 0u;   // r >= 0: bits order as values
         row[i] = i;
     }
 }
@@ -755,7 +755,10 @@ void SgdEngine<T>::setup(const DeviceEpochs<T>* ep, cudaStream_t s, int base_epo
     if (n > 0) {
         DevArray<uint32_t> key(n, s), key_sorted(n, s);
         DevArray<int32_t> row(n, s);
-        row_rate_kernel<T><<<grid_for(n, 256), 256, 0, s>>>(n, ep->ptr.get(), ep->eps.get(), key.get(), row.get());
+        float hub_rate = static_cast<float>(HUB_RATE);   // UMAPB_SGD_HUB_RATE overrides it
+        if (const char* e = std::getenv("UMAPB_SGD_HUB_RATE")) hub_rate = static_cast<float>(std::atof(e));
+        row_rate_kernel<T><<<grid_for(n, 256), 256, 0, s>>>(n, ep->ptr.get(), ep->eps.get(), hub_rate, key.get(),
+                                                           row.get());
         UMAPB_LAUNCH_CHECK();
         size_t tb = 0;
         UMAPB_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, key.get(), key_sorted.get(), row.get(),
@@ -766,9 +769,9 @@ void SgdEngine<T>::setup(const DeviceEpochs<T>* ep, cudaStream_t s, int base_epo
         // hub rows (expected to fire at least HUB_RATE edges per epoch) lead the order
         DevArray<int> cnt(1, s);
         cnt.zero(s);
-        const float thr = static_cast<float>(HUB_RATE);
         uint32_t thr_bits;
-        std::memcpy(&thr_bits, &thr, sizeof(thr_bits));
+        std::memcpy(&thr_bits, &hub_rate, sizeof(thr_bits));
+        if (hub_rate <= 0.0f) thr_bits = 1u;   // every row with a non-zero rate
         count_at_least_kernel<<<grid_for(n, 256, 1024), 256, 0, s>>>(n, key_sorted.get(), thr_bits, cnt.get());
         UMAPB_LAUNCH_CHECK();
         UMAPB_CUDA(cudaMemcpyAsync(&nhub_, cnt.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
