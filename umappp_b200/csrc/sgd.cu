@@ -129,11 +129,11 @@ constexpr int HUB_RATE = 32;
 // order.
 template <typename T>
 __global__ void row_rate_kernel(int32_t n, const int64_t* __restrict__ ptr, const T* __restrict__ eps, float hub_rate,
-                                uint32_t* __restrict__ key, int32_t* __restrict__ row) {
+                                int all_by_rate, uint32_t* __restrict__ key, int32_t* __restrict__ row) {
     for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float r = 0.0f;
         for (int64_t j = ptr[i]; j < ptr[i + 1]; ++j) r += 1.0f / static_cast<float>(eps[j]);
-        key[i] = r >= hub_rate ? __float_as_uint(r) : 0u;   // r >= 0: bits order as values
+        key[i] = (all_by_rate || r >= hub_rate) ? __float_as_uint(r) : 0u;   // r >= 0: bits order as values
         row[i] = i;
     }
 }
@@ -757,8 +757,11 @@ void SgdEngine<T>::setup(const DeviceEpochs<T>* ep, cudaStream_t s, int base_epo
         DevArray<int32_t> row(n, s);
         float hub_rate = static_cast<float>(HUB_RATE);   // UMAPB_SGD_HUB_RATE overrides it
         if (const char* e = std::getenv("UMAPB_SGD_HUB_RATE")) hub_rate = static_cast<float>(std::atof(e));
-        row_rate_kernel<T><<<grid_for(n, 256), 256, 0, s>>>(n, ep->ptr.get(), ep->eps.get(), hub_rate, key.get(),
-                                                           row.get());
+        // UMAPB_SGD_ORDER=1: every row by rate (0: hub rows by rate, then the others in index order)
+        const char* oe = std::getenv("UMAPB_SGD_ORDER");
+        const int all_by_rate = (oe && std::atoi(oe) == 1) ? 1 : 0;
+        row_rate_kernel<T><<<grid_for(n, 256), 256, 0, s>>>(n, ep->ptr.get(), ep->eps.get(), hub_rate, all_by_rate,
+                                                           key.get(), row.get());
         UMAPB_LAUNCH_CHECK();
         size_t tb = 0;
         UMAPB_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, key.get(), key_sorted.get(), row.get(),
@@ -877,7 +880,8 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
     // UMAPB_SGD_MAX_BLOCKS overrides the block count (0: from the window).
     int max_blocks = 0;
     if (const char* e = std::getenv("UMAPB_SGD_MAX_BLOCKS")) max_blocks = std::max(0, std::atoi(e));
-    const int64_t window_rows = window_div > 0 ? std::max<int64_t>(1, ep_->n / window_div) : int64_t(1) << 40;
+    const int64_t window_rows =
+        window_div > 0 ? std::max<int64_t>(ep_->n / window_div, std::min<int64_t>(ep_->n, 32768)) : int64_t(1) << 40;
 
     // One epoch launch on (Yp, schedule state en/enn), claiming rows from 'counter'.
     auto launch = [&](T* Yp, T* en, T* enn, int* counter, unsigned long long* totals, int e_abs, int block,
