@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(SCHED_BLOCK) sched_totals_kernel(int64_t nnz, 
 // ------------------------------------------------------------ row order --
 
 // Hub rows: expected to fire at least HUB_RATE edges per epoch.
-constexpr int HUB_RATE = 32;
+constexpr int HUB_RATE = 128;
 
 // Order key of each row: its firing rate (sum of 1 / epochs_per_sample over
 // its edges, the expected number of firing edges per epoch) for hub rows, 0
@@ -177,7 +177,7 @@ struct RowArgs {
     const T* eps;
     T* enext;
     T* enneg;
-    int* counter;              // work units claimed so far in this epoch
+    int* counter;              // claims so far in this epoch: [0] hub rows (or row groups), [1] other rows
     unsigned long long* totals;   // optional: [firing edges, negative samples drawn] of this epoch
     int32_t nhub;              // 2-d kernel: order[0, nhub) are hub rows, one warp each
 };
@@ -365,103 +365,108 @@ struct RowScan {
     }
 };
 
-// A lane's row.  Per firing edge the head (re-read: it sees the pulls of
+// A lane's current row: its scan, the firing edge at hand (j, its target and
+// schedule state) and its instance's range for negative samples.
+struct LaneRow {
+    int32_t h;       // -1: none
+    int32_t t;
+    int32_t nbase;
+    uint32_t nsize;
+    int64_t j;
+    float en, ep, enn;
+    RowScan sc;
+};
+
+// Starts row h on a lane: false when the row fires no edge this epoch.
+template <typename P>
+__device__ __forceinline__ bool lane_row_start(LaneRow& L, int32_t h, const RowArgs<float>& r, const P& p) {
+    const float ef = p.epoch;
+    const int64_t j0 = r.ptr[h], r1 = r.ptr[h + 1];
+    if (j0 >= r1) return false;
+    L.sc.start(r.enext, j0, r1, ef);
+    if (!L.sc.next(r.enext, ef, L.j, L.en)) return false;
+    L.h = h;
+    L.t = r.targets[L.j];
+    L.ep = r.eps[L.j];
+    L.enn = r.enneg[L.j];
+    instance_range(h, p, L.nbase, L.nsize);
+    return true;
+}
+
+// One firing edge of a lane's row.  The head (re-read: it sees the pulls of
 // other rows' attractive steps), the tail and the first NB negative samples
 // are gathered together -- the negative-sample indices do not depend on the
 // layout; while they are in flight the schedule step is written and the
 // row's next firing edge found and its target and state loaded; then the
 // updates are applied in the reference's order and the head's move is
-// published.  Every lane of a warp works on its own row's next firing edge
-// in the same iteration.
+// published.  Returns false when the row has no firing edge left.
 template <int NB>
-__device__ __forceinline__ void bulk_row(int32_t h, const RowArgs<float>& r, float2* __restrict__ Y,
-                                         const SgdParams<float>& p, unsigned long long& fired,
-                                         unsigned long long& drawn) {
+__device__ __forceinline__ bool lane_row_step(LaneRow& L, const RowArgs<float>& r, float2* __restrict__ Y,
+                                              const SgdParams<float>& p, unsigned long long& fired,
+                                              unsigned long long& drawn) {
     const float ef = p.epoch;
-    const int64_t j0 = r.ptr[h], r1 = r.ptr[h + 1];
-    if (j0 >= r1) return;
-    RowScan sc;
-    sc.start(r.enext, j0, r1, ef);
-    int64_t j;
-    float en;
-    if (!sc.next(r.enext, ef, j, en)) return;
-    int32_t nbase;
-    uint32_t nsize;
-    instance_range(h, p, nbase, nsize);
-    int32_t t = r.targets[j];
-    float ep = r.eps[j], enn = r.enneg[j];
-    while (true) {
-        const float2 yh = ld_relaxed_f2(&Y[h]);
-        const float2 yt = __ldcg(&Y[t]);
-        const float epns = ep / p.rate;   // optimize_layout.hpp:160-161
-        const int nn = static_cast<int>((ef - enn) / epns);
-        int remaining = nn > 0 ? nn : 0;   // a negative count draws nothing, as in the reference's loop
-        NegStream rng(static_cast<uint32_t>(h), static_cast<uint32_t>(t), p.epoch_u, p.k0, p.k1);
-        int m = remaining < NB ? remaining : NB;
-        int32_t ks[NB];
-        float2 yk[NB];
+    const int32_t h = L.h, t = L.t;
+    const float2 yh = ld_relaxed_f2(&Y[h]);
+    const float2 yt = __ldcg(&Y[t]);
+    const float epns = L.ep / p.rate;   // optimize_layout.hpp:160-161
+    const int nn = static_cast<int>((ef - L.enn) / epns);
+    int remaining = nn > 0 ? nn : 0;     // a negative count draws nothing, as in the reference's loop
+    NegStream rng(static_cast<uint32_t>(h), static_cast<uint32_t>(t), p.epoch_u, p.k0, p.k1);
+    int m = remaining < NB ? remaining : NB;
+    int32_t ks[NB];
+    float2 yk[NB];
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+        if (b < m) {
+            ks[b] = L.nbase + rng.bounded(L.nsize);
+            yk[b] = __ldcg(&Y[ks[b]]);
+        }
+    }
+    r.enext[L.j] = L.en + L.ep;                    // :178-179
+    r.enneg[L.j] = L.enn + static_cast<float>(nn) * epns;
+    ++fired;
+    drawn += remaining;
+    const bool more = L.sc.next(r.enext, ef, L.j, L.en);
+    if (more) {
+        L.t = r.targets[L.j];
+        L.ep = r.eps[L.j];
+        L.enn = r.enneg[L.j];
+    }
+    float hx = yh.x, hy = yh.y;
+    {   // attractive step (:145-155)
+        const float dx = hx - yt.x, dy = hy - yt.y;
+        const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
+        const float cf = attract_coef_fast(d2, p);
+        const float gx = p.alpha * clamp4(cf * dx);
+        const float gy = p.alpha * clamp4(cf * dy);
+        hx += gx;
+        hy += gy;
+        atomicAdd(&Y[t], make_float2(-gx, -gy));
+    }
+    while (true) {   // negative samples (:157-176)
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            if (b < m && ks[b] != h) {
+                const float dx = hx - yk[b].x, dy = hy - yk[b].y;
+                const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
+                const float cf = repulse_coef_fast(d2, p);
+                hx = __fmaf_rn(p.alpha, clamp4(cf * dx), hx);
+                hy = __fmaf_rn(p.alpha, clamp4(cf * dy), hy);
+            }
+        }
+        remaining -= m;
+        if (remaining <= 0) break;
+        m = remaining < NB ? remaining : NB;
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
             if (b < m) {
-                ks[b] = nbase + rng.bounded(nsize);
+                ks[b] = L.nbase + rng.bounded(L.nsize);
                 yk[b] = __ldcg(&Y[ks[b]]);
             }
         }
-        r.enext[j] = en + ep;                          // :178-179
-        r.enneg[j] = enn + static_cast<float>(nn) * epns;
-        ++fired;
-        drawn += remaining;
-        int64_t j2;
-        float en2;
-        const bool more = sc.next(r.enext, ef, j2, en2);
-        int32_t t2 = 0;
-        float ep2 = 0.0f, enn2 = 0.0f;
-        if (more) {
-            t2 = r.targets[j2];
-            ep2 = r.eps[j2];
-            enn2 = r.enneg[j2];
-        }
-        float hx = yh.x, hy = yh.y;
-        {   // attractive step (:145-155)
-            const float dx = hx - yt.x, dy = hy - yt.y;
-            const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
-            const float cf = attract_coef_fast(d2, p);
-            const float gx = p.alpha * clamp4(cf * dx);
-            const float gy = p.alpha * clamp4(cf * dy);
-            hx += gx;
-            hy += gy;
-            atomicAdd(&Y[t], make_float2(-gx, -gy));
-        }
-        while (true) {   // negative samples (:157-176)
-#pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                if (b < m && ks[b] != h) {
-                    const float dx = hx - yk[b].x, dy = hy - yk[b].y;
-                    const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
-                    const float cf = repulse_coef_fast(d2, p);
-                    hx = __fmaf_rn(p.alpha, clamp4(cf * dx), hx);
-                    hy = __fmaf_rn(p.alpha, clamp4(cf * dy), hy);
-                }
-            }
-            remaining -= m;
-            if (remaining <= 0) break;
-            m = remaining < NB ? remaining : NB;
-#pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                if (b < m) {
-                    ks[b] = nbase + rng.bounded(nsize);
-                    yk[b] = __ldcg(&Y[ks[b]]);
-                }
-            }
-        }
-        atomicAdd(&Y[h], make_float2(hx - yh.x, hy - yh.y));
-        if (!more) break;
-        j = j2;
-        en = en2;
-        t = t2;
-        ep = ep2;
-        enn = enn2;
     }
+    atomicAdd(&Y[h], make_float2(hx - yh.x, hy - yh.y));
+    return more;
 }
 
 // Gathered operands of one firing edge of a hub row (shared memory).
@@ -578,26 +583,48 @@ __device__ __forceinline__ void hub_row(int32_t h, const RowArgs<float>& r, floa
     }
 }
 
+// The epoch: warps first take the hub rows, one per warp, from counter[0];
+// then every lane takes the other rows one at a time from counter[1]
+// (claims of a warp's idle lanes aggregated into one atomic) and each loop
+// iteration applies one firing edge of every busy lane's row, so that lanes
+// do not wait for the longest row of a group.
 template <int NB, int MINB>
 __global__ void __launch_bounds__(256, MINB) sgd_rows_2d_f32(RowArgs<float> r, float2* __restrict__ Y,
                                                              SgdParams<float> p) {
     __shared__ HubEvent<NB> hub_ev[256 / 32][32];
     unsigned long long fired = 0, drawn = 0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int32_t nbulk_units = (r.nrows - r.nhub + 31) / 32;
-    const int32_t units = r.nhub + nbulk_units;
     while (true) {
         int32_t u = 0;
-        if (lane == 0) u = atomicAdd(r.counter, 1);
+        if (lane == 0) u = atomicAdd(&r.counter[0], 1);
         u = __shfl_sync(0xffffffffu, u, 0);
-        if (u >= units) break;
-        if (u < r.nhub) {
-            hub_row<NB>(r.order[u], r, Y, p, hub_ev[warp], fired, drawn);
-        } else {
-            const int32_t i = r.nhub + (u - r.nhub) * 32 + lane;
-            if (i < r.nrows) bulk_row<NB>(r.order[i], r, Y, p, fired, drawn);
-        }
+        if (u >= r.nhub) break;
+        hub_row<NB>(r.order[u], r, Y, p, hub_ev[warp], fired, drawn);
         __syncwarp();
+    }
+    const int32_t nbulk = r.nrows - r.nhub;
+    LaneRow L;
+    L.h = -1;
+    bool exhausted = false;
+    while (true) {
+        const bool need = L.h < 0 && !exhausted;
+        const unsigned needm = __ballot_sync(0xffffffffu, need);
+        if (needm) {
+            const int leader = __ffs(needm) - 1;
+            int32_t base = 0;
+            if (lane == leader) base = atomicAdd(&r.counter[1], __popc(needm));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (need) {
+                const int32_t idx = base + __popc(needm & ((1u << lane) - 1u));
+                if (idx >= nbulk) {
+                    exhausted = true;
+                } else if (!lane_row_start(L, r.order[r.nhub + idx], r, p)) {
+                    L.h = -1;   // no firing edge this epoch: take another row next iteration
+                }
+            }
+        }
+        if (__all_sync(0xffffffffu, exhausted && L.h < 0)) break;
+        if (L.h >= 0 && !lane_row_step<NB>(L, r, Y, p, fired, drawn)) L.h = -1;
     }
     add_totals(r.totals, fired, drawn);
 }
@@ -821,7 +848,7 @@ void SgdEngine<T>::tune(T* Y, int num_dim, int epoch, Launch& launch, cudaStream
     }
     const size_t total = static_cast<size_t>(ep_->n) * num_dim;
     DevArray<T> yscr(total, s), en(nnz, s), enn(nnz, s);
-    DevArray<int> counter(1, s);
+    DevArray<int> counter(2, s);
     cudaEvent_t a = event_get(), b = event_get();
     float best = 1e30f;
     for (int v = 0; v < NUM_SGD_2D_VARIANTS; ++v) {
@@ -880,8 +907,9 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
     // UMAPB_SGD_MAX_BLOCKS overrides the block count (0: from the window).
     int max_blocks = 0;
     if (const char* e = std::getenv("UMAPB_SGD_MAX_BLOCKS")) max_blocks = std::max(0, std::atoi(e));
-    const int64_t window_rows =
-        window_div > 0 ? std::max<int64_t>(ep_->n / window_div, std::min<int64_t>(ep_->n, 32768)) : int64_t(1) << 40;
+    const int64_t window_rows = window_div > 0
+        ? std::max<int64_t>(1, std::max<int64_t>(ep_->n / window_div, std::min<int64_t>(ep_->n / 8, 32768)))
+        : int64_t(1) << 40;
 
     // One epoch launch on (Yp, schedule state en/enn), claiming rows from 'counter'.
     auto launch = [&](T* Yp, T* en, T* enn, int* counter, unsigned long long* totals, int e_abs, int block,
@@ -925,17 +953,17 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
     }
     if (autotune && use_2d) tune(Y, num_dim, first, launch, s);
     const int W = last - first;
-    DevArray<int> counters(W, s);
+    DevArray<int> counters(2 * static_cast<size_t>(W), s);
     DevArray<unsigned long long> totals(check ? 2 * static_cast<size_t>(W) : 0, s);
     cudaEvent_t start = event_get(), finish = event_get();
     cudaGraphExec_t exec = nullptr;
     try {
         UMAPB_CUDA(cudaEventRecord(start, s));
         auto enqueue = [&] {
-            UMAPB_CUDA(cudaMemsetAsync(counters.get(), 0, W * sizeof(int), s));
+            UMAPB_CUDA(cudaMemsetAsync(counters.get(), 0, 2 * W * sizeof(int), s));
             if (check) UMAPB_CUDA(cudaMemsetAsync(totals.get(), 0, 2 * W * sizeof(unsigned long long), s));
             for (int e = first; e < last; ++e)
-                launch(Y, enext_.get(), enneg_.get(), counters.get() + (e - first),
+                launch(Y, enext_.get(), enneg_.get(), counters.get() + 2 * (e - first),
                        check ? totals.get() + 2 * (e - first) : nullptr, e, block_, variant_);
         };
         if (use_graphs) {
@@ -1018,12 +1046,13 @@ int SgdEngine<T>::default_variant() {
     return (x >= 0 && x < NUM_SGD_2D_VARIANTS) ? x : 0;
 }
 
-// UMAPB_SGD_WINDOW_DIV: rows in flight at most n / this (default 16; 0: no cap).
+// UMAPB_SGD_WINDOW_DIV: rows in flight at most max(n / this, min(n / 8, 32768))
+// (default 25; 0: no cap).
 template <typename T>
 int SgdEngine<T>::default_window_div() {
     const char* e = std::getenv("UMAPB_SGD_WINDOW_DIV");
     const int x = e ? std::atoi(e) : -1;
-    return (x >= 0 && x <= 1 << 20) ? x : 16;
+    return (x >= 0 && x <= 1 << 20) ? x : 25;
 }
 
 // UMAPB_SGD_PUBLISH_EVERY: firing edges between publications of a row's head
