@@ -45,8 +45,13 @@ _ref = None
 
 
 def build() -> None:
-    """Compile liboracle.so (and _ref when the reference sources are present)."""
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    """Compile liboracle.so, and _ref from the reference's headers when its
+    source tree is present ($UMAPB_REFERENCE, else /root/reference)."""
+    ref = os.environ.get("UMAPB_REFERENCE", "/root/reference")
+    args = ["make", "-s", "-C", HERE]
+    if os.path.isdir(os.path.join(ref, "include", "umappp")):
+        args.append(f"REFERENCE={ref}")
+    subprocess.run(args, check=True)
 
 
 def lib():

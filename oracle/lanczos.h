@@ -4,7 +4,8 @@
  *
  * The reference computes its spectral initialisation with irlba::compute on
  * the shifted normalised Laplacian (include/umappp/spectral_init.hpp:105-126).
- * irlba (and Eigen) are not on this machine, so this file restates the
+ * irlba and Eigen are dependencies the reference fetches at configure time
+ * (not vendored with it), so this file restates the
  * published thick-restart Lanczos method (Wu and Simon, SIAM J. Matrix Anal.
  * Appl. 22(2), 2000) for the symmetric positive semi-definite case, where the
  * top singular vectors are the top eigenvectors.  It is shared by the C

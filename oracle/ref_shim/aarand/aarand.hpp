@@ -1,5 +1,5 @@
 // Project-written stand-in for the aarand library (random distributions over a
-// C++ engine), absent from this machine.  The distributions are written from
+// C++ engine), which the reference fetches at configure time and is not vendored.  The distributions are written from
 // their textbook definitions; the streams therefore differ from upstream
 // aarand, which is why layouts are compared by quality metrics rather than
 // bit-for-bit against upstream umappp.  oracle/oracle.c draws from the same
