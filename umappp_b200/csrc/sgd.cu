@@ -211,7 +211,10 @@ struct NegStream {
             buf = philox4x32_10(c0, c1, c2, c3++, k0, k1);
             used = 0;
         }
-        return buf.v[used++];
+        // a select chain rather than buf.v[used]: a dynamically indexed array would live in local memory
+        const uint32_t v = used == 0 ? buf.v[0] : used == 1 ? buf.v[1] : used == 2 ? buf.v[2] : buf.v[3];
+        ++used;
+        return v;
     }
     // Exactly uniform integer in [0, n) (Lemire, "Fast random integer generation
     // in an interval", ACM TOMACS 2019): multiply-shift with rejection.
