@@ -45,9 +45,10 @@ CONFIGS = {
     "small_2k": (2_000, 10, 1, 0.0, "equal", 15, 500),
 }
 METRIC = "end-to-end s & SGD edge-updates/s, 1M pts; FP32/batched vs plain at equal trust"
-# DRAM bytes (read + write) per launch of the dominant kernels, from one ncu
-# capture (profiles/launches_mixture_1m.md; knn_tc16_kernel.md, sgd_epoch_2d_f32.md).
-TRAFFIC = {"mixture_1m": {"knn_tc16_kernel": 4.116e9 + 0.216e9, "sgd_epoch_2d_f32": 91.3e6 + 0.2e6}}
+# DRAM bytes (read + write) per launch of the dominant kernels, from ncu
+# captures summarised in profiles/traffic.json (each entry names the capture
+# it comes from and how it was scaled to the workload).
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "traffic.json")
 # Batched workload: 64 independent instances, sizes log-uniform in [500, 50000],
 # 30 dims, float32 5-cluster mixtures, k = 15, 200 epochs.
 BATCH = {"instances": 64, "min": 500, "max": 50_000, "dim": 30, "clusters": 5, "k": 15, "epochs": 200}
@@ -61,6 +62,30 @@ def make_data(cfg: str, seed: int = 20241203) -> np.ndarray:
     labels = rng.choice(nc, size=n, p=p)
     out = rng.standard_normal(size=(n, dim), dtype=np.float32)
     out += centres[labels]
+    return out
+
+
+def load_traffic(config: str, kernel: str):
+    """(bytes per launch, source note) of a kernel at a workload, or (None, None)."""
+    try:
+        with open(TRAFFIC_FILE) as f:
+            e = json.load(f)[config][kernel]
+        return float(e["bytes_per_launch"]), e["source"]
+    except (OSError, KeyError, ValueError, TypeError):
+        return None, None
+
+
+def l2_random_access_peaks(U) -> dict:
+    """Measured rates of uniformly random float2 loads and atomic adds over a
+    10^6-point (8 MB, L2-resident) array: the ceiling of the SGD epochs,
+    whose accesses are of that kind (umapb_measure_random_access)."""
+    import ctypes
+
+    out = {}
+    for mode, name in ((0, "gather_per_s"), (1, "atomic_add_per_s")):
+        r = ctypes.c_double()
+        U._lib.check(U.lib().umapb_measure_random_access(1_000_000, 400_000_000, mode, 5, ctypes.byref(r)))
+        out[name] = r.value
     return out
 
 
@@ -205,21 +230,39 @@ def run_ours(args, rank: int, world: int) -> dict | None:
     e2e_ms, _, _ = timed(step_host, args.steps)
 
     peaks = load_peaks()
-    # SGD roofline (algorithmic bytes per epoch: 4 nnz + 56 F + 8 N_neg, F and N_neg exact)
+    l2 = l2_random_access_peaks(U)
+    # SGD roofline.  Its accesses are random 8-byte loads and atomic adds that
+    # hit L2 (the 8 MB embedding stays there): per firing edge the head is read
+    # and its move added, the tail read and moved; per negative sample one
+    # read.  The ceiling is the measured rate of such loads and atomic adds,
+    # taken in proportion.  The HBM figure (algorithmic bytes of the schedule
+    # and the layout, 4 nnz + 56 F + 8 N_neg per epoch) is given beside it.
+    loads, adds = 2.0 * firing + negs, 2.0 * firing
+    l2_floor_s = loads / l2["gather_per_s"] + adds / l2["atomic_add_per_s"]
+    sgd_s = sgd_ms * 1e-3
     sgd_bytes = 4.0 * nnz * epochs + 56.0 * firing + 8.0 * negs
-    sgd_gbs = sgd_bytes / (sgd_ms * 1e-3) / 1e9
-    roof_sgd = {"bound": "hbm", "kernel": "sgd_epoch_2d_f32", "achieved": round(sgd_gbs, 1),
-                "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": round(sgd_gbs / peaks["hbm_gbs"], 4),
-                "traffic": TRAFFIC.get(args.config, {}).get("sgd_epoch_2d_f32"), "traffic_unit": "bytes per epoch launch",
-                "peak_source": peaks["source"], "time_ms": round(sgd_ms, 3),
-                "note": "algorithmic bytes 4*nnz*epochs + 56*F + 8*N_neg over the SGD stage time (all epochs)"}
+    sgd_gbs = sgd_bytes / sgd_s / 1e9
+    traffic_sgd, traffic_sgd_src = load_traffic(args.config, "sgd_rows_2d_f32")
+    roof_sgd = {"bound": "l2", "kernel": "sgd_rows_2d_f32",
+                "achieved": round((loads + adds) / sgd_s / 1e9, 2), "peak": round((loads + adds) / l2_floor_s / 1e9, 2),
+                "unit": "G random L2 accesses/s", "frac": round(l2_floor_s / sgd_s, 4),
+                "peak_source": "measured in this run (umapb_measure_random_access: loads "
+                               f"{l2['gather_per_s'] / 1e9:.1f} G/s, atomic adds {l2['atomic_add_per_s'] / 1e9:.1f} G/s)",
+                "frac_hbm": round(sgd_gbs / peaks["hbm_gbs"], 4), "achieved_hbm_gbs": round(sgd_gbs, 1),
+                "peak_hbm_gbs": peaks["hbm_gbs"], "peak_hbm_source": peaks["source"],
+                "traffic": traffic_sgd, "traffic_unit": "DRAM bytes per epoch launch", "traffic_source": traffic_sgd_src,
+                "time_ms": round(sgd_ms, 3),
+                "note": "accesses 4 F + N_neg (F firing edges, N_neg negative samples, exact) over the SGD stage "
+                        "time; frac = the time those accesses take at the measured random-access rates / the "
+                        "stage time"}
     # kNN roofline: the distances the pruned search computes (128 x 128 per tile pair,
     # 2*dim FLOP each, the FP32 GEMM count) over the kernel's device time
     knn_flops = tile_pairs * 128.0 * 128.0 * 2.0 * dim
     knn_tflops = knn_flops / (knn_kernel_ms * 1e-3) / 1e12 if knn_kernel_ms > 0 else 0.0
+    traffic_knn, traffic_knn_src = load_traffic(args.config, "knn_tc16_kernel")
     roof_knn = {"bound": "tensor", "kernel": "knn_tc16_kernel", "achieved": round(knn_tflops, 2),
                 "peak": peaks["bf16_tflops"], "unit": "TFLOP/s", "frac": round(knn_tflops / peaks["bf16_tflops"], 4),
-                "traffic": TRAFFIC.get(args.config, {}).get("knn_tc16_kernel"), "traffic_unit": "bytes per launch",
+                "traffic": traffic_knn, "traffic_unit": "DRAM bytes per launch", "traffic_source": traffic_knn_src,
                 "peak_source": peaks["source"], "time_ms": round(knn_kernel_ms, 3),
                 "note": "2*dim FLOP per computed (query, reference) pair over the kernel's CUDA-event time; "
                         "peak = measured dense BF16 (FP16 runs at the same rate); the 3-product FP16 split "
@@ -382,6 +425,7 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="mixture_1m", choices=sorted(CONFIGS) + ["batch64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batch64 sub-object of the default line")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -403,6 +447,12 @@ def main() -> None:
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     try:
         out = run_batch(args, rank, world) if args.config == "batch64" else run_ours(args, rank, world)
+        if world == 1 and args.config == "mixture_1m" and not args.no_batch and out is not None:
+            # the batched mode (64 independent instances in one call) beside the headline
+            b = run_batch(argparse.Namespace(steps=2, warmup=1), rank, world)
+            out["batch64"] = {k_: b[k_] for k_ in ("value", "unit", "sequential_plain_s", "speedup_vs_sequential",
+                                                   "gpu_launches", "sequential_gpu_launches")}
+            out["batch64"]["workload"] = b["config"]["workload"]
         if rank == 0 and out is not None:
             if world == 1 and not args.no_cpu_baseline and args.config != "batch64":
                 out["cpu_baseline"] = cpu_sample(args.config)
