@@ -485,7 +485,10 @@ struct HubEvent {
 // A hub row, by a whole warp: the lanes take 32 edges at a time -- schedule
 // step, tail and first NB negative samples gathered into shared memory, all
 // in parallel -- and lane 0 then applies the chunk's firing edges in order,
-// keeping the head in registers and publishing its move after each edge.
+// publishing the head's move after each edge.  Lane 0 re-reads the head once
+// per edge (the value arrives while the edge is computed and is used for the
+// next one, with this edge's move added), so that the pulls of other rows'
+// attractive steps on the hub are seen, as in the per-lane rows.
 template <int NB>
 __device__ __forceinline__ void hub_row(int32_t h, const RowArgs<float>& r, float2* __restrict__ Y,
                                         const SgdParams<float>& p, HubEvent<NB>* __restrict__ ev,
@@ -543,6 +546,7 @@ __device__ __forceinline__ void hub_row(int32_t h, const RowArgs<float>& r, floa
                 const int q = __ffs(mask) - 1;
                 mask &= mask - 1;
                 const HubEvent<NB>& e = ev[q];
+                const float2 seen = ld_relaxed_f2(&Y[h]);   // includes this lane's earlier publications
                 const float sx = hx, sy = hy;
                 {
                     const float dx = hx - e.yt.x, dy = hy - e.yt.y;
@@ -580,6 +584,8 @@ __device__ __forceinline__ void hub_row(int32_t h, const RowArgs<float>& r, floa
                     }
                 }
                 atomicAdd(&Y[h], make_float2(hx - sx, hy - sy));
+                hx = seen.x + (hx - sx);
+                hy = seen.y + (hy - sy);
             }
         }
         __syncwarp();
