@@ -485,10 +485,10 @@ struct HubEvent {
 // A hub row, by a whole warp: the lanes take 32 edges at a time -- schedule
 // step, tail and first NB negative samples gathered into shared memory, all
 // in parallel -- and lane 0 then applies the chunk's firing edges in order,
-// publishing the head's move after each edge.  Lane 0 re-reads the head once
-// per edge (the value arrives while the edge is computed and is used for the
-// next one, with this edge's move added), so that the pulls of other rows'
-// attractive steps on the hub are seen, as in the per-lane rows.
+// publishing the head's move after each edge.  Lane 0 re-reads the head at
+// the start of every chunk (the value arrives while the chunk is gathered) and
+// at the chunk's end takes it, plus the chunk's own moves, as the head: the
+// pulls of other rows' attractive steps on the hub are seen a chunk late.
 template <int NB>
 __device__ __forceinline__ void hub_row(int32_t h, const RowArgs<float>& r, float2* __restrict__ Y,
                                         const SgdParams<float>& p, HubEvent<NB>* __restrict__ ev,
@@ -502,6 +502,10 @@ __device__ __forceinline__ void hub_row(int32_t h, const RowArgs<float>& r, floa
     float hx = 0.0f, hy = 0.0f;   // lane 0: the head
     bool have = false;
     for (int64_t c = j0; c < r1; c += 32) {
+        float2 seen = make_float2(0.0f, 0.0f);
+        const bool resync = lane == 0 && have;
+        if (resync) seen = ld_relaxed_f2(&Y[h]);   // includes this lane's earlier publications
+        const float cx = hx, cy = hy;                          // lane 0: the head at the chunk's start
         const int64_t j = c + lane;
         bool fire = false;
         if (j < r1) {
@@ -546,7 +550,6 @@ __device__ __forceinline__ void hub_row(int32_t h, const RowArgs<float>& r, floa
                 const int q = __ffs(mask) - 1;
                 mask &= mask - 1;
                 const HubEvent<NB>& e = ev[q];
-                const float2 seen = ld_relaxed_f2(&Y[h]);   // includes this lane's earlier publications
                 const float sx = hx, sy = hy;
                 {
                     const float dx = hx - e.yt.x, dy = hy - e.yt.y;
@@ -584,8 +587,10 @@ __device__ __forceinline__ void hub_row(int32_t h, const RowArgs<float>& r, floa
                     }
                 }
                 atomicAdd(&Y[h], make_float2(hx - sx, hy - sy));
-                hx = seen.x + (hx - sx);
-                hy = seen.y + (hy - sy);
+            }
+            if (resync) {   // a read was issued at this chunk's start
+                hx = seen.x + (hx - cx);
+                hy = seen.y + (hy - cy);
             }
         }
         __syncwarp();
