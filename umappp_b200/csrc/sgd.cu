@@ -368,17 +368,33 @@ struct RowScan {
     }
 };
 
-// A lane's current row: its scan, the firing edge at hand (j, its target and
-// schedule state) and its instance's range for negative samples.
-struct LaneRow {
-    int32_t h;       // -1: none
-    int32_t t;
-    int32_t nbase;
-    uint32_t nsize;
+// One firing edge of a lane's row, with its target and schedule state.
+struct RowEdge {
     int64_t j;
     float en, ep, enn;
+    int32_t t;
+};
+
+// A lane's current row: its scan, the firing edge at hand (cur: state loaded
+// two steps ago), the one after it (nxt: state loads in flight) and its
+// instance's range for negative samples.
+struct LaneRow {
+    int32_t h;       // -1: none
+    int32_t nbase;
+    uint32_t nsize;
+    bool has_nxt;
+    RowEdge cur, nxt;
     RowScan sc;
 };
+
+// Finds the row's next firing edge and issues its state loads.
+__device__ __forceinline__ bool lane_row_fetch(LaneRow& L, RowEdge& e, const RowArgs<float>& r, float ef) {
+    if (!L.sc.next(r.enext, ef, e.j, e.en)) return false;
+    e.t = r.targets[e.j];
+    e.ep = r.eps[e.j];
+    e.enn = r.enneg[e.j];
+    return true;
+}
 
 // Starts row h on a lane: false when the row fires no edge this epoch.
 template <typename P>
@@ -387,11 +403,9 @@ __device__ __forceinline__ bool lane_row_start(LaneRow& L, int32_t h, const RowA
     const int64_t j0 = r.ptr[h], r1 = r.ptr[h + 1];
     if (j0 >= r1) return false;
     L.sc.start(r.enext, j0, r1, ef);
-    if (!L.sc.next(r.enext, ef, L.j, L.en)) return false;
+    if (!lane_row_fetch(L, L.cur, r, ef)) return false;
+    L.has_nxt = lane_row_fetch(L, L.nxt, r, ef);
     L.h = h;
-    L.t = r.targets[L.j];
-    L.ep = r.eps[L.j];
-    L.enn = r.enneg[L.j];
     instance_range(h, p, L.nbase, L.nsize);
     return true;
 }
@@ -400,20 +414,21 @@ __device__ __forceinline__ bool lane_row_start(LaneRow& L, int32_t h, const RowA
 // other rows' attractive steps), the tail and the first NB negative samples
 // are gathered together -- the negative-sample indices do not depend on the
 // layout; while they are in flight the schedule step is written and the
-// row's next firing edge found and its target and state loaded; then the
-// updates are applied in the reference's order and the head's move is
-// published.  Returns false when the row has no firing edge left.
+// state loads of the firing edge after the next one are issued (so an edge's
+// gathers never wait for its own state); then the updates are applied in the
+// reference's order and the head's move is published.  Returns false when
+// the row has no firing edge left.
 template <int NB>
 __device__ __forceinline__ bool lane_row_step(LaneRow& L, const RowArgs<float>& r, float2* __restrict__ Y,
                                               const SgdParams<float>& p, unsigned long long& fired,
                                               unsigned long long& drawn) {
     const float ef = p.epoch;
-    const int32_t h = L.h, t = L.t;
+    const int32_t h = L.h, t = L.cur.t;
     const float2 yh = ld_relaxed_f2(&Y[h]);
     const float2 yt = __ldcg(&Y[t]);
-    const float epns = L.ep / p.rate;   // optimize_layout.hpp:160-161
-    const int nn = static_cast<int>((ef - L.enn) / epns);
-    int remaining = nn > 0 ? nn : 0;     // a negative count draws nothing, as in the reference's loop
+    const float epns = L.cur.ep / p.rate;   // optimize_layout.hpp:160-161
+    const int nn = static_cast<int>((ef - L.cur.enn) / epns);
+    int remaining = nn > 0 ? nn : 0;         // a negative count draws nothing, as in the reference's loop
     NegStream rng(static_cast<uint32_t>(h), static_cast<uint32_t>(t), p.epoch_u, p.k0, p.k1);
     int m = remaining < NB ? remaining : NB;
     int32_t ks[NB];
@@ -425,15 +440,15 @@ __device__ __forceinline__ bool lane_row_step(LaneRow& L, const RowArgs<float>& 
             yk[b] = __ldcg(&Y[ks[b]]);
         }
     }
-    r.enext[L.j] = L.en + L.ep;                    // :178-179
-    r.enneg[L.j] = L.enn + static_cast<float>(nn) * epns;
+    r.enext[L.cur.j] = L.cur.en + L.cur.ep;                    // :178-179
+    r.enneg[L.cur.j] = L.cur.enn + static_cast<float>(nn) * epns;
     ++fired;
     drawn += remaining;
-    const bool more = L.sc.next(r.enext, ef, L.j, L.en);
+    // rotate: nxt becomes cur; fetch the one after
+    const bool more = L.has_nxt;
     if (more) {
-        L.t = r.targets[L.j];
-        L.ep = r.eps[L.j];
-        L.enn = r.enneg[L.j];
+        L.cur = L.nxt;
+        L.has_nxt = lane_row_fetch(L, L.nxt, r, ef);
     }
     float hx = yh.x, hy = yh.y;
     {   // attractive step (:145-155)
@@ -648,10 +663,10 @@ struct Sgd2dVariant {
     int neg_batch, min_blocks;
 };
 const Sgd2dVariant SGD_2D_VARIANTS[] = {
-    {sgd_rows_2d_f32<8, 3>, 8, 3},     // default
-    {sgd_rows_2d_f32<8, 2>, 8, 2},
+    {sgd_rows_2d_f32<6, 3>, 6, 3},     // default
+    {sgd_rows_2d_f32<8, 3>, 8, 3},
     {sgd_rows_2d_f32<6, 4>, 6, 4},
-    {sgd_rows_2d_f32<8, 4>, 8, 4},
+    {sgd_rows_2d_f32<6, 2>, 6, 2},
 };
 constexpr int NUM_SGD_2D_VARIANTS = sizeof(SGD_2D_VARIANTS) / sizeof(SGD_2D_VARIANTS[0]);
 
