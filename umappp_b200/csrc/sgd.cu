@@ -121,29 +121,32 @@ __global__ void __launch_bounds__(SCHED_BLOCK) sched_totals_kernel(int64_t nnz, 
 
 // Hub rows: expected to fire at least HUB_RATE edges per epoch.
 constexpr int HUB_RATE = 128;
+// Rows per group of the claim order (row_order_key_kernel).
+constexpr int ORDER_GROUP = 4096;
 
-// Order key of each row: its firing rate (sum of 1 / epochs_per_sample over
-// its edges, the expected number of firing edges per epoch) for hub rows, 0
-// for the others, as an order-preserving integer; a stable descending sort
-// then puts the hubs first, heaviest first, and keeps the other rows in index
-// order.
+// Order key of each row, sorted ascending: hub rows (firing rate -- the sum
+// of 1 / epochs_per_sample over the row, the expected number of firing edges
+// per epoch -- at least hub_rate) first, heaviest first; then the other rows
+// in groups of 'group' consecutive indices, in index order of the groups and
+// by descending rate within a group.  Rows in flight together then come from
+// a narrow index range (the concurrency the layout's quality depends on),
+// while the 32 rows a warp takes at once have similar lengths.
 template <typename T>
-__global__ void row_rate_kernel(int32_t n, const int64_t* __restrict__ ptr, const T* __restrict__ eps, float hub_rate,
-                                int all_by_rate, uint32_t* __restrict__ key, int32_t* __restrict__ row) {
+__global__ void row_order_key_kernel(int32_t n, const int64_t* __restrict__ ptr, const T* __restrict__ eps,
+                                     float hub_rate, int32_t group, uint64_t* __restrict__ key,
+                                     int32_t* __restrict__ row, int* __restrict__ nhub) {
+    int hubs = 0;
     for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float r = 0.0f;
         for (int64_t j = ptr[i]; j < ptr[i + 1]; ++j) r += 1.0f / static_cast<float>(eps[j]);
-        key[i] = (all_by_rate || r >= hub_rate) ? __float_as_uint(r) : 0u;   // r >= 0: bits order as values
+        const bool hub = r >= hub_rate;
+        hubs += hub;
+        const uint64_t g = hub ? 0ull : 1ull + static_cast<uint64_t>(i / group);
+        key[i] = (g << 32) | static_cast<uint64_t>(~__float_as_uint(r));   // r >= 0: bits order as values
         row[i] = i;
     }
-}
-
-__global__ void count_at_least_kernel(int32_t n, const uint32_t* __restrict__ key, uint32_t threshold,
-                                      int* __restrict__ count) {
-    int c = 0;
-    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) c += key[i] >= threshold;
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
+    for (int o = 16; o > 0; o >>= 1) hubs += __shfl_xor_sync(0xffffffffu, hubs, o);
+    if ((threadIdx.x & 31) == 0 && hubs) atomicAdd(nhub, hubs);
 }
 
 // ---------------------------------------------------------- epoch kernels --
@@ -613,10 +616,9 @@ __device__ __forceinline__ void hub_row(int32_t h, const RowArgs<float>& r, floa
 }
 
 // The epoch: warps first take the hub rows, one per warp, from counter[0];
-// then every lane takes the other rows one at a time from counter[1]
-// (claims of a warp's idle lanes aggregated into one atomic) and each loop
-// iteration applies one firing edge of every busy lane's row, so that lanes
-// do not wait for the longest row of a group.
+// then the other rows 32 at a time from counter[1], one per lane, each loop
+// iteration applying one firing edge of every lane's row (the rows a warp
+// takes have similar lengths, row_order_key_kernel).
 template <int NB, int MINB>
 __global__ void __launch_bounds__(256, MINB) sgd_rows_2d_f32(RowArgs<float> r, float2* __restrict__ Y,
                                                              SgdParams<float> p) {
@@ -632,28 +634,18 @@ __global__ void __launch_bounds__(256, MINB) sgd_rows_2d_f32(RowArgs<float> r, f
         __syncwarp();
     }
     const int32_t nbulk = r.nrows - r.nhub;
-    LaneRow L;
-    L.h = -1;
-    bool exhausted = false;
     while (true) {
-        const bool need = L.h < 0 && !exhausted;
-        const unsigned needm = __ballot_sync(0xffffffffu, need);
-        if (needm) {
-            const int leader = __ffs(needm) - 1;
-            int32_t base = 0;
-            if (lane == leader) base = atomicAdd(&r.counter[1], __popc(needm));
-            base = __shfl_sync(0xffffffffu, base, leader);
-            if (need) {
-                const int32_t idx = base + __popc(needm & ((1u << lane) - 1u));
-                if (idx >= nbulk) {
-                    exhausted = true;
-                } else if (!lane_row_start(L, r.order[r.nhub + idx], r, p)) {
-                    L.h = -1;   // no firing edge this epoch: take another row next iteration
-                }
-            }
+        int32_t base = 0;
+        if (lane == 0) base = atomicAdd(&r.counter[1], 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= nbulk) break;
+        LaneRow L;
+        L.h = -1;
+        const int32_t idx = base + lane;
+        if (idx < nbulk && !lane_row_start(L, r.order[r.nhub + idx], r, p)) L.h = -1;
+        while (__any_sync(0xffffffffu, L.h >= 0)) {
+            if (L.h >= 0 && !lane_row_step<NB>(L, r, Y, p, fired, drawn)) L.h = -1;
         }
-        if (__all_sync(0xffffffffu, exhausted && L.h < 0)) break;
-        if (L.h >= 0 && !lane_row_step<NB>(L, r, Y, p, fired, drawn)) L.h = -1;
     }
     add_totals(r.totals, fired, drawn);
 }
@@ -809,30 +801,25 @@ void SgdEngine<T>::setup(const DeviceEpochs<T>* ep, cudaStream_t s, int base_epo
     // rows by descending firing rate
     order_.allocate(n, s);
     if (n > 0) {
-        DevArray<uint32_t> key(n, s), key_sorted(n, s);
+        DevArray<uint64_t> key(n, s), key_sorted(n, s);
         DevArray<int32_t> row(n, s);
-        float hub_rate = static_cast<float>(HUB_RATE);   // UMAPB_SGD_HUB_RATE overrides it
-        if (const char* e = std::getenv("UMAPB_SGD_HUB_RATE")) hub_rate = static_cast<float>(std::atof(e));
-        // UMAPB_SGD_ORDER=1: every row by rate (0: hub rows by rate, then the others in index order)
-        const char* oe = std::getenv("UMAPB_SGD_ORDER");
-        const int all_by_rate = (oe && std::atoi(oe) == 1) ? 1 : 0;
-        row_rate_kernel<T><<<grid_for(n, 256), 256, 0, s>>>(n, ep->ptr.get(), ep->eps.get(), hub_rate, all_by_rate,
-                                                           key.get(), row.get());
-        UMAPB_LAUNCH_CHECK();
-        size_t tb = 0;
-        UMAPB_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, key.get(), key_sorted.get(), row.get(),
-                                                             order_.get(), n, 0, 32, s));
-        DevArray<unsigned char> temp(tb, s);
-        UMAPB_CUDA(cub::DeviceRadixSort::SortPairsDescending(temp.get(), tb, key.get(), key_sorted.get(), row.get(),
-                                                             order_.get(), n, 0, 32, s));
-        // hub rows (expected to fire at least HUB_RATE edges per epoch) lead the order
         DevArray<int> cnt(1, s);
         cnt.zero(s);
-        uint32_t thr_bits;
-        std::memcpy(&thr_bits, &hub_rate, sizeof(thr_bits));
-        if (hub_rate <= 0.0f) thr_bits = 1u;   // every row with a non-zero rate
-        count_at_least_kernel<<<grid_for(n, 256, 1024), 256, 0, s>>>(n, key_sorted.get(), thr_bits, cnt.get());
+        float hub_rate = static_cast<float>(HUB_RATE);   // UMAPB_SGD_HUB_RATE overrides it
+        if (const char* e = std::getenv("UMAPB_SGD_HUB_RATE")) hub_rate = static_cast<float>(std::atof(e));
+        int32_t group = ORDER_GROUP;                       // UMAPB_SGD_ORDER_GROUP overrides it
+        if (const char* e = std::getenv("UMAPB_SGD_ORDER_GROUP")) group = std::max(1, std::atoi(e));
+        row_order_key_kernel<T><<<grid_for(n, 256), 256, 0, s>>>(n, ep->ptr.get(), ep->eps.get(), hub_rate, group,
+                                                                key.get(), row.get(), cnt.get());
         UMAPB_LAUNCH_CHECK();
+        int end_bit = 33;
+        while (end_bit < 64 && (int64_t(1) << (end_bit - 32)) <= int64_t(n) / group + 1) ++end_bit;
+        size_t tb = 0;
+        UMAPB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, key.get(), key_sorted.get(), row.get(), order_.get(), n,
+                                                   0, end_bit, s));
+        DevArray<unsigned char> temp(tb, s);
+        UMAPB_CUDA(cub::DeviceRadixSort::SortPairs(temp.get(), tb, key.get(), key_sorted.get(), row.get(), order_.get(),
+                                                   n, 0, end_bit, s));
         UMAPB_CUDA(cudaMemcpyAsync(&nhub_, cnt.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
         UMAPB_SYNC(s);
     } else {
