@@ -383,6 +383,7 @@ struct RowEdge {
 // instance's range for negative samples.
 struct LaneRow {
     int32_t h;       // -1: none
+    float hx, hy;    // the head, when it is not re-read (FRESH = false)
     int32_t nbase;
     uint32_t nsize;
     bool has_nxt;
@@ -401,7 +402,8 @@ __device__ __forceinline__ bool lane_row_fetch(LaneRow& L, RowEdge& e, const Row
 
 // Starts row h on a lane: false when the row fires no edge this epoch.
 template <typename P>
-__device__ __forceinline__ bool lane_row_start(LaneRow& L, int32_t h, const RowArgs<float>& r, const P& p) {
+__device__ __forceinline__ bool lane_row_start(LaneRow& L, int32_t h, const RowArgs<float>& r, const float2* Y,
+                                               const P& p) {
     const float ef = p.epoch;
     const int64_t j0 = r.ptr[h], r1 = r.ptr[h + 1];
     if (j0 >= r1) return false;
@@ -409,6 +411,9 @@ __device__ __forceinline__ bool lane_row_start(LaneRow& L, int32_t h, const RowA
     if (!lane_row_fetch(L, L.cur, r, ef)) return false;
     L.has_nxt = lane_row_fetch(L, L.nxt, r, ef);
     L.h = h;
+    const float2 y0 = __ldcg(&Y[h]);
+    L.hx = y0.x;
+    L.hy = y0.y;
     instance_range(h, p, L.nbase, L.nsize);
     return true;
 }
@@ -421,13 +426,13 @@ __device__ __forceinline__ bool lane_row_start(LaneRow& L, int32_t h, const RowA
 // gathers never wait for its own state); then the updates are applied in the
 // reference's order and the head's move is published.  Returns false when
 // the row has no firing edge left.
-template <int NB>
+template <int NB, bool FRESH>
 __device__ __forceinline__ bool lane_row_step(LaneRow& L, const RowArgs<float>& r, float2* __restrict__ Y,
                                               const SgdParams<float>& p, unsigned long long& fired,
                                               unsigned long long& drawn) {
     const float ef = p.epoch;
     const int32_t h = L.h, t = L.cur.t;
-    const float2 yh = ld_relaxed_f2(&Y[h]);
+    const float2 yh = FRESH ? ld_relaxed_f2(&Y[h]) : make_float2(L.hx, L.hy);
     const float2 yt = __ldcg(&Y[t]);
     const float epns = L.cur.ep / p.rate;   // optimize_layout.hpp:160-161
     const int nn = static_cast<int>((ef - L.cur.enn) / epns);
@@ -487,6 +492,8 @@ __device__ __forceinline__ bool lane_row_step(LaneRow& L, const RowArgs<float>& 
         }
     }
     atomicAdd(&Y[h], make_float2(hx - yh.x, hy - yh.y));
+    L.hx = hx;
+    L.hy = hy;
     return more;
 }
 
@@ -619,7 +626,7 @@ __device__ __forceinline__ void hub_row(int32_t h, const RowArgs<float>& r, floa
 // then the other rows 32 at a time from counter[1], one per lane, each loop
 // iteration applying one firing edge of every lane's row (the rows a warp
 // takes have similar lengths, row_order_key_kernel).
-template <int NB, int MINB>
+template <int NB, int MINB, bool FRESH>
 __global__ void __launch_bounds__(256, MINB) sgd_rows_2d_f32(RowArgs<float> r, float2* __restrict__ Y,
                                                              SgdParams<float> p) {
     __shared__ HubEvent<NB> hub_ev[256 / 32][32];
@@ -642,9 +649,9 @@ __global__ void __launch_bounds__(256, MINB) sgd_rows_2d_f32(RowArgs<float> r, f
         LaneRow L;
         L.h = -1;
         const int32_t idx = base + lane;
-        if (idx < nbulk && !lane_row_start(L, r.order[r.nhub + idx], r, p)) L.h = -1;
+        if (idx < nbulk && !lane_row_start(L, r.order[r.nhub + idx], r, Y, p)) L.h = -1;
         while (__any_sync(0xffffffffu, L.h >= 0)) {
-            if (L.h >= 0 && !lane_row_step<NB>(L, r, Y, p, fired, drawn)) L.h = -1;
+            if (L.h >= 0 && !lane_row_step<NB, FRESH>(L, r, Y, p, fired, drawn)) L.h = -1;
         }
     }
     add_totals(r.totals, fired, drawn);
@@ -655,10 +662,10 @@ struct Sgd2dVariant {
     int neg_batch, min_blocks;
 };
 const Sgd2dVariant SGD_2D_VARIANTS[] = {
-    {sgd_rows_2d_f32<6, 3>, 6, 3},     // default
-    {sgd_rows_2d_f32<8, 3>, 8, 3},
-    {sgd_rows_2d_f32<6, 4>, 6, 4},
-    {sgd_rows_2d_f32<6, 2>, 6, 2},
+    {sgd_rows_2d_f32<6, 2, true>, 6, 2},     // default
+    {sgd_rows_2d_f32<6, 3, true>, 6, 3},
+    {sgd_rows_2d_f32<6, 2, false>, 6, 2},    // head kept in registers (not re-read), published per firing edge
+    {sgd_rows_2d_f32<6, 3, false>, 6, 3},
 };
 constexpr int NUM_SGD_2D_VARIANTS = sizeof(SGD_2D_VARIANTS) / sizeof(SGD_2D_VARIANTS[0]);
 
