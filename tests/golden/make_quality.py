@@ -6,7 +6,7 @@ benchmark's seeded Gaussian mixture: exact kNN (the reference's brute-force
 search), initialize() and Status::run() with the benchmark's options, for a
 few optimisation seeds.  Records, per seed, the fuzzy cross-entropy of the
 layout over the union graph and its trustworthiness (k = 15) on a fixed,
-seeded sample of query points.  The device test
+seeded sample of 10,000 query points (the full data set as candidates).  The device test
 (tests/test_gpu_quality.py) recomputes both for the device's layout on the
 same data and queries.
 
@@ -33,8 +33,11 @@ sys.path.insert(0, ROOT)
 import bench  # noqa: E402
 import oracle  # noqa: E402
 
+sys.path.insert(0, os.path.dirname(HERE))
+from helpers import trustworthiness_torch  # noqa: E402
+
 QUERY_SEED = 123
-NUM_QUERIES = 1000
+NUM_QUERIES = 10000
 
 
 def query_sample(n: int) -> np.ndarray:
@@ -76,7 +79,8 @@ def main() -> None:
         st.run(Y)
         secs = time.time() - t0
         ce = oracle.cross_entropy(g, Y, a, b)
-        tr = oracle.trustworthiness(X, Y, 15, queries=q)
+        # equal to oracle.trustworthiness (tests/test_quality_metrics.py), on all host cores
+        tr = trustworthiness_torch(X, Y, 15, queries=q, device="cpu", batch=16)
         runs.append({"optimize_seed": seed, "cross_entropy": ce, "trustworthiness": tr, "seconds": round(secs, 1)})
         print(runs[-1], flush=True)
 

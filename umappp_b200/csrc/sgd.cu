@@ -202,7 +202,7 @@ __device__ __forceinline__ void instance_range(int32_t h, const SgdParams<T>& p,
     size = static_cast<uint32_t>(p.inst_start[lo + 1] - base);
 }
 
-// Counter-based negative-sample stream of one firing edge.
+// Counter-based negative-sample stream of one firing edge (Philox4x32-7).
 struct NegStream {
     uint32_t c0, c1, c2, c3, k0, k1;
     Philox4 buf;
@@ -211,7 +211,10 @@ struct NegStream {
         : c0(h), c1(t), c2(epoch), c3(0), k0(key0), k1(key1), used(4) {}
     __device__ __forceinline__ uint32_t next() {
         if (used == 4) {
-            buf = philox4x32_10(c0, c1, c2, c3++, k0, k1);
+            // 7 rounds: the fewest for which Salmon et al. found Philox4x32
+            // free of BigCrush failures; negative samples only need uniform,
+            // independent indices, and the rounds are a tenth of an edge's work
+            buf = philox4x32<7>(c0, c1, c2, c3++, k0, k1);
             used = 0;
         }
         // a select chain rather than buf.v[used]: a dynamically indexed array would live in local memory
@@ -662,10 +665,10 @@ struct Sgd2dVariant {
     int neg_batch, min_blocks;
 };
 const Sgd2dVariant SGD_2D_VARIANTS[] = {
-    {sgd_rows_2d_f32<6, 2, true>, 6, 2},     // default
-    {sgd_rows_2d_f32<6, 3, true>, 6, 3},
-    {sgd_rows_2d_f32<6, 2, false>, 6, 2},    // head kept in registers (not re-read), published per firing edge
+    {sgd_rows_2d_f32<6, 2, false>, 6, 2},    // default: head kept in registers, published per firing edge
     {sgd_rows_2d_f32<6, 3, false>, 6, 3},
+    {sgd_rows_2d_f32<8, 2, false>, 8, 2},
+    {sgd_rows_2d_f32<6, 2, true>, 6, 2},     // head re-read before every firing edge
 };
 constexpr int NUM_SGD_2D_VARIANTS = sizeof(SGD_2D_VARIANTS) / sizeof(SGD_2D_VARIANTS[0]);
 
@@ -1070,12 +1073,12 @@ int SgdEngine<T>::default_variant() {
 }
 
 // UMAPB_SGD_WINDOW_DIV: rows in flight at most max(n / this, min(n / 8, 32768))
-// (default 25; 0: no cap).
+// (default 12; 0: no cap).
 template <typename T>
 int SgdEngine<T>::default_window_div() {
     const char* e = std::getenv("UMAPB_SGD_WINDOW_DIV");
     const int x = e ? std::atoi(e) : -1;
-    return (x >= 0 && x <= 1 << 20) ? x : 25;
+    return (x >= 0 && x <= 1 << 20) ? x : 12;
 }
 
 // UMAPB_SGD_PUBLISH_EVERY: firing edges between publications of a row's head
