@@ -500,111 +500,6 @@ __device__ __forceinline__ bool lane_row_step(LaneRow& L, const RowArgs<float>& 
     return more;
 }
 
-// Gathered operands of a lane's firing edge: tail, the first NB negative
-// samples, and the edge's negative-sample count.
-template <int NB>
-struct EdgeGather {
-    float2 yt;
-    float2 yk[NB];
-    int32_t ks[NB];
-    int32_t nn;     // negative samples to draw (0 when the reference's count is negative)
-};
-
-// Negative-sample count of an edge at epoch ef (optimize_layout.hpp:160-161).
-__device__ __forceinline__ int edge_negatives(const RowEdge& e, float ef, float rate, float& epns) {
-    epns = e.ep / rate;
-    return static_cast<int>((ef - e.enn) / epns);
-}
-
-// Issues the gathers of edge e of head h into g.
-template <int NB>
-__device__ __forceinline__ void edge_gather(EdgeGather<NB>& g, const RowEdge& e, int32_t h, int32_t nbase,
-                                            uint32_t nsize, float2* __restrict__ Y, const SgdParams<float>& p) {
-    float epns;
-    const int nn = edge_negatives(e, p.epoch, p.rate, epns);
-    g.nn = nn > 0 ? nn : 0;
-    g.yt = __ldcg(&Y[e.t]);
-    NegStream rng(static_cast<uint32_t>(h), static_cast<uint32_t>(e.t), p.epoch_u, p.k0, p.k1);
-    const int m = g.nn < NB ? g.nn : NB;
-#pragma unroll
-    for (int b = 0; b < NB; ++b) {
-        if (b < m) {
-            g.ks[b] = nbase + rng.bounded(nsize);
-            g.yk[b] = __ldcg(&Y[g.ks[b]]);
-        }
-    }
-}
-
-// One firing edge of a lane's row, its operands gathered one edge ahead: the
-// gathers of the next firing edge are issued before this edge's updates are
-// computed, so that an edge's loads are in flight while the previous edge's
-// arithmetic runs (the negative-sample indices and the tail do not depend on
-// the layout; the tail's position is read one edge earlier than in the plain
-// step).  The head is kept in registers and its move published per edge.
-template <int NB>
-__device__ __forceinline__ bool lane_row_step_pf(LaneRow& L, EdgeGather<NB>& g, const RowArgs<float>& r,
-                                                 float2* __restrict__ Y, const SgdParams<float>& p,
-                                                 unsigned long long& fired, unsigned long long& drawn) {
-    const float ef = p.epoch;
-    const int32_t h = L.h;
-    const RowEdge e = L.cur;
-    float epns;
-    const int nn = edge_negatives(e, ef, p.rate, epns);
-    r.enext[e.j] = e.en + e.ep;                    // :178-179
-    r.enneg[e.j] = e.enn + static_cast<float>(nn) * epns;
-    ++fired;
-    drawn += g.nn;
-    // rotate: nxt becomes cur (its gathers issued now), fetch the one after
-    const bool more = L.has_nxt;
-    EdgeGather<NB> gn;
-    if (more) {
-        L.cur = L.nxt;
-        edge_gather<NB>(gn, L.cur, h, L.nbase, L.nsize, Y, p);
-        L.has_nxt = lane_row_fetch(L, L.nxt, r, ef);
-    }
-    float hx = L.hx, hy = L.hy;
-    const float sx = hx, sy = hy;
-    {   // attractive step (:145-155)
-        const float dx = hx - g.yt.x, dy = hy - g.yt.y;
-        const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
-        const float cf = attract_coef_fast(d2, p);
-        const float gx = p.alpha * clamp4(cf * dx);
-        const float gy = p.alpha * clamp4(cf * dy);
-        hx += gx;
-        hy += gy;
-        atomicAdd(&Y[e.t], make_float2(-gx, -gy));
-    }
-    const int m = g.nn < NB ? g.nn : NB;
-#pragma unroll
-    for (int b = 0; b < NB; ++b) {   // negative samples (:157-176)
-        if (b < m && g.ks[b] != h) {
-            const float dx = hx - g.yk[b].x, dy = hy - g.yk[b].y;
-            const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
-            const float cf = repulse_coef_fast(d2, p);
-            hx = __fmaf_rn(p.alpha, clamp4(cf * dx), hx);
-            hy = __fmaf_rn(p.alpha, clamp4(cf * dy), hy);
-        }
-    }
-    if (g.nn > NB) {   // the rest of this edge's negative samples, from the same stream
-        NegStream rng(static_cast<uint32_t>(h), static_cast<uint32_t>(e.t), p.epoch_u, p.k0, p.k1);
-        for (int b = 0; b < g.nn; ++b) {
-            const int32_t k = L.nbase + rng.bounded(L.nsize);
-            if (b < NB || k == h) continue;
-            const float2 y = __ldcg(&Y[k]);
-            const float dx = hx - y.x, dy = hy - y.y;
-            const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
-            const float cf = repulse_coef_fast(d2, p);
-            hx = __fmaf_rn(p.alpha, clamp4(cf * dx), hx);
-            hy = __fmaf_rn(p.alpha, clamp4(cf * dy), hy);
-        }
-    }
-    atomicAdd(&Y[h], make_float2(hx - sx, hy - sy));
-    L.hx = hx;
-    L.hy = hy;
-    if (more) g = gn;
-    return more;
-}
-
 // Gathered operands of one firing edge of a hub row (shared memory).
 template <int NB>
 struct HubEvent {
@@ -734,7 +629,7 @@ __device__ __forceinline__ void hub_row(int32_t h, const RowArgs<float>& r, floa
 // then the other rows 32 at a time from counter[1], one per lane, each loop
 // iteration applying one firing edge of every lane's row (the rows a warp
 // takes have similar lengths, row_order_key_kernel).
-template <int NB, int MINB, bool FRESH, bool PF = false>
+template <int NB, int MINB, bool FRESH>
 __global__ void __launch_bounds__(256, MINB) sgd_rows_2d_f32(RowArgs<float> r, float2* __restrict__ Y,
                                                              SgdParams<float> p) {
     __shared__ HubEvent<NB> hub_ev[256 / 32][32];
@@ -758,16 +653,8 @@ __global__ void __launch_bounds__(256, MINB) sgd_rows_2d_f32(RowArgs<float> r, f
         L.h = -1;
         const int32_t idx = base + lane;
         if (idx < nbulk && !lane_row_start(L, r.order[r.nhub + idx], r, Y, p)) L.h = -1;
-        if (PF) {
-            EdgeGather<NB> g;
-            if (L.h >= 0) edge_gather<NB>(g, L.cur, L.h, L.nbase, L.nsize, Y, p);
-            while (__any_sync(0xffffffffu, L.h >= 0)) {
-                if (L.h >= 0 && !lane_row_step_pf<NB>(L, g, r, Y, p, fired, drawn)) L.h = -1;
-            }
-        } else {
-            while (__any_sync(0xffffffffu, L.h >= 0)) {
-                if (L.h >= 0 && !lane_row_step<NB, FRESH>(L, r, Y, p, fired, drawn)) L.h = -1;
-            }
+        while (__any_sync(0xffffffffu, L.h >= 0)) {
+            if (L.h >= 0 && !lane_row_step<NB, FRESH>(L, r, Y, p, fired, drawn)) L.h = -1;
         }
     }
     add_totals(r.totals, fired, drawn);
@@ -782,8 +669,6 @@ const Sgd2dVariant SGD_2D_VARIANTS[] = {
     {sgd_rows_2d_f32<6, 3, false>, 6, 3},
     {sgd_rows_2d_f32<8, 2, false>, 8, 2},
     {sgd_rows_2d_f32<6, 2, true>, 6, 2},     // head re-read before every firing edge
-    {sgd_rows_2d_f32<6, 2, false, true>, 6, 2},   // gathers one firing edge ahead
-    {sgd_rows_2d_f32<4, 2, false, true>, 4, 2},
 };
 constexpr int NUM_SGD_2D_VARIANTS = sizeof(SGD_2D_VARIANTS) / sizeof(SGD_2D_VARIANTS[0]);
 
