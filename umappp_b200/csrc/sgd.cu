@@ -322,54 +322,67 @@ __device__ __forceinline__ float2 ld_relaxed_f2(const float2* q) {
 // (one row per warp), then the other rows, 32 per warp (one per lane).
 constexpr int BULK_CHUNK = 8;    // edges of a row whose schedule state a lane loads at once
 
-// Value q of an 8-entry register window.
-__device__ __forceinline__ float pick8(const float (&w)[BULK_CHUNK], int q) {
-    float v = w[0];
-#pragma unroll
-    for (int k = 1; k < BULK_CHUNK; ++k) v = (q == k) ? w[k] : v;
-    return v;
-}
-
 // A row's schedule state, read BULK_CHUNK edges at a time into registers
 // (the next window's loads in flight while the current one is used), and the
 // row's firing edges found in it in order.
+__device__ __forceinline__ void cp_async4(float* dst_shared, const float* src, bool valid) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst_shared));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(valid ? 4 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// A lane's scan of its row's epoch_of_next_sample, BULK_CHUNK edges at a
+// time, through two windows in shared memory (the lane's column of its warp's
+// slab, [buffer][edge][lane]: conflict-free): the next window is copied
+// asynchronously (cp.async) while the current one is used.
 struct RowScan {
     int64_t cb, nb, r1;        // current window's first edge, next window's first edge, row end
-    float cw[BULK_CHUNK], nw[BULK_CHUNK];
+    float* w;                  // this lane's column: w[(buffer * BULK_CHUNK + q) * 32]
     unsigned cm;               // firing edges of the current window not yet taken
-    __device__ __forceinline__ void load(float (&w)[BULK_CHUNK], const float* __restrict__ enext, int64_t b) {
+    int cur;                   // buffer of the current window
+    __device__ __forceinline__ void load(int buf, const float* __restrict__ enext, int64_t b) {
 #pragma unroll
-        for (int q = 0; q < BULK_CHUNK; ++q) w[q] = (b + q < r1) ? enext[b + q] : CUDART_INF_F;
+        for (int q = 0; q < BULK_CHUNK; ++q) {
+            const bool ok = b + q < r1;
+            cp_async4(&w[(buf * BULK_CHUNK + q) * 32], ok ? enext + b + q : enext, ok);
+        }
+        cp_async_commit();
     }
-    __device__ __forceinline__ unsigned fire_mask(const float (&w)[BULK_CHUNK], float ef) {
+    __device__ __forceinline__ unsigned fire_mask(int buf, int64_t b, float ef) {
         unsigned m = 0;
 #pragma unroll
-        for (int q = 0; q < BULK_CHUNK; ++q) m |= (w[q] <= ef ? 1u : 0u) << q;
+        for (int q = 0; q < BULK_CHUNK; ++q) m |= (b + q < r1 && w[(buf * BULK_CHUNK + q) * 32] <= ef ? 1u : 0u) << q;
         return m;
     }
-    __device__ __forceinline__ void start(const float* __restrict__ enext, int64_t j0, int64_t end, float ef) {
+    __device__ __forceinline__ void start(float* column, const float* __restrict__ enext, int64_t j0, int64_t end,
+                                          float ef) {
+        w = column;
         r1 = end;
         cb = j0;
         nb = j0 + BULK_CHUNK;
-        load(cw, enext, cb);
-        load(nw, enext, nb);
-        cm = fire_mask(cw, ef);
+        cur = 0;
+        load(0, enext, cb);
+        load(1, enext, nb);
+        cp_async_wait<1>();
+        cm = fire_mask(0, cb, ef);
     }
     // Next firing edge (false: none left); en = its epoch_of_next_sample.
     __device__ __forceinline__ bool next(const float* __restrict__ enext, float ef, int64_t& j, float& en) {
         while (cm == 0) {
             if (nb >= r1) return false;
             cb = nb;
-#pragma unroll
-            for (int q = 0; q < BULK_CHUNK; ++q) cw[q] = nw[q];
+            cur ^= 1;
+            cp_async_wait<0>();
+            cm = fire_mask(cur, cb, ef);
             nb += BULK_CHUNK;
-            load(nw, enext, nb);
-            cm = fire_mask(cw, ef);
+            load(cur ^ 1, enext, nb);
         }
         const int q = __ffs(cm) - 1;
         cm &= cm - 1;
         j = cb + q;
-        en = pick8(cw, q);
+        en = w[(cur * BULK_CHUNK + q) * 32];
         return true;
     }
 };
@@ -406,11 +419,11 @@ __device__ __forceinline__ bool lane_row_fetch(LaneRow& L, RowEdge& e, const Row
 // Starts row h on a lane: false when the row fires no edge this epoch.
 template <typename P>
 __device__ __forceinline__ bool lane_row_start(LaneRow& L, int32_t h, const RowArgs<float>& r, const float2* Y,
-                                               const P& p) {
+                                               const P& p, float* column) {
     const float ef = p.epoch;
     const int64_t j0 = r.ptr[h], r1 = r.ptr[h + 1];
     if (j0 >= r1) return false;
-    L.sc.start(r.enext, j0, r1, ef);
+    L.sc.start(column, r.enext, j0, r1, ef);
     if (!lane_row_fetch(L, L.cur, r, ef)) return false;
     L.has_nxt = lane_row_fetch(L, L.nxt, r, ef);
     L.h = h;
@@ -633,6 +646,7 @@ template <int NB, int MINB, bool FRESH>
 __global__ void __launch_bounds__(256, MINB) sgd_rows_2d_f32(RowArgs<float> r, float2* __restrict__ Y,
                                                              SgdParams<float> p) {
     __shared__ HubEvent<NB> hub_ev[256 / 32][32];
+    __shared__ float scan_win[256 / 32][2 * BULK_CHUNK * 32];
     unsigned long long fired = 0, drawn = 0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     while (true) {
@@ -652,7 +666,7 @@ __global__ void __launch_bounds__(256, MINB) sgd_rows_2d_f32(RowArgs<float> r, f
         LaneRow L;
         L.h = -1;
         const int32_t idx = base + lane;
-        if (idx < nbulk && !lane_row_start(L, r.order[r.nhub + idx], r, Y, p)) L.h = -1;
+        if (idx < nbulk && !lane_row_start(L, r.order[r.nhub + idx], r, Y, p, &scan_win[warp][lane])) L.h = -1;
         while (__any_sync(0xffffffffu, L.h >= 0)) {
             if (L.h >= 0 && !lane_row_step<NB, FRESH>(L, r, Y, p, fired, drawn)) L.h = -1;
         }
