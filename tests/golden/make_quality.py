@@ -12,9 +12,14 @@ same data and queries.
 
     python tests/golden/make_quality.py [--workload mixture_1m] [--seeds 2]
         [--knn-cache PATH]     # .npz with the kNN, reused if present
+        [--layouts-out DIR | --layouts-in DIR] [--out PATH]
 
-The 1M-point workload takes about half an hour on 8 cores (mostly the
-exact kNN).
+The 1M-point workload takes about half an hour on 8 cores for the exact kNN
+and seven minutes per seed for the reference's SGD.  Its 10,000-query
+trustworthiness takes hours on host cores but seconds on a GPU, so the two
+halves can run apart: --layouts-out writes the reference's layouts (raw
+float32) and stops; --layouts-in reads them and takes the measures (with
+torch on a GPU when one is present).
 """
 from __future__ import annotations
 
@@ -44,12 +49,28 @@ def query_sample(n: int) -> np.ndarray:
     return np.sort(np.random.default_rng(QUERY_SEED).choice(n, size=min(NUM_QUERIES, n), replace=False)).astype(np.int32)
 
 
+def measures(X, g, a, b, Y, q):
+    """Cross-entropy over the union graph (oracle, FP64) and trustworthiness on
+    the query sample (tests/helpers.trustworthiness_torch, equal to
+    oracle.trustworthiness; on a GPU when there is one)."""
+    import torch
+
+    device = "cuda" if torch.cuda.is_available() else "cpu"
+    ce = oracle.cross_entropy(g, Y, a, b)
+    tr = trustworthiness_torch(X, Y, 15, queries=q, device=device, batch=16 if device == "cpu" else 8)
+    return ce, tr
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="mixture_1m", choices=sorted(bench.CONFIGS))
     ap.add_argument("--seeds", type=int, default=2)
     ap.add_argument("--threads", type=int, default=os.cpu_count() or 1)
     ap.add_argument("--knn-cache", default=None)
+    ap.add_argument("--layouts-out", default=None,
+                    help="write the reference layouts (<dir>/<workload>_<seed>.f32) and stop before the measures")
+    ap.add_argument("--layouts-in", default=None, help="take the reference layouts from this directory")
+    ap.add_argument("--out", default=None, help="fixture path (default tests/golden/quality_<workload>.json)")
     args = ap.parse_args()
 
     n, dim, _, _, _, k, epochs = bench.CONFIGS[args.workload]
@@ -72,17 +93,27 @@ def main() -> None:
     runs = []
     for s in range(args.seeds):
         seed = 1234567890 + s
-        Y = np.zeros((n, 2), np.float32)
-        t0 = time.time()
-        st = oracle.ref_initialize(nl, 2, Y, num_epochs=epochs, optimize_seed=seed, num_threads=args.threads,
-                                   num_threads_optimize=args.threads, num_threads_spectral=args.threads)
-        st.run(Y)
-        secs = time.time() - t0
-        ce = oracle.cross_entropy(g, Y, a, b)
-        # equal to oracle.trustworthiness (tests/test_quality_metrics.py), on all host cores
-        tr = trustworthiness_torch(X, Y, 15, queries=q, device="cpu", batch=16)
-        runs.append({"optimize_seed": seed, "cross_entropy": ce, "trustworthiness": tr, "seconds": round(secs, 1)})
+        path = lambda d: os.path.join(d, f"{args.workload}_{seed}.f32")  # noqa: E731
+        secs = None
+        if args.layouts_in:
+            Y = np.fromfile(path(args.layouts_in), dtype=np.float32).reshape(n, 2)
+        else:
+            Y = np.zeros((n, 2), np.float32)
+            t0 = time.time()
+            st = oracle.ref_initialize(nl, 2, Y, num_epochs=epochs, optimize_seed=seed, num_threads=args.threads,
+                                       num_threads_optimize=args.threads, num_threads_spectral=args.threads)
+            st.run(Y)
+            secs = round(time.time() - t0, 1)
+        if args.layouts_out:
+            os.makedirs(args.layouts_out, exist_ok=True)
+            Y.tofile(path(args.layouts_out))
+            print("wrote", path(args.layouts_out), secs, flush=True)
+            continue
+        ce, tr = measures(X, g, a, b, Y, q)
+        runs.append({"optimize_seed": seed, "cross_entropy": ce, "trustworthiness": tr, "seconds": secs})
         print(runs[-1], flush=True)
+    if args.layouts_out:
+        return
 
     out = {
         "workload": args.workload, "n": n, "dim": dim, "k": k, "epochs": epochs,
@@ -91,7 +122,7 @@ def main() -> None:
         "cross_entropy_graph": "FP64 similarities + union of the exact kNN, oracle.cross_entropy",
         "reference": runs,
     }
-    path = os.path.join(HERE, f"quality_{args.workload}.json")
+    path = args.out or os.path.join(HERE, f"quality_{args.workload}.json")
     with open(path, "w") as f:
         json.dump(out, f, indent=1)
     print("wrote", path)
