@@ -156,6 +156,39 @@ int umapb_initialize_data(int dtype, size_t data_dim, int32_t num_obs, const voi
                           void* embedding, const umapb_options* opt, umapb_status** out);
 
 /*
+ * umappp::initialize(NeighborList, ...) (include/umappp/initialize.hpp:69-119)
+ * with the neighbours given as two k x num_obs column-major matrices, one
+ * column per observation -- indices[i * k + j] and distances[i * k + j] are
+ * observation i's j-th neighbour, sorted by increasing distance -- the layout
+ * the reference's R harness builds its NeighborList from
+ * (tests/R/package/src/test.cpp:9-19) and knncolle's dense outputs use.
+ * Device arrays are used in place and host arrays copied as they are: no
+ * CSR is built on the host.  index_base is 0, or 1 for R's 1-based indices.
+ */
+int umapb_initialize_knn_matrix(int dtype, int32_t num_obs, int32_t k, const int32_t* indices, const void* distances,
+                                int index_base, size_t num_dim, void* embedding, const umapb_options* opt,
+                                umapb_status** out);
+
+/*
+ * A neighbour-search index resident on the device, the role of
+ * knncolle::Prebuilt: the data (num_obs x data_dim of dtype, observation i at
+ * [i * data_dim, (i + 1) * data_dim)) copied to the current device once and
+ * searched by every umapb_initialize_prebuilt, without copying it again.
+ */
+typedef struct umapb_prebuilt umapb_prebuilt;
+int umapb_prebuilt_create(int dtype, size_t data_dim, int32_t num_obs, const void* data, umapb_prebuilt** out);
+void umapb_prebuilt_free(umapb_prebuilt* prebuilt);
+
+/*
+ * umappp::initialize(const knncolle::Prebuilt&, num_dim, embedding, Options)
+ * (include/umappp/initialize.hpp:138-142): the exact Euclidean neighbour search
+ * of opt->num_neighbors on the prebuilt index's device data, then as
+ * umapb_initialize_neighbors.  Call with the index's device current.
+ */
+int umapb_initialize_prebuilt(const umapb_prebuilt* prebuilt, size_t num_dim, void* embedding, const umapb_options* opt,
+                              umapb_status** out);
+
+/*
  * Status::run(embedding, epoch_limit) (include/umappp/Status.hpp:101-128):
  * advances the layout in 'embedding' (read on entry, written on exit) from
  * epoch() to epoch_limit.  epoch_limit < 0 means num_epochs()

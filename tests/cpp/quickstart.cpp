@@ -1,7 +1,8 @@
 // Drop-in check: the reference's quick-start usage (README "Quick start")
 // written against the GPU headers: 2000 observations x 10 dims of N(0, 1)
 // data, exact neighbours on the device, initialize() then run(), plus a
-// partial run and the NeighborList overload.  Prints one line of results.
+// partial run, the NeighborList overload and a device-resident prebuilt
+// index.  Prints one line of results.
 #include <cmath>
 #include <cstdio>
 #include <random>
@@ -37,6 +38,15 @@ int main() {
     auto st2 = umappp::initialize(nl, out_dim, emb2.data(), opt);
     st2.run(emb2.data());
     const auto ep = st2.get_epoch_data();
+
+    // a device-resident prebuilt index (initialize.hpp:138-142) gives the same
+    // initial state as the data overload
+    umappp::DevicePrebuilt<double> prebuilt(ndim, nobs, data.data());
+    std::vector<double> e_a(nobs * out_dim), e_b(nobs * out_dim);
+    umappp::Options o2;
+    auto sa = umappp::initialize<int, double>(prebuilt, out_dim, e_a.data(), o2);
+    auto sb = umappp::initialize(ndim, nobs, data.data(), umappp::DeviceBuilder(), out_dim, e_b.data(), o2);
+    if (e_a != e_b || sa.get_epoch_data().edge_targets != sb.get_epoch_data().edge_targets) return 6;
     const auto ab = umappp::find_ab<double>(1.0, 0.1);
     std::printf("quickstart ok: epochs=%d edges=%zu a=%.6f b=%.6f y0=%.4f\n", status.epoch(), ep.edge_targets.size(),
                 ab.first, ab.second, embedding[0]);

@@ -271,3 +271,47 @@ def test_cpp_quickstart_runs(umap, tmp_path):
     r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
     assert "quickstart ok: epochs=500" in r.stdout
+
+
+def test_knn_matrix_input_matches_neighbor_list(umap):
+    """Neighbour matrices with one column per observation (the R harness's
+    layout, tests/R/package/src/test.cpp:9-19), 0- or 1-based, host or device,
+    give the same state as the same neighbours as a NeighborList."""
+    torch = pytest.importorskip("torch")
+    X = normal_data(700, 6, seed=31)
+    idx, dist = oracle.knn(X, 12)
+    ref_Y = np.zeros((700, 2))
+    ref = umap.initialize(oracle.CSR.from_dense(idx, dist).to_lists(), 2, ref_Y, umap.Options(num_epochs=30))
+    ref_ep = ref.get_epoch_data()
+    cases = [(idx, 0), (idx + 1, 1)]
+    for ind, base in cases:
+        Y = np.zeros((700, 2))
+        st = umap.initialize_knn_matrix(ind, dist, 2, Y, umap.Options(num_epochs=30), index_base=base)
+        ep = st.get_epoch_data()
+        assert np.array_equal(Y, ref_Y)
+        assert np.array_equal(ep.edge_targets, ref_ep.edge_targets)
+        assert np.array_equal(ep.epochs_per_sample, ref_ep.epochs_per_sample)
+    dev = torch.device("cuda", 0)
+    d_idx = torch.from_numpy(np.ascontiguousarray(idx, dtype=np.int32)).to(dev)
+    d_dist = torch.from_numpy(dist).to(dev)
+    Y = np.zeros((700, 2))
+    st = umap.initialize_knn_matrix(d_idx, d_dist, 2, Y, umap.Options(num_epochs=30))
+    assert np.array_equal(Y, ref_Y) and np.array_equal(st.get_epoch_data().edge_targets, ref_ep.edge_targets)
+    st.run(Y)
+    assert st.epoch() == 30 and np.all(np.isfinite(Y))
+
+
+def test_prebuilt_index_matches_data_overload(umap):
+    """initialize(const Prebuilt&, ...) (include/umappp/initialize.hpp:138-142):
+    a device-resident index searched twice gives the data overload's state."""
+    X = normal_data(900, 8, seed=32).astype(np.float32)
+    Y_ref = np.zeros((900, 2), np.float32)
+    ref = umap.initialize_from_data(X, 2, Y_ref, umap.Options(num_epochs=40))
+    pb = umap.Prebuilt(X)
+    for _ in range(2):
+        Y = np.zeros((900, 2), np.float32)
+        st = umap.initialize_prebuilt(pb, 2, Y, umap.Options(num_epochs=40))
+        assert np.array_equal(Y, Y_ref)
+        assert np.array_equal(st.get_epoch_data().edge_targets, ref.get_epoch_data().edge_targets)
+    st.run(Y)
+    assert st.epoch() == 40 and np.all(np.isfinite(Y))

@@ -36,7 +36,7 @@ __all__ = [
     "InitializeMethod", "Options", "Status", "EpochData", "initialize", "initialize_from_data", "knn",
     "neighbor_similarities", "combine_neighbor_sets", "similarities_to_epochs", "has_multiple_components",
     "spectral_init", "random_init", "find_ab", "choose_num_epochs", "optimize_layout", "loss_grad", "UmapbError",
-    "to_csr", "batch_run",
+    "to_csr", "batch_run", "initialize_knn_matrix", "Prebuilt", "initialize_prebuilt",
 ]
 
 
@@ -252,9 +252,15 @@ class Status:
 
 
 def initialize(neighbors, num_dim: int, embedding, options: Optional[Options] = None, dtype=None) -> Status:
-    """initialize(NeighborList x, num_dim, embedding, Options) (include/umappp/initialize.hpp:69-119)."""
+    """initialize(NeighborList x, num_dim, embedding, Options) (include/umappp/initialize.hpp:69-119).
+    A dense (indices, distances) pair of (n, k) arrays -- the k x n
+    column-per-observation matrices of the reference's R harness, in memory --
+    goes to the device as it is (initialize_knn_matrix)."""
     options = options or Options()
     dt = np.dtype(dtype) if dtype is not None else _float_dtype(embedding)
+    if isinstance(neighbors, tuple) and len(neighbors) == 2:
+        idx, dist = neighbors
+        return initialize_knn_matrix(idx, np.asarray(dist, dtype=dt), num_dim, embedding, options)
     ptr, idx, val = to_csr(neighbors, dt)
     n = len(ptr) - 1
     out = ctypes.c_void_p()
@@ -262,6 +268,67 @@ def initialize(neighbors, num_dim: int, embedding, options: Optional[Options] = 
     check(lib().umapb_initialize_neighbors(_dtype_code(dt), n, _ptr(ptr), _ptr(idx), _ptr(val), num_dim,
                                            _ptr(embedding), ctypes.byref(copt), ctypes.byref(out)))
     return Status(out.value, dt)
+
+
+def initialize_knn_matrix(indices, distances, num_dim: int, embedding, options: Optional[Options] = None,
+                          index_base: int = 0, num_obs: Optional[int] = None, k: Optional[int] = None) -> Status:
+    """initialize(NeighborList, ...) from neighbour matrices with one column per
+    observation (k x n column-major = (n, k) C-ordered: row i holds observation
+    i's neighbours by increasing distance), the R harness's layout
+    (tests/R/package/src/test.cpp:9-19); index_base=1 for R's 1-based indices.
+    Arrays may be host or device memory; for device pointers give num_obs and k."""
+    options = options or Options()
+    dt = _float_dtype(distances) if not isinstance(distances, int) else _float_dtype(embedding)
+    if isinstance(indices, np.ndarray):
+        indices = np.ascontiguousarray(indices, dtype=np.int32)
+    if isinstance(distances, np.ndarray):
+        distances = np.ascontiguousarray(distances)
+    if num_obs is None or k is None:
+        shape = indices.shape if isinstance(indices, np.ndarray) else tuple(indices.__cuda_array_interface__["shape"])
+        num_obs, k = int(shape[0]), int(shape[1])
+    out = ctypes.c_void_p()
+    copt = options.to_c()
+    check(lib().umapb_initialize_knn_matrix(_dtype_code(dt), num_obs, k, _ptr(indices), _ptr(distances),
+                                            int(index_base), num_dim, _ptr(embedding), ctypes.byref(copt),
+                                            ctypes.byref(out)))
+    return Status(out.value, dt)
+
+
+class Prebuilt:
+    """A neighbour-search index resident on the device (knncolle::Prebuilt's
+    role, include/umappp/initialize.hpp:138-142): the data copied to the
+    current device once, searched by every initialize_prebuilt."""
+
+    def __init__(self, data, num_obs: Optional[int] = None, data_dim: Optional[int] = None):
+        self.dtype = _float_dtype(data)
+        if num_obs is None or data_dim is None:
+            shape = data.shape if isinstance(data, np.ndarray) else tuple(data.__cuda_array_interface__["shape"])
+            num_obs, data_dim = int(shape[0]), int(shape[1])
+        if isinstance(data, np.ndarray):
+            data = np.ascontiguousarray(data)
+        h = ctypes.c_void_p()
+        check(lib().umapb_prebuilt_create(_dtype_code(self.dtype), data_dim, num_obs, _ptr(data), ctypes.byref(h)))
+        self._h = h.value
+        self.num_obs, self.data_dim = num_obs, data_dim
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            try:
+                lib().umapb_prebuilt_free(self._h)
+            except Exception:
+                pass
+            self._h = None
+
+
+def initialize_prebuilt(prebuilt: Prebuilt, num_dim: int, embedding, options: Optional[Options] = None) -> Status:
+    """initialize(const knncolle::Prebuilt&, num_dim, embedding, Options)
+    (include/umappp/initialize.hpp:138-142) on a device-resident index."""
+    options = options or Options()
+    out = ctypes.c_void_p()
+    copt = options.to_c()
+    check(lib().umapb_initialize_prebuilt(prebuilt._h, num_dim, _ptr(embedding), ctypes.byref(copt),
+                                          ctypes.byref(out)))
+    return Status(out.value, prebuilt.dtype)
 
 
 def initialize_from_data(data, num_dim: int, embedding, options: Optional[Options] = None,

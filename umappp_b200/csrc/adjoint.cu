@@ -22,6 +22,7 @@
 #include <type_traits>
 
 #include "stages.cuh"
+#include "umap_grad.cuh"
 
 namespace umapb {
 
@@ -68,8 +69,8 @@ __global__ void __launch_bounds__(ADJ_BLOCK) loss_grad_kernel(int32_t n, int dim
                 if (wij > 0) loss += wij * log(wij);
                 if (wij < 1) loss += (1 - wij) * log(1 - wij);
             }
-            const double att = a * b * pd2b / (d2 * denom);
-            const double rep = -b / ((d2 + eps_rep) * denom);
+            const double att = attract_dd2<false>(d2, a, b, a * b);    // dA/dd2 (umap_grad.cuh)
+            const double rep = repulse_dd2<false>(d2, a, b, -b, eps_rep);   // dR/dd2
             const double dd2 = wij * att + (1 - wij) * rep;
             if (gY) {
                 for (int d = 0; d < dim; ++d) {

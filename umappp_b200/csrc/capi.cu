@@ -83,6 +83,20 @@ struct StatusBase {
 
 }  // namespace umapb
 
+// A search index resident on the device (the role of knncolle::Prebuilt): the
+// data, kept for repeated neighbour searches without copying it again.
+struct umapb_prebuilt {
+    int dtype = UMAPB_F32;
+    int device = 0;
+    size_t dim = 0;
+    int32_t n = 0;
+    size_t bytes = 0;
+    void* data = nullptr;
+    ~umapb_prebuilt() {
+        if (data) cudaFree(data);
+    }
+};
+
 struct umapb_status {
     int dtype = UMAPB_F32;
     int device = 0;
@@ -296,6 +310,7 @@ void init_from_data(umapb_status* st, size_t data_dim, const void* data, void* e
     const int k = std::min<int>(st->opt.num_neighbors, n - 1);   // knncolle returns at most n - 1 neighbours
     require(st->opt.num_neighbors >= 1, "num_neighbors must be positive");
     StageTimer tm(s, st->stage_ms);
+    // resident data (a prebuilt index of this device) is used in place, host data staged
     DeviceIn<T> d(static_cast<const T*>(data), static_cast<size_t>(n) * data_dim, s);
     const int64_t nnz = static_cast<int64_t>(n) * k;
     DevArray<int32_t> idx(nnz, s);
@@ -308,6 +323,47 @@ void init_from_data(umapb_status* st, size_t data_dim, const void* data, void* e
     tm.end();
     auto impl = std::make_unique<StatusImpl<T>>(st);
     impl->initialize(ptr.get(), idx.get(), dist.get(), nnz, embedding, tm);
+    tm.resolve();
+    st->impl = std::move(impl);
+}
+
+__global__ void rebase_indices_kernel(int64_t total, const int32_t* __restrict__ in, int32_t base,
+                                      int32_t* __restrict__ out) {
+    for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < total; t += int64_t(gridDim.x) * blockDim.x)
+        out[t] = in[t] - base;
+}
+
+// Neighbour matrices with one column per observation (k x n, column-major:
+// observation i's neighbours at [i k, (i + 1) k), sorted by distance) -- the
+// layout of the reference's R harness (tests/R/package/src/test.cpp:9-19) and
+// of knncolle's dense outputs.  Device arrays are used in place (no CSR is
+// built on the host: the row pointers are i k); index_base 1 takes R's
+// 1-based indices.
+template <typename T>
+void init_from_knn_matrix(umapb_status* st, int32_t k, const int32_t* indices, const void* distances,
+                          int index_base, void* embedding) {
+    cudaStream_t s = st->stream;
+    const int32_t n = st->n;
+    require(k >= 0 && k < n, "k must be in [0, num_obs)");
+    require(index_base == 0 || index_base == 1, "index_base must be 0 or 1");
+    const int64_t nnz = static_cast<int64_t>(n) * k;
+    DeviceIn<int32_t> din(indices, nnz, s);
+    DevArray<int32_t> rebased;
+    const int32_t* idx = din.get();
+    if (index_base != 0 && nnz) {
+        rebased.allocate(nnz, s);
+        rebase_indices_kernel<<<grid_for(nnz, 256), 256, 0, s>>>(nnz, din.get(), index_base, rebased.get());
+        UMAPB_LAUNCH_CHECK();
+        idx = rebased.get();
+    }
+    DevArray<T> w(nnz, s);   // consumed (turned into weights)
+    if (nnz) UMAPB_CUDA(cudaMemcpyAsync(w.get(), distances, sizeof(T) * nnz, cudaMemcpyDefault, s));
+    DevArray<int64_t> ptr(static_cast<size_t>(n) + 1, s);
+    dense_row_ptr_kernel<<<grid_for(static_cast<size_t>(n) + 1, 256), 256, 0, s>>>(n, k, ptr.get());
+    UMAPB_LAUNCH_CHECK();
+    auto impl = std::make_unique<StatusImpl<T>>(st);
+    StageTimer tm(s, st->stage_ms);
+    impl->initialize(ptr.get(), idx, w.get(), nnz, embedding, tm);
     tm.resolve();
     st->impl = std::move(impl);
 }
@@ -526,6 +582,64 @@ int umapb_initialize_neighbors(int dtype, int32_t num_obs, const int64_t* row_pt
             init_from_neighbors<double>(st.get(), row_ptr, indices, distances, embedding);
         } else {
             init_from_neighbors<float>(st.get(), row_ptr, indices, distances, embedding);
+        }
+        *out = st.release();
+    });
+}
+
+int umapb_initialize_knn_matrix(int dtype, int32_t num_obs, int32_t k, const int32_t* indices, const void* distances,
+                                int index_base, size_t num_dim, void* embedding, const umapb_options* opt,
+                                umapb_status** out) {
+    return guarded([&] {
+        require(out != nullptr, "out must not be NULL");
+        *out = nullptr;
+        auto st = new_status(dtype, num_obs, num_dim, opt);
+        if (dtype == UMAPB_F64) {
+            init_from_knn_matrix<double>(st.get(), k, indices, distances, index_base, embedding);
+        } else {
+            init_from_knn_matrix<float>(st.get(), k, indices, distances, index_base, embedding);
+        }
+        *out = st.release();
+    });
+}
+
+int umapb_prebuilt_create(int dtype, size_t data_dim, int32_t num_obs, const void* data, umapb_prebuilt** out) {
+    return guarded([&] {
+        require(out != nullptr, "out must not be NULL");
+        *out = nullptr;
+        require_device();
+        require(dtype == UMAPB_F32 || dtype == UMAPB_F64, "dtype must be UMAPB_F32 or UMAPB_F64");
+        require(num_obs >= 2, "the neighbour search needs at least two observations");
+        require(data_dim >= 1 && data_dim <= INT32_MAX, "data_dim must be positive");
+        require(data != nullptr, "data must not be NULL");
+        auto pb = std::make_unique<umapb_prebuilt>();
+        pb->dtype = dtype;
+        pb->dim = data_dim;
+        pb->n = num_obs;
+        UMAPB_CUDA(cudaGetDevice(&pb->device));
+        pb->bytes = static_cast<size_t>(num_obs) * data_dim * (dtype == UMAPB_F64 ? 8 : 4);
+        UMAPB_CUDA(cudaMalloc(&pb->data, pb->bytes));
+        UMAPB_CUDA(cudaMemcpy(pb->data, data, pb->bytes, cudaMemcpyDefault));
+        *out = pb.release();
+    });
+}
+
+void umapb_prebuilt_free(umapb_prebuilt* pb) { delete pb; }
+
+int umapb_initialize_prebuilt(const umapb_prebuilt* pb, size_t num_dim, void* embedding, const umapb_options* opt,
+                              umapb_status** out) {
+    return guarded([&] {
+        require(pb != nullptr && pb->data != nullptr, "invalid prebuilt index");
+        int dev = -1;
+        UMAPB_CUDA(cudaGetDevice(&dev));
+        require(dev == pb->device, "the prebuilt index belongs to another device");
+        require(out != nullptr, "out must not be NULL");
+        *out = nullptr;
+        auto st = new_status(pb->dtype, pb->n, num_dim, opt);
+        if (pb->dtype == UMAPB_F64) {
+            init_from_data<double>(st.get(), pb->dim, pb->data, embedding);
+        } else {
+            init_from_data<float>(st.get(), pb->dim, pb->data, embedding);
         }
         *out = st.release();
     });

@@ -40,6 +40,7 @@
 #include <vector>
 
 #include "stages.cuh"
+#include "umap_grad.cuh"
 
 namespace umapb {
 
@@ -244,37 +245,25 @@ __device__ __forceinline__ T clamp4(T g) {
     return (T(4) < g) ? T(4) : g;
 }
 
-// FP32 layouts use the hardware-approximated power (__powf, an exp2 of b log2 x
-// in the special-function unit): the step is stochastic and clamped, and a
-// few-ulp error in d^(2b) is far below the noise of negative sampling (the
-// layout's cross-entropy was measured unchanged with libm's powf and IEEE
-// division at a million points).
-__device__ __forceinline__ float pow_b(float x, float b) { return __powf(x, b); }
-__device__ __forceinline__ double pow_b(double x, double b) { return pow(x, b); }
-
-// Attractive coefficient, optimize_layout.hpp:147-149.
+// The step coefficients, optimize_layout.hpp:147-149 (attractive) and
+// :170-171 (repulsive), from the edge derivatives shared with the adjoint
+// (umap_grad.cuh): attractive = -2 dA/dd2, repulsive = -2 gamma dR/dd2 with
+// eps = 0.001.  FP32 layouts use the hardware-approximated power (__powf, an
+// exp2 of b log2 x in the special-function unit) and divide (__fdividef): the
+// step is stochastic and clamped, and the layout's cross-entropy was measured
+// unchanged with libm's powf and IEEE division at a million points.
 template <typename T>
 __device__ __forceinline__ T attract_coef(T d2, const SgdParams<T>& p) {
-    const T pd2b = pow_b(d2, p.b);
-    return (p.neg2ab * pd2b) / (d2 * (p.a * pd2b + T(1)));
+    return attract_dd2<std::is_same<T, float>::value>(d2, p.a, p.b, p.neg2ab);
 }
 
-// Repulsive coefficient, optimize_layout.hpp:170-171.
 template <typename T>
 __device__ __forceinline__ T repulse_coef(T d2, const SgdParams<T>& p) {
-    return p.gamma2b / ((T(0.001) + d2) * (p.a * pow_b(d2, p.b) + T(1)));
+    return repulse_dd2<std::is_same<T, float>::value>(d2, p.a, p.b, p.gamma2b, T(0.001));
 }
 
-// FP32 coefficients for the 2-d kernel with fused multiply-adds and the
-// approximate divide (__fdividef, 2 ulp).
-__device__ __forceinline__ float attract_coef_fast(float d2, const SgdParams<float>& p) {
-    const float pd2b = pow_b(d2, p.b);
-    return __fdividef(p.neg2ab * pd2b, d2 * __fmaf_rn(p.a, pd2b, 1.0f));
-}
-
-__device__ __forceinline__ float repulse_coef_fast(float d2, const SgdParams<float>& p) {
-    return __fdividef(p.gamma2b, (0.001f + d2) * __fmaf_rn(p.a, pow_b(d2, p.b), 1.0f));
-}
+__device__ __forceinline__ float attract_coef_fast(float d2, const SgdParams<float>& p) { return attract_coef(d2, p); }
+__device__ __forceinline__ float repulse_coef_fast(float d2, const SgdParams<float>& p) { return repulse_coef(d2, p); }
 
 template <typename T>
 __device__ __forceinline__ T floor_eps(T d2) {
