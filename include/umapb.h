@@ -239,6 +239,23 @@ void umapb_status_free(umapb_status* st);
  * split-precision tensor-core distances and the k-th boundary is rescored in
  * FP64; for F64 data distances are computed in FP64.  k must be below num_obs.
  */
+/*
+ * One shard of umapb_knn, for a neighbour search split across GPUs (every
+ * rank holds the whole data and computes its shard; an all-gather of the
+ * shards' rows gives every rank the full lists -- umappp_b200.distributed).
+ * Shard 'shard' of 'num_shards' takes, for F32 data on the tensor-core path, a
+ * contiguous range of the search's tree-ordered query tiles carrying an equal
+ * share of the computed tile pairs, else a contiguous range of observations;
+ * the shards partition the observations.  Writes *out_count rows, ascending:
+ * out_rows[r] is an observation and out_indices / out_distances[r * k ..) its
+ * neighbours as umapb_knn gives them.  The output arrays need room for
+ * num_obs rows (host or device memory).  An extension: the reference's
+ * search runs on one machine.
+ */
+int umapb_knn_shard(int dtype, size_t data_dim, int32_t num_obs, const void* data, int k, int32_t shard,
+                    int32_t num_shards, int32_t* out_rows, int32_t* out_indices, void* out_distances,
+                    int32_t* out_count);
+
 int umapb_knn(int dtype, size_t data_dim, int32_t num_obs, const void* data, int k, int32_t* out_indices,
               void* out_distances);
 

@@ -12,14 +12,18 @@ same data and queries.
 
     python tests/golden/make_quality.py [--workload mixture_1m] [--seeds 2]
         [--knn-cache PATH]     # .npz with the kNN, reused if present
-        [--layouts-out DIR | --layouts-in DIR] [--out PATH]
+        [--layouts-out DIR | --layouts-in DIR] [--only cross_entropy|trustworthiness]
+        [--out PATH]
 
 The 1M-point workload takes about half an hour on 8 cores for the exact kNN
 and seven minutes per seed for the reference's SGD.  Its 10,000-query
 trustworthiness takes hours on host cores but seconds on a GPU, so the two
 halves can run apart: --layouts-out writes the reference's layouts (raw
 float32) and stops; --layouts-in reads them and takes the measures (with
-torch on a GPU when one is present).
+torch on a GPU when one is present).  --only takes one of the two measures
+and merges it into an existing fixture for the same workload and seeds, so the
+cross-entropy (which needs the kNN graph) can be taken where the kNN is, and
+the trustworthiness (which needs only the data and the layouts) on a GPU.
 """
 from __future__ import annotations
 
@@ -49,15 +53,17 @@ def query_sample(n: int) -> np.ndarray:
     return np.sort(np.random.default_rng(QUERY_SEED).choice(n, size=min(NUM_QUERIES, n), replace=False)).astype(np.int32)
 
 
-def measures(X, g, a, b, Y, q):
+def measures(X, g, a, b, Y, q, only=None):
     """Cross-entropy over the union graph (oracle, FP64) and trustworthiness on
     the query sample (tests/helpers.trustworthiness_torch, equal to
-    oracle.trustworthiness; on a GPU when there is one)."""
+    oracle.trustworthiness; on a GPU when there is one).  With 'only', the
+    other measure is None."""
     import torch
 
     device = "cuda" if torch.cuda.is_available() else "cpu"
-    ce = oracle.cross_entropy(g, Y, a, b)
-    tr = trustworthiness_torch(X, Y, 15, queries=q, device=device, batch=16 if device == "cpu" else 8)
+    ce = oracle.cross_entropy(g, Y, a, b) if only in (None, "cross_entropy") else None
+    tr = trustworthiness_torch(X, Y, 15, queries=q, device=device, batch=16 if device == "cpu" else 8) \
+        if only in (None, "trustworthiness") else None
     return ce, tr
 
 
@@ -70,24 +76,30 @@ def main() -> None:
     ap.add_argument("--layouts-out", default=None,
                     help="write the reference layouts (<dir>/<workload>_<seed>.f32) and stop before the measures")
     ap.add_argument("--layouts-in", default=None, help="take the reference layouts from this directory")
+    ap.add_argument("--only", default=None, choices=["cross_entropy", "trustworthiness"],
+                    help="take one measure and merge it into the existing fixture")
     ap.add_argument("--out", default=None, help="fixture path (default tests/golden/quality_<workload>.json)")
     args = ap.parse_args()
 
     n, dim, _, _, _, k, epochs = bench.CONFIGS[args.workload]
     X = bench.make_data(args.workload)
-    t0 = time.time()
-    if args.knn_cache and os.path.exists(args.knn_cache):
-        z = np.load(args.knn_cache)
-        idx, dist = z["idx"], z["dist"]
-    else:
-        idx, dist = oracle.ref_knn(X, k, nthreads=args.threads)
-        if args.knn_cache:
-            np.savez(args.knn_cache, idx=idx, dist=dist)
-    print(f"knn {time.time() - t0:.0f} s", flush=True)
-    nl = oracle.CSR.from_dense(idx, dist)
-    w, _, _ = oracle.neighbor_similarities(nl.astype(np.float64))
-    g = oracle.combine_neighbor_sets(w, 1.0)
+    if args.only is not None and not args.layouts_in:
+        ap.error("--only measures the layouts of --layouts-in")
+    nl = g = None
     a, b = oracle.find_ab(1.0, 0.1)
+    if args.only != "trustworthiness":   # the trustworthiness alone needs no kNN
+        t0 = time.time()
+        if args.knn_cache and os.path.exists(args.knn_cache):
+            z = np.load(args.knn_cache)
+            idx, dist = z["idx"], z["dist"]
+        else:
+            idx, dist = oracle.ref_knn(X, k, nthreads=args.threads)
+            if args.knn_cache:
+                np.savez(args.knn_cache, idx=idx, dist=dist)
+        print(f"knn {time.time() - t0:.0f} s", flush=True)
+        nl = oracle.CSR.from_dense(idx, dist)
+        w, _, _ = oracle.neighbor_similarities(nl.astype(np.float64))
+        g = oracle.combine_neighbor_sets(w, 1.0)
     q = query_sample(n)
 
     runs = []
@@ -109,8 +121,9 @@ def main() -> None:
             Y.tofile(path(args.layouts_out))
             print("wrote", path(args.layouts_out), secs, flush=True)
             continue
-        ce, tr = measures(X, g, a, b, Y, q)
-        runs.append({"optimize_seed": seed, "cross_entropy": ce, "trustworthiness": tr, "seconds": secs})
+        ce, tr = measures(X, g, a, b, Y, q, args.only)
+        run = {"optimize_seed": seed, "cross_entropy": ce, "trustworthiness": tr, "seconds": secs}
+        runs.append({key: v for key, v in run.items() if v is not None or key == "seconds"})
         print(runs[-1], flush=True)
     if args.layouts_out:
         return
@@ -123,6 +136,17 @@ def main() -> None:
         "reference": runs,
     }
     path = args.out or os.path.join(HERE, f"quality_{args.workload}.json")
+    if args.only is not None and os.path.exists(path):
+        with open(path) as f:
+            old = json.load(f)
+        same = (old.get("workload") == args.workload and old.get("query_seed") == QUERY_SEED
+                and old.get("num_queries") == len(q))
+        by_seed = {r["optimize_seed"]: r for r in old["reference"]} if same else {}
+        for r in runs:   # keep the other measure (and the timing) of the same seed
+            merged = dict(by_seed.get(r["optimize_seed"], {}))
+            merged.update({key: v for key, v in r.items() if v is not None})
+            r.clear()
+            r.update(merged)
     with open(path, "w") as f:
         json.dump(out, f, indent=1)
     print("wrote", path)

@@ -35,3 +35,28 @@ def test_knn_exact_on_benchmark_data(umap, workload):
           f"largest tensor-core distance error {L.umapb_knn_last_tc_error():.2e}")
     assert bad == 0
     assert err <= 1e-6
+
+
+@pytest.mark.parametrize("workload,dtype,num_shards", [("mixture_100k", np.float32, 2), ("mixture_100k", np.float32, 7),
+                                                       ("mixture_100k", np.float64, 3)])
+def test_knn_shards_partition_and_reproduce_full_search(umap, workload, dtype, num_shards):
+    """umapb_knn_shard: the shards' rows partition the observations and, put
+    together, equal the unsharded search bit for bit (indices and distances)."""
+    X = bench.make_data(workload).astype(dtype)
+    k = bench.CONFIGS[workload][5]
+    idx, dist = umap.knn(X, k)
+    seen = np.zeros(X.shape[0], np.int64)
+    got_idx = np.full_like(idx, -1)
+    got_dist = np.zeros_like(dist)
+    counts = []
+    for s in range(num_shards):
+        rows, si, sd = umap.knn_shard(X, k, s, num_shards)
+        assert np.all(np.diff(rows) > 0)
+        seen[rows] += 1
+        got_idx[rows] = si
+        got_dist[rows] = sd
+        counts.append(len(rows))
+    print(f"{workload} {np.dtype(dtype).name} {num_shards} shards: rows per shard {counts}")
+    assert np.all(seen == 1)
+    assert np.array_equal(got_idx, idx)
+    assert np.array_equal(got_dist, dist)

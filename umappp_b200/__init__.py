@@ -36,7 +36,7 @@ __all__ = [
     "InitializeMethod", "Options", "Status", "EpochData", "initialize", "initialize_from_data", "knn",
     "neighbor_similarities", "combine_neighbor_sets", "similarities_to_epochs", "has_multiple_components",
     "spectral_init", "random_init", "find_ab", "choose_num_epochs", "optimize_layout", "loss_grad", "UmapbError",
-    "to_csr", "batch_run", "initialize_knn_matrix", "Prebuilt", "initialize_prebuilt",
+    "to_csr", "batch_run", "initialize_knn_matrix", "Prebuilt", "initialize_prebuilt", "knn_shard",
 ]
 
 
@@ -370,6 +370,22 @@ def batch_run(data, sizes, num_dim: int, embedding, options: Optional[Options] =
 
 
 # ------------------------------------------------------------ stage calls --
+
+def knn_shard(data: np.ndarray, k: int, shard: int, num_shards: int):
+    """One shard of knn() for a search split across ranks (umapb_knn_shard):
+    (rows, indices, distances) with rows ascending and indices / distances of
+    shape (len(rows), k).  The shards of 0 .. num_shards - 1 partition the rows."""
+    data = np.ascontiguousarray(data)
+    n, dim = data.shape
+    rows = np.zeros(n, dtype=np.int32)
+    idx = np.zeros((n, k), dtype=np.int32)
+    dist = np.zeros((n, k), dtype=data.dtype)
+    count = ctypes.c_int32()
+    check(lib().umapb_knn_shard(_dtype_code(data.dtype), dim, n, _ptr(data), k, int(shard), int(num_shards),
+                                _ptr(rows), _ptr(idx), _ptr(dist), ctypes.byref(count)))
+    m = count.value
+    return rows[:m].copy(), idx[:m].copy(), dist[:m].copy()
+
 
 def knn(data: np.ndarray, k: int):
     """Exact Euclidean kNN; returns (indices int32 (n, k), distances (n, k) of data's type)."""

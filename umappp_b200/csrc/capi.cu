@@ -327,6 +327,17 @@ void init_from_data(umapb_status* st, size_t data_dim, const void* data, void* e
     st->impl = std::move(impl);
 }
 
+// out[r * k + c] = in[rows[r] * k + c]
+template <typename V>
+__global__ void gather_rows_kernel(int32_t nrows, int32_t k, const int32_t* __restrict__ rows, const V* __restrict__ in,
+                                   V* __restrict__ out) {
+    const int64_t total = static_cast<int64_t>(nrows) * k;
+    for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < total; t += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t r = t / k, c = t % k;
+        out[t] = in[static_cast<int64_t>(rows[r]) * k + c];
+    }
+}
+
 __global__ void rebase_indices_kernel(int64_t total, const int32_t* __restrict__ in, int32_t base,
                                       int32_t* __restrict__ out) {
     for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < total; t += int64_t(gridDim.x) * blockDim.x)
@@ -725,6 +736,46 @@ int umapb_knn(int dtype, size_t data_dim, int32_t num_obs, const void* data, int
         }
         oi.finish();
         UMAPB_SYNC(c.stream);
+    });
+}
+
+int umapb_knn_shard(int dtype, size_t data_dim, int32_t num_obs, const void* data, int k, int32_t shard,
+                    int32_t num_shards, int32_t* out_rows, int32_t* out_indices, void* out_distances,
+                    int32_t* out_count) {
+    return guarded([&] {
+        require_device();
+        require(out_count != nullptr, "out_count must not be NULL");
+        require(num_shards >= 1 && shard >= 0 && shard < num_shards, "shard must be in [0, num_shards)");
+        Context& c = thread_context();
+        cudaStream_t s = c.stream;
+        const size_t total = static_cast<size_t>(num_obs) * data_dim;
+        const size_t nk = static_cast<size_t>(num_obs) * (k > 0 ? k : 0);
+        auto body = [&](auto tag) {
+            using T = decltype(tag);
+            DeviceIn<T> d(static_cast<const T*>(data), total, s);
+            DevArray<int32_t> idx(nk, s), rows;
+            DevArray<T> dist(nk, s);
+            int32_t nrows = 0;
+            knn_exact_shard<T>(d.get(), num_obs, static_cast<int32_t>(data_dim), k, KnnShard{shard, num_shards},
+                               idx.get(), dist.get(), rows, nrows, s);
+            // the shard's rows, compacted in row order
+            DevArray<int32_t> cidx(static_cast<size_t>(nrows) * k, s);
+            DevArray<T> cdist(static_cast<size_t>(nrows) * k, s);
+            if (nrows > 0) {
+                gather_rows_kernel<int32_t><<<grid_for(static_cast<size_t>(nrows) * k, 256), 256, 0, s>>>(
+                    nrows, k, rows.get(), idx.get(), cidx.get());
+                gather_rows_kernel<T><<<grid_for(static_cast<size_t>(nrows) * k, 256), 256, 0, s>>>(
+                    nrows, k, rows.get(), dist.get(), cdist.get());
+                UMAPB_LAUNCH_CHECK();
+                require(out_rows && out_indices && out_distances, "output arrays must not be NULL");
+                UMAPB_CUDA(cudaMemcpyAsync(out_rows, rows.get(), sizeof(int32_t) * nrows, cudaMemcpyDefault, s));
+                UMAPB_CUDA(cudaMemcpyAsync(out_indices, cidx.get(), sizeof(int32_t) * nrows * k, cudaMemcpyDefault, s));
+                UMAPB_CUDA(cudaMemcpyAsync(out_distances, cdist.get(), sizeof(T) * nrows * k, cudaMemcpyDefault, s));
+            }
+            UMAPB_SYNC(s);
+            *out_count = nrows;
+        };
+        if (dtype == UMAPB_F64) body(double{}); else body(float{});
     });
 }
 

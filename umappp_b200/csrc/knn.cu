@@ -164,17 +164,20 @@ __global__ void __launch_bounds__(KNN_BLOCK) knn_bruteforce_kernel(const T* __re
 // true neighbour.
 template <int KCAP>
 __global__ void knn_rescore_kernel(const float* __restrict__ data, int32_t n, int32_t dim, int32_t k,
+                                   const int32_t* __restrict__ queries, int32_t nq, int cand_by_slot,
                                    const int32_t* __restrict__ cand_idx, const float* __restrict__ cand_d2,
                                    int32_t* __restrict__ out_idx, float* __restrict__ out_dist,
                                    double* __restrict__ out_dist64, int32_t* __restrict__ redo,
                                    int32_t* __restrict__ redo_count, const float* __restrict__ norms,
                                    const unsigned int* __restrict__ norm_max_bits, double tc_rel,
                                    unsigned int* __restrict__ tc_err_bits) {
-    const int32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= n) return;
+    const int32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= nq) return;
+    const int32_t q = queries ? queries[slot] : slot;     // the query's data row (output row)
+    const size_t crow = static_cast<size_t>(cand_by_slot ? slot : q);   // its candidate list
     double d64[KCAP];
     int id[KCAP];
-    const int32_t* ci = cand_idx + static_cast<size_t>(q) * KCAP;
+    const int32_t* ci = cand_idx + crow * KCAP;
     const float* xq = data + static_cast<size_t>(q) * dim;
     int m = 0;
     float worst = 0.0f;   // largest |FP32 candidate distance - FP64 distance| / (|q|^2 + max |r|^2)
@@ -191,7 +194,7 @@ __global__ void knn_rescore_kernel(const float* __restrict__ data, int32_t n, in
                 s = __dadd_rn(s, __dmul_rn(diff, diff));
             }
             if (err_scale > 0.0) {
-                const double e = fabs(static_cast<double>(cand_d2[static_cast<size_t>(q) * KCAP + c]) - s) * err_scale;
+                const double e = fabs(static_cast<double>(cand_d2[crow * KCAP + c]) - s) * err_scale;
                 worst = fmaxf(worst, static_cast<float>(e));
             }
         } else {
@@ -215,7 +218,7 @@ __global__ void knn_rescore_kernel(const float* __restrict__ data, int32_t n, in
     // true distance of such a point, the query is recomputed in FP64.
     // For tensor-core candidates (norms given) the FP32 values are
     // |q|^2 + |r|^2 - 2 q.r with an absolute error below tc_rel * (|q|^2 + max |r|^2).
-    const float last32 = cand_d2[static_cast<size_t>(q) * KCAP + KCAP - 1];
+    const float last32 = cand_d2[crow * KCAP + KCAP - 1];
     const double rel = (dim + 2) * 1.2e-7 * 2.0;
     const double kth = d64[k - 1];
     const bool full_list = (n - 1) <= KCAP;   // every other point is a candidate
@@ -283,40 +286,88 @@ __global__ void norm_max_kernel(int32_t n, const float* __restrict__ norms, unsi
 // the final FP32 additions stay below 2^-17.
 constexpr double TC_REL_BOUND = 1.0 / 131072.0;
 
+__global__ void iota_kernel(int32_t count, int32_t first, int32_t* __restrict__ out) {
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) out[i] = first + i;
+}
+
+// The rows [lo, hi) of shard 'index' of 'count' equal contiguous ranges of the data rows.
+void shard_row_range(int32_t n, KnnShard shard, int32_t& lo, int32_t& hi) {
+    lo = static_cast<int32_t>(static_cast<int64_t>(n) * shard.index / shard.count);
+    hi = static_cast<int32_t>(static_cast<int64_t>(n) * (shard.index + 1) / shard.count);
+}
+
+// With a shard (count > 1) the search covers only the shard's queries, whose
+// data rows go to *rows (*nrows of them); out_idx / out_dist are written at
+// those rows only.
 template <int KCAP>
 void run_f32(const float* data, int32_t n, int32_t dim, int32_t k, int32_t* out_idx, float* out_dist,
-             double* out_dist64, cudaStream_t s) {
-    DevArray<int32_t> ci(static_cast<size_t>(n) * KCAP, s);
-    DevArray<float> cd(static_cast<size_t>(n) * KCAP, s);
+             double* out_dist64, cudaStream_t s, KnnShard shard = KnnShard(), DevArray<int32_t>* rows = nullptr,
+             int32_t* nrows = nullptr) {
+    const bool sharded = shard.count > 1;
     DevArray<float> norms;
     DevArray<unsigned int> norm_max(1, s);
-    const bool tc = use_tensor_cores() && knn_tc_supported(dim, KCAP);
+    bool tc = use_tensor_cores() && knn_tc_supported(dim, KCAP);
+    // candidates: by data row (tensor-core search, unsharded brute force) or by
+    // slot of the shard's row list (sharded brute force)
+    DevArray<int32_t> ci;
+    DevArray<float> cd;
+    int32_t nq = n;
+    const int32_t* queries = nullptr;
+    bool by_slot = false;
     if (tc) {
+        ci.allocate(static_cast<size_t>(n) * KCAP, s);
+        cd.allocate(static_cast<size_t>(n) * KCAP, s);
         const int32_t n_pad = ((n + 127) / 128) * 128;
         norms.allocate(n_pad, s);
         DevArray<int> err(1, s);
         err.zero(s);
-        knn_tc_candidates(data, n, dim, KCAP, ci.get(), cd.get(), norms.get(), err.get(), s);
+        tc = knn_tc_candidates(data, n, dim, KCAP, ci.get(), cd.get(), norms.get(), err.get(), s, shard, rows, nrows);
         int h_err = 0;
         UMAPB_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
         UMAPB_SYNC(s);
         if (h_err != DEV_OK) fail(UMAPB_ERR_DEVICE_TIMEOUT, "tensor-core kNN: a pipeline wait gave up");
-        norm_max.zero(s);
-        norm_max_kernel<<<grid_for(n, 256, 1024), 256, 0, s>>>(n, norms.get(), norm_max.get());
-        UMAPB_LAUNCH_CHECK();
-    } else {
-        knn_bruteforce_kernel<float, float, KCAP><<<(n + KNN_BLOCK - 1) / KNN_BLOCK, KNN_BLOCK, 0, s>>>(
-            data, n, dim, nullptr, n, ci.get(), cd.get());
-        UMAPB_LAUNCH_CHECK();
+        if (tc) {
+            norm_max.zero(s);
+            norm_max_kernel<<<grid_for(n, 256, 1024), 256, 0, s>>>(n, norms.get(), norm_max.get());
+            UMAPB_LAUNCH_CHECK();
+            if (sharded) {
+                nq = *nrows;
+                queries = rows->get();
+            }
+        }
     }
-    DevArray<int32_t> redo(n, s), redo_count(1, s);
+    if (!tc) {
+        if (sharded) {   // contiguous data rows, CUDA-core candidates by slot
+            int32_t lo, hi;
+            shard_row_range(n, shard, lo, hi);
+            *nrows = hi - lo;
+            rows->allocate(std::max<int32_t>(hi - lo, 1), s);
+            if (hi > lo) {
+                iota_kernel<<<grid_for(hi - lo, 256), 256, 0, s>>>(hi - lo, lo, rows->get());
+                UMAPB_LAUNCH_CHECK();
+            }
+            nq = hi - lo;
+            queries = rows->get();
+            by_slot = true;
+        }
+        ci.allocate(static_cast<size_t>(std::max(nq, 1)) * KCAP, s);
+        cd.allocate(static_cast<size_t>(std::max(nq, 1)) * KCAP, s);
+        if (nq > 0) {
+            knn_bruteforce_kernel<float, float, KCAP><<<(nq + KNN_BLOCK - 1) / KNN_BLOCK, KNN_BLOCK, 0, s>>>(
+                data, n, dim, queries, nq, ci.get(), cd.get());
+            UMAPB_LAUNCH_CHECK();
+        }
+    }
+    DevArray<int32_t> redo(std::max(nq, 1), s), redo_count(1, s);
     redo_count.zero(s);
     DevArray<unsigned int> tc_err(1, s);
     tc_err.zero(s);
-    knn_rescore_kernel<KCAP><<<(n + 127) / 128, 128, 0, s>>>(data, n, dim, k, ci.get(), cd.get(), out_idx, out_dist,
-                                                             out_dist64, redo.get(), redo_count.get(),
-                                                             tc ? norms.get() : nullptr, norm_max.get(), TC_REL_BOUND,
-                                                             tc_err.get());
+    if (nq > 0) {
+        knn_rescore_kernel<KCAP><<<(nq + 127) / 128, 128, 0, s>>>(data, n, dim, k, queries, nq, by_slot ? 1 : 0, ci.get(),
+                                                                  cd.get(), out_idx, out_dist, out_dist64, redo.get(),
+                                                                  redo_count.get(), tc ? norms.get() : nullptr,
+                                                                  norm_max.get(), TC_REL_BOUND, tc_err.get());
+    }
     UMAPB_LAUNCH_CHECK();
     int32_t nredo = 0;
     unsigned int err_bits = 0;
@@ -380,7 +431,8 @@ void run_f32_batched(const float* data, const std::vector<int32_t>& inst, int32_
     redo_count.zero(s);
     DevArray<unsigned int> tc_err(1, s);
     tc_err.zero(s);
-    knn_rescore_kernel<KCAP><<<(n + 127) / 128, 128, 0, s>>>(data, n, dim, k, ci.get(), cd.get(), out_idx, out_dist,
+    knn_rescore_kernel<KCAP><<<(n + 127) / 128, 128, 0, s>>>(data, n, dim, k, nullptr, n, 0, ci.get(), cd.get(), out_idx,
+                                                             out_dist,
                                                              nullptr, redo.get(), redo_count.get(), norms.get(),
                                                              norm_max.get(), TC_REL_BOUND, tc_err.get());
     UMAPB_LAUNCH_CHECK();
@@ -444,6 +496,49 @@ template void knn_exact_batched<float>(const float*, const std::vector<int32_t>&
                                        cudaStream_t);
 template void knn_exact_batched<double>(const double*, const std::vector<int32_t>&, int32_t, int32_t, int32_t*,
                                         double*, cudaStream_t);
+
+template <typename T>
+void knn_exact_shard(const T* data, int32_t n, int32_t dim, int32_t k, KnnShard shard, int32_t* out_idx, T* out_dist,
+                     DevArray<int32_t>& rows, int32_t& nrows, cudaStream_t s) {
+    require(n >= 2, "the neighbour search needs at least two observations");
+    require(dim >= 1, "data_dim must be positive");
+    require(k >= 1 && k < n, "num_neighbors must be in [1, num_obs)");
+    require(k <= 120, "num_neighbors above 120 is not supported by the device search");
+    require(shard.count >= 1 && shard.index >= 0 && shard.index < shard.count, "shard must be in [0, num_shards)");
+    if (shard.count == 1) {
+        knn_exact<T>(data, n, dim, k, out_idx, out_dist, s);
+        rows.allocate(n, s);
+        iota_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, 0, rows.get());
+        UMAPB_LAUNCH_CHECK();
+        nrows = n;
+        return;
+    }
+    if constexpr (std::is_same<T, float>::value) {
+        if (k + 8 <= 16) run_f32<16>(data, n, dim, k, out_idx, out_dist, nullptr, s, shard, &rows, &nrows);
+        else if (k + 8 <= 24) run_f32<24>(data, n, dim, k, out_idx, out_dist, nullptr, s, shard, &rows, &nrows);
+        else if (k + 8 <= 32) run_f32<32>(data, n, dim, k, out_idx, out_dist, nullptr, s, shard, &rows, &nrows);
+        else if (k + 8 <= 64) run_f32<64>(data, n, dim, k, out_idx, out_dist, nullptr, s, shard, &rows, &nrows);
+        else run_f32<128>(data, n, dim, k, out_idx, out_dist, nullptr, s, shard, &rows, &nrows);
+    } else {
+        int32_t lo, hi;
+        shard_row_range(n, shard, lo, hi);
+        nrows = hi - lo;
+        rows.allocate(std::max<int32_t>(nrows, 1), s);
+        if (nrows > 0) {
+            iota_kernel<<<grid_for(nrows, 256), 256, 0, s>>>(nrows, lo, rows.get());
+            UMAPB_LAUNCH_CHECK();
+            if (k <= 16) run_f64<double, 16>(data, n, dim, k, rows.get(), nrows, out_idx, out_dist, nullptr, s);
+            else if (k <= 32) run_f64<double, 32>(data, n, dim, k, rows.get(), nrows, out_idx, out_dist, nullptr, s);
+            else if (k <= 64) run_f64<double, 64>(data, n, dim, k, rows.get(), nrows, out_idx, out_dist, nullptr, s);
+            else run_f64<double, 128>(data, n, dim, k, rows.get(), nrows, out_idx, out_dist, nullptr, s);
+        }
+    }
+}
+
+template void knn_exact_shard<float>(const float*, int32_t, int32_t, int32_t, KnnShard, int32_t*, float*,
+                                     DevArray<int32_t>&, int32_t&, cudaStream_t);
+template void knn_exact_shard<double>(const double*, int32_t, int32_t, int32_t, KnnShard, int32_t*, double*,
+                                      DevArray<int32_t>&, int32_t&, cudaStream_t);
 
 template <typename T>
 void knn_exact(const T* data, int32_t n, int32_t dim, int32_t k, int32_t* out_idx, T* out_dist, cudaStream_t s,

@@ -465,12 +465,15 @@ bool prune_enabled() {
 
 // FP16 search over the (pruned) tile lists of the instances 'inst'.
 void run_f16_pruned(const float* data, const std::vector<int32_t>& inst, int32_t dim, int kcap, float scale,
-                    int32_t* cand_idx, float* cand_d2, float* norms_by_row, int* d_err, cudaStream_t s) {
+                    int32_t* cand_idx, float* cand_d2, float* norms_by_row, int* d_err, cudaStream_t s,
+                    KnnShard shard = KnnShard(), DevArray<int32_t>* shard_rows = nullptr,
+                    int32_t* shard_count = nullptr) {
     const bool prune = prune_enabled();
     KnnTiles tiles;
     knn_tree_order(data, dim, inst, prune, tiles, s);
     KnnTasks tasks;
-    knn_tile_tasks(data, dim, tiles, inst, knn_tc16_query_tiles(dim), kcap, prune, tasks, s);
+    knn_tile_tasks(data, dim, tiles, inst, knn_tc16_query_tiles(dim), kcap, prune, tasks, s, shard);
+    if (shard_rows) knn_task_rows(tiles, tasks, inst.back(), *shard_rows, *shard_count, s);
     knn_tc16_run_tasks(data, dim, kcap, scale, tiles, tasks, cand_idx, cand_d2, norms_by_row, d_err, s,
                        &last_knn_kernel_ms());
     last_knn_tiles_scanned() = tasks.total_tiles;
@@ -500,18 +503,22 @@ static float f16_scale_or_zero(const float* data, size_t count, int32_t dim, int
 // Candidate lists (KCAP per query, FP32 squared distances, ascending) from the
 // tensor-core search; norms_out receives |x|^2 for the certainty bound of the
 // FP64 rescoring.
-void knn_tc_candidates(const float* data, int32_t n, int32_t dim, int kcap, int32_t* cand_idx, float* cand_d2,
-                       float* norms_out, int* d_err, cudaStream_t s) {
+bool knn_tc_candidates(const float* data, int32_t n, int32_t dim, int kcap, int32_t* cand_idx, float* cand_d2,
+                       float* norms_out, int* d_err, cudaStream_t s, KnnShard shard, DevArray<int32_t>* shard_rows,
+                       int32_t* shard_count) {
     require(knn_tc_supported(dim, kcap), "tensor-core kNN: unsupported dimension or candidate count");
     const int32_t n_pad = ((n + TC_M - 1) / TC_M) * TC_M;
     const float scale = f16_scale_or_zero(data, static_cast<size_t>(n) * dim, dim, kcap, s);
     if (scale > 0.0f) {
-        run_f16_pruned(data, {0, n}, dim, kcap, scale, cand_idx, cand_d2, norms_out, d_err, s);
-        return;
+        run_f16_pruned(data, {0, n}, dim, kcap, scale, cand_idx, cand_d2, norms_out, d_err, s, shard, shard_rows,
+                       shard_count);
+        return true;
     }
+    if (shard.count > 1) return false;   // the TF32 search covers every query: the caller shards by rows instead
     last_knn_tiles_scanned() = static_cast<int64_t>(n_pad / TC_M) * (n_pad / TC_N);
     run_candidates(data, n, dim, kcap, n_pad, nullptr, n_pad / TC_M, nullptr, nullptr, cand_idx, cand_d2, norms_out,
                    d_err, s);
+    return true;
 }
 
 // Batched: instance i is data rows [inst[i], inst[i + 1]); every query's

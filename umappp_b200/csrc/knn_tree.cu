@@ -418,7 +418,7 @@ void knn_tree_order(const float* data, int32_t dim, const std::vector<int32_t>& 
 }
 
 void knn_tile_tasks(const float* data, int32_t dim, const KnnTiles& t, const std::vector<int32_t>& inst, int qt,
-                    int32_t k, bool prune, KnnTasks& out, cudaStream_t s) {
+                    int32_t k, bool prune, KnnTasks& out, cudaStream_t s, KnnShard shard) {
     const int ninst = static_cast<int>(inst.size()) - 1;
     const int32_t ntiles = t.n_pad / TREE_LEAF;
     // every tile's instance tile range; CTAs of qt tiles within an instance
@@ -466,15 +466,71 @@ void knn_tile_tasks(const float* data, int32_t dim, const KnnTiles& t, const std
         for (int x = 0; x < tasks[j].z; ++x) w += hc[tasks[j].y + x];
         work[j] = w;
     }
+    if (shard.count > 1) {
+        // this shard's tasks: a contiguous range (tree order) holding an equal
+        // share of the work, cut where the running total crosses index / count
+        int64_t total = 0;
+        for (int64_t w : work) total += w;
+        std::vector<int4> kept;
+        std::vector<int64_t> kept_work;
+        int64_t run = 0;
+        for (size_t j = 0; j < tasks.size(); ++j) {
+            const int64_t mid = run + work[j] / 2;   // the task belongs to the shard its midpoint falls in
+            const int32_t owner = total > 0 ? static_cast<int32_t>(std::min<int64_t>(shard.count - 1, mid * shard.count / total))
+                                            : static_cast<int32_t>(j * shard.count / std::max<size_t>(tasks.size(), 1));
+            run += work[j];
+            if (owner == shard.index) {
+                kept.push_back(tasks[j]);
+                kept_work.push_back(work[j]);
+            }
+        }
+        tasks.swap(kept);
+        work.swap(kept_work);
+        out.total_tiles = 0;
+        for (int64_t w : work) out.total_tiles += w;
+    }
     std::vector<int32_t> order(tasks.size());
     for (size_t j = 0; j < order.size(); ++j) order[j] = static_cast<int32_t>(j);
     std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return work[x] > work[y]; });
     std::vector<int4> sorted(tasks.size());
     for (size_t j = 0; j < order.size(); ++j) sorted[j] = tasks[order[j]];
     out.count = static_cast<int32_t>(sorted.size());
+    out.host_tasks = sorted;
     out.tasks.allocate(std::max<size_t>(sorted.size(), 1), s);
     UMAPB_CUDA(cudaMemcpyAsync(out.tasks.get(), sorted.data(), sorted.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
     UMAPB_SYNC(s);   // host vectors above
+}
+
+namespace {
+__global__ void task_rows_flag_kernel(const int4* __restrict__ tasks, const int32_t* __restrict__ row_map,
+                                      int32_t n_pad, uint8_t* __restrict__ flag) {
+    const int4 tk = tasks[blockIdx.x];
+    const int32_t end = min(n_pad, tk.x + TREE_LEAF * tk.z);
+    for (int32_t r = tk.x + threadIdx.x; r < end; r += blockDim.x) {
+        const int32_t d = row_map[r];
+        if (d >= 0) flag[d] = 1;
+    }
+}
+}  // namespace
+
+void knn_task_rows(const KnnTiles& t, const KnnTasks& tk, int32_t n, DevArray<int32_t>& rows, int32_t& count,
+                   cudaStream_t s) {
+    DevArray<uint8_t> flag(n, s);
+    UMAPB_CUDA(cudaMemsetAsync(flag.get(), 0, static_cast<size_t>(n), s));
+    if (tk.count > 0) {
+        task_rows_flag_kernel<<<static_cast<unsigned>(tk.count), 128, 0, s>>>(tk.tasks.get(), t.row_map.get(), t.n_pad,
+                                                                             flag.get());
+        UMAPB_LAUNCH_CHECK();
+    }
+    rows.allocate(std::max<int32_t>(n, 1), s);
+    DevArray<int32_t> d_count(1, s);
+    cub::CountingInputIterator<int32_t> it(0);
+    size_t tb = 0;
+    UMAPB_CUDA(cub::DeviceSelect::Flagged(nullptr, tb, it, flag.get(), rows.get(), d_count.get(), n, s));
+    DevArray<unsigned char> temp(tb, s);
+    UMAPB_CUDA(cub::DeviceSelect::Flagged(temp.get(), tb, it, flag.get(), rows.get(), d_count.get(), n, s));
+    UMAPB_CUDA(cudaMemcpyAsync(&count, d_count.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    UMAPB_SYNC(s);
 }
 
 }  // namespace umapb

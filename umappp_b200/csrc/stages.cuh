@@ -36,18 +36,33 @@ struct DeviceEpochs {
 };
 
 // ---- kNN (knn.cu) ----------------------------------------------------------
+// The shard of a neighbour search split across ranks: shard 'index' of
+// 'count' takes a contiguous range of the query tiles in tree order with an
+// equal share of the tile pairs (count 1: everything).
+struct KnnShard {
+    int32_t index = 0, count = 1;
+};
 // Exact Euclidean neighbours: out_idx/out_dist are n x k row-major, sorted by
 // (distance, index), self excluded.  Float data: FP32 candidate search then
 // FP64 rescoring of the candidate set; double data: FP64 throughout.
 template <typename T>
 void knn_exact(const T* data, int32_t n, int32_t dim, int32_t k, int32_t* out_idx, T* out_dist, cudaStream_t s,
                double* out_dist_f64 = nullptr);
+// The shard's part of knn_exact: its queries' data rows in rows[0, nrows)
+// (ascending), their neighbours at those rows of out_idx / out_dist.
+template <typename T>
+void knn_exact_shard(const T* data, int32_t n, int32_t dim, int32_t k, KnnShard shard, int32_t* out_idx, T* out_dist,
+                     DevArray<int32_t>& rows, int32_t& nrows, cudaStream_t s);
 
 // Tensor-core candidate search (knn_tc.cu): KCAP candidates per query with
 // FP32 squared distances; norms_out receives |x|^2 (n rounded up to 128 entries).
 bool knn_tc_supported(int32_t dim, int kcap);
-void knn_tc_candidates(const float* data, int32_t n, int32_t dim, int kcap, int32_t* cand_idx, float* cand_d2,
-                       float* norms_out, int* d_err, cudaStream_t s);
+// With a shard (count > 1): only the shard's queries (their data rows in
+// *shard_rows, *shard_count of them); returns false, computing nothing, when
+// the search in use cannot be sharded.
+bool knn_tc_candidates(const float* data, int32_t n, int32_t dim, int kcap, int32_t* cand_idx, float* cand_d2,
+                       float* norms_out, int* d_err, cudaStream_t s, KnnShard shard = KnnShard(),
+                       DevArray<int32_t>* shard_rows = nullptr, int32_t* shard_count = nullptr);
 // Batched: instance i is data rows [inst[i], inst[i + 1]) (host vector).
 void knn_tc_candidates_batched(const float* data, const std::vector<int32_t>& inst, int32_t dim, int kcap,
                                int32_t* cand_idx, float* cand_d2, int* d_err, cudaStream_t s);
@@ -68,7 +83,12 @@ struct KnnTasks {
     DevArray<int32_t> tile_list;
     int32_t count = 0;
     int64_t total_tiles = 0;       // sum of the query tiles' list lengths
+    std::vector<int4> host_tasks;  // the tasks, in launch order
 };
+// Data rows of the query tiles of a task list (ascending): the rows a sharded
+// search computes.
+void knn_task_rows(const KnnTiles& t, const KnnTasks& tk, int32_t n, DevArray<int32_t>& rows, int32_t& count,
+                   cudaStream_t s);
 // tree == false keeps each instance in data order.
 void knn_tree_order(const float* data, int32_t dim, const std::vector<int32_t>& inst, bool tree, KnnTiles& out,
                     cudaStream_t s);
@@ -76,7 +96,7 @@ void knn_tree_order(const float* data, int32_t dim, const std::vector<int32_t>& 
 // of its rows' k nearest neighbours (all of them when prune is false); CTAs
 // take qt consecutive query tiles of one instance.
 void knn_tile_tasks(const float* data, int32_t dim, const KnnTiles& t, const std::vector<int32_t>& inst, int qt,
-                    int32_t k, bool prune, KnnTasks& out, cudaStream_t s);
+                    int32_t k, bool prune, KnnTasks& out, cudaStream_t s, KnnShard shard = KnnShard());
 // Candidate search over tree-ordered operands and task lists; candidate and
 // norm outputs are indexed by data row.
 void knn_tc16_run_tasks(const float* data, int32_t dim, int kcap, float scale, const KnnTiles& tiles,
