@@ -2,29 +2,36 @@
 // points and, per block of queries, the reference tiles that can hold one of
 // its neighbours.
 //
-// Ordering (random-projection tree): the points of every instance are split
-// recursively -- projected on the difference of two of the segment's own
-// points, sorted by the projection, cut so that the left part is a whole
-// number of 128-row tiles -- until each segment is one tile.  Clustered data
-// (single-cell profiles, mixtures) then come out with tiles that each sit in
-// one cluster.
+// Ordering (projection tree): the points of every instance are split
+// recursively -- projected on the direction from a random point of the
+// segment to the segment's point farthest from it, sorted by the projection,
+// cut at a wide gap of the projections if there is one (a hard cut: the two
+// sides go to separate padded runs of tiles) and otherwise so that the left
+// part is a whole number of 128-row tiles -- until each segment is one tile.
+// The farthest point of a segment that spans several clusters lies in
+// another cluster than the random one, so the direction separates clusters,
+// and clustered data (single-cell profiles, mixtures) come out with tiles that
+// each sit in one cluster.
 //
 // Bounds: every 128-row reference tile T and every query block B (the rows one
 // CTA of the search serves) gets a centroid c (FP32) and a radius R (an upper
 // bound of |x - c| over its points, FP64 rounded up).  For a query q in B and a
 // point r in T the triangle inequality gives
 //     |q - r| >= |c_B - c_T| - R_B - R_T =: lb(B, T),
-// and every query of B has at least (|B| - 1) other points of B within 2 R_B.
-// If |B| - 1 >= k, the k-th neighbour of q is therefore within 2 R_B, and a
-// tile with lb(B, T) > 2 R_B cannot hold any of q's k nearest neighbours: it
-// is left out of B's list.  This is exact (no neighbour is lost); for data
-// without cluster structure the lists simply cover every tile.
+// and the k-th neighbour of every query q of B lies within a radius rho_B of q
+// -- the largest over B's queries of the distance to the k-th nearest other
+// point of B (computed exactly, rounded up; it needs |B| - 1 >= k), or a bound
+// through a nearby tile.  A tile with lb(B, T) > rho_B cannot hold any of
+// q's k nearest neighbours: it is left out of B's list.  This is exact (no
+// neighbour is lost); for data without cluster structure the lists simply
+// cover every tile.
 #include <cub/cub.cuh>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "stages.cuh"
@@ -74,6 +81,63 @@ __global__ void rp_keys_kernel(const float* __restrict__ data, int32_t dim, int3
     }
 }
 
+// The window of a segment of len points in which a hard cut may fall.
+__host__ __device__ __forceinline__ int32_t gap_window_first(int32_t len) { return len / 16 > 1 ? len / 16 : 1; }
+__host__ __device__ __forceinline__ int32_t gap_window_last(int32_t len) { return (15 * len) / 16; }
+
+// best[seg] = max(best[seg], key) for every lane of the warp, with one atomic
+// per run of lanes that share a segment (seg < 0: nothing).  The lanes' items
+// are consecutive, so equal segments form runs: a segmented max down each run
+// leaves the run's maximum in its first lane.  All 32 lanes take part.
+__device__ __forceinline__ void warp_segment_max(unsigned long long* __restrict__ best, int seg,
+                                                 unsigned long long key) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long k2 = __shfl_down_sync(0xffffffffu, key, o);
+        const int s2 = __shfl_down_sync(0xffffffffu, seg, o);
+        if (lane + o < 32 && s2 == seg && k2 > key) key = k2;
+    }
+    const int prev = __shfl_up_sync(0xffffffffu, seg, 1);
+    if (seg >= 0 && (lane == 0 || prev != seg)) atomicMax(&best[seg], key);
+}
+
+// The point of every active segment farthest from its point a (squared FP32
+// distance): each position folds (distance bits, reversed position) into its
+// segment's 64-bit maximum, so that ties go to the smallest position.  The
+// loop runs whole warps (warp_segment_max).
+__global__ void far_point_kernel(const float* __restrict__ data, int32_t dim, int32_t n,
+                                 const int32_t* __restrict__ perm, int32_t nseg, const int32_t* __restrict__ seg_start,
+                                 const int32_t* __restrict__ seg_a, unsigned long long* __restrict__ best) {
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int64_t base = static_cast<int64_t>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        const int32_t p = static_cast<int32_t>(base + (threadIdx.x & 31));
+        int seg = -1;
+        unsigned long long key = 0;
+        if (p < n) {
+            int lo = 0, hi = nseg - 1;   // segment of position p: last start <= p
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (seg_start[mid] <= p) lo = mid; else hi = mid - 1;
+            }
+            const int32_t a = seg_a[lo];
+            if (a >= 0) {
+                const float* x = data + static_cast<size_t>(perm[p]) * dim;
+                const float* xa = data + static_cast<size_t>(perm[a]) * dim;
+                float d2 = 0.0f;
+                for (int d = 0; d < dim; ++d) {
+                    const float v = x[d] - xa[d];
+                    d2 = fmaf(v, v, d2);
+                }
+                seg = lo;
+                key = (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) |
+                      static_cast<unsigned long long>(0xffffffffu - static_cast<uint32_t>(p));
+            }
+        }
+        warp_segment_max(best, seg, key);
+    }
+}
+
 __device__ __forceinline__ float sorted_key(const unsigned long long* __restrict__ keys, int64_t p) {
     return order_bits_float(static_cast<uint32_t>(keys[p] & 0xffffffffull));
 }
@@ -82,26 +146,34 @@ __global__ void iota_kernel(int32_t* __restrict__ v, int32_t n) {
     for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = i;
 }
 
-// Widest gap between consecutive sorted keys with the cut in the middle half
-// of each active segment j ([start + len/4, start + 3 len/4]): every position
-// of every middle half folds (gap bits, reversed position) into its segment's
+// Widest gap between consecutive sorted keys with the cut in the window
+// [start + len/16, start + 15 len/16] of each active segment j: every position
+// of every window folds (gap bits, reversed position) into its segment's
 // 64-bit maximum, so that ties go to the smallest position.
 __global__ void widest_gap_kernel(const unsigned long long* __restrict__ keys, int32_t nact,
                                   const int32_t* __restrict__ seg_start,
                                   const int32_t* __restrict__ seg_end, const int64_t* __restrict__ mid_off,
                                   int64_t total, unsigned long long* __restrict__ best) {
-    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x) {
-        int lo = 0, hi = nact - 1;   // segment of middle-half item i: last offset <= i
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (mid_off[mid] <= i) lo = mid; else hi = mid - 1;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int64_t base = static_cast<int64_t>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31); base < total;
+         base += stride) {   // whole warps (warp_segment_max)
+        const int64_t i = base + (threadIdx.x & 31);
+        int seg = -1;
+        unsigned long long key = 0;
+        if (i < total) {
+            int lo = 0, hi = nact - 1;   // segment of window item i: last offset <= i
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (mid_off[mid] <= i) lo = mid; else hi = mid - 1;
+            }
+            const int32_t st = seg_start[lo], len = seg_end[lo] - st;
+            const int32_t p = st + gap_window_first(len) + static_cast<int32_t>(i - mid_off[lo]);
+            const float g = fmaxf(sorted_key(keys, p) - sorted_key(keys, p - 1), 0.0f);
+            seg = lo;
+            key = (static_cast<unsigned long long>(__float_as_uint(g)) << 32) |
+                  static_cast<unsigned long long>(0xffffffffu - static_cast<uint32_t>(p - st));
         }
-        const int32_t st = seg_start[lo], len = seg_end[lo] - st;
-        const int32_t p = st + max(1, len / 4) + static_cast<int32_t>(i - mid_off[lo]);
-        const float g = fmaxf(sorted_key(keys, p) - sorted_key(keys, p - 1), 0.0f);
-        const unsigned long long key = (static_cast<unsigned long long>(__float_as_uint(g)) << 32) |
-                                       static_cast<unsigned long long>(0xffffffffu - static_cast<uint32_t>(p - st));
-        atomicMax(&best[lo], key);
+        warp_segment_max(best, seg, key);
     }
 }
 
@@ -181,6 +253,69 @@ __global__ void group_bounds_kernel(const float* __restrict__ data, int32_t dim,
     }
 }
 
+constexpr int KTH_MAX = 32;
+constexpr float D2_LOW = 1.0f - 1.0e-4f;    // lower-bound factor on FP32 squared distances
+constexpr float D2_HIGH = 1.0f + 1.0e-4f;   // upper-bound factor
+
+// For every tile g: a distance within which each of its points has at least k
+// other points of the tile -- the largest over the tile's points of the
+// distance to the k-th nearest other point (FP32 sums of squares, relative
+// error below (dim + 2) 2^-24, rounded up through the D2_HIGH margins) --, or
+// infinity when the tile holds k points or fewer or k exceeds KTH_MAX.
+// One block of TREE_LEAF threads per tile, one thread per row; the tile's
+// points are staged in shared memory ([TREE_LEAF][dim]).
+__global__ void __launch_bounds__(TREE_LEAF)
+    tile_kth_kernel(const float* __restrict__ data, int32_t dim, const int32_t* __restrict__ row_map,
+                    const int32_t* __restrict__ count, int32_t k, float* __restrict__ kth_out) {
+    extern __shared__ float pts[];
+    __shared__ int valid[TREE_LEAF];
+    __shared__ float red[TREE_LEAF / 32];
+    const int32_t g = blockIdx.x;
+    const int r = threadIdx.x;
+    if (k > KTH_MAX || count[g] < k + 1) {   // uniform over the block
+        if (r == 0) kth_out[g] = CUDART_INF_F;
+        return;
+    }
+    const int32_t* rows = row_map + static_cast<size_t>(g) * TREE_LEAF;
+    valid[r] = rows[r] >= 0;
+    for (int i = r; i < TREE_LEAF * dim; i += TREE_LEAF) {
+        const int rr = i / dim;
+        const int32_t src = rows[rr];
+        pts[i] = src >= 0 ? data[static_cast<size_t>(src) * dim + (i - rr * dim)] : 0.0f;
+    }
+    __syncthreads();
+    float top[KTH_MAX];   // the smallest squared distances so far, ascending
+#pragma unroll
+    for (int i = 0; i < KTH_MAX; ++i) top[i] = CUDART_INF_F;
+    float kth2 = 0.0f;
+    if (valid[r]) {
+        const float* x = pts + r * dim;
+        for (int j = 0; j < TREE_LEAF; ++j) {
+            if (j == r || !valid[j]) continue;
+            const float* y = pts + j * dim;
+            float d2 = 0.0f;
+            for (int d = 0; d < dim; ++d) {
+                const float v = x[d] - y[d];
+                d2 = fmaf(v, v, d2);
+            }
+#pragma unroll
+            for (int i = KTH_MAX - 1; i > 0; --i) top[i] = d2 < top[i - 1] ? top[i - 1] : fminf(top[i], d2);
+            top[0] = fminf(top[0], d2);
+        }
+#pragma unroll
+        for (int i = 0; i < KTH_MAX; ++i)
+            if (i == k - 1) kth2 = top[i];
+    }
+    for (int o = 16; o > 0; o >>= 1) kth2 = fmaxf(kth2, __shfl_xor_sync(0xffffffffu, kth2, o));
+    if ((r & 31) == 0) red[r >> 5] = kth2;
+    __syncthreads();
+    if (r == 0) {
+        float m = red[0];
+        for (int w = 1; w < TREE_LEAF / 32; ++w) m = fmaxf(m, red[w]);
+        kth_out[g] = sqrtf(m * D2_HIGH) * D2_HIGH;
+    }
+}
+
 // Squared distance between the centroid cb (shared memory) and tile t's
 // centroid, read from the [dim][tiles] copy ct (coalesced across a warp), in
 // FP32: relative error below dim * 2^-23, covered by the margins below.
@@ -197,19 +332,19 @@ __device__ __forceinline__ float centroid_d2(const float* __restrict__ cb, const
 // One warp per query tile b (tiles [t0, t0 + nt) of its instance).
 // Radius rho of b's k-neighbourhoods: every query q of b has at least k other
 // points within rho --
-//   2 R_b                                if b holds k + 1 or more points,
+//   kth_b (tile_kth_kernel)              if b holds k + 1 or more points,
+//   2 R_b                                likewise (never below kth_b),
 //   R_b + |c_b - c_w| + R_w (upper)      for any tile w with k + 1 or more points,
 // the smallest of these (infinite if none applies).  Tile t is needed unless
 // |c_b - c_t| - R_b - R_t > rho.  The needed tiles are written in ascending
 // order from lists[slot[b]] (room for nt entries), their number to counts[b].
 constexpr int LIST_WARPS = 8;
 constexpr int MAX_TREE_DIM = 128;
-constexpr float D2_LOW = 1.0f - 1.0e-4f;    // lower-bound factor on FP32 squared distances
-constexpr float D2_HIGH = 1.0f + 1.0e-4f;   // upper-bound factor
 __global__ void __launch_bounds__(32 * LIST_WARPS)
     tile_lists_kernel(int32_t nq, const int32_t* __restrict__ q_tile0, const int32_t* __restrict__ q_ntiles,
                       const float* __restrict__ ct, int32_t ntiles, const float* __restrict__ tr,
-                      const int32_t* __restrict__ tcount, int32_t dim, int32_t k, bool prune,
+                      const int32_t* __restrict__ tcount, const float* __restrict__ tkth, int32_t dim, int32_t k,
+                      bool prune,
                       const int64_t* __restrict__ slot, int32_t* __restrict__ counts, int32_t* __restrict__ lists) {
     __shared__ float cbs[LIST_WARPS][MAX_TREE_DIM];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -220,7 +355,7 @@ __global__ void __launch_bounds__(32 * LIST_WARPS)
     __syncwarp();
     const int32_t t0 = q_tile0[b], nt = q_ntiles[b];
     const float rb = tr[b];
-    float rho = (tcount[b] >= k + 1) ? 2.0f * rb : CUDART_INF_F;
+    float rho = (tcount[b] >= k + 1) ? (tkth ? fminf(2.0f * rb, tkth[b]) : 2.0f * rb) : CUDART_INF_F;
     if (prune) {
         for (int32_t base = 0; base < nt; base += 32) {
             const int32_t w = t0 + base + lane;
@@ -272,13 +407,14 @@ void knn_tree_order(const float* data, int32_t dim, const std::vector<int32_t>& 
     std::vector<Seg> seg(ninst);
     for (int i = 0; i < ninst; ++i) seg[i] = {inst[i], inst[i + 1] - inst[i], true};
     uint64_t h = 0x9E3779B97F4A7C15ull;
-    auto next = [&h]() {   // splitmix64: the choice of the two direction points
+    auto next = [&h]() {   // splitmix64: the choice of the direction's first point
         uint64_t z = (h += 0x9E3779B97F4A7C15ull);
         z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
         z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
         return z ^ (z >> 31);
     };
     DevArray<int32_t> d_start, d_end, d_a, d_b;
+    DevArray<unsigned long long> d_far;
     for (int level = 0; tree && level < 64; ++level) {
         const int nseg = static_cast<int>(seg.size());
         std::vector<int32_t> st(nseg), en(nseg), a(nseg, -1), b(nseg, -1);
@@ -289,7 +425,6 @@ void knn_tree_order(const float* data, int32_t dim, const std::vector<int32_t>& 
             if (seg[g].len > TREE_LEAF) {
                 act.push_back(g);
                 a[g] = st[g] + static_cast<int32_t>(next() % static_cast<uint64_t>(seg[g].len));
-                b[g] = st[g] + static_cast<int32_t>(next() % static_cast<uint64_t>(seg[g].len));
             }
         }
         if (act.empty()) break;
@@ -297,9 +432,22 @@ void knn_tree_order(const float* data, int32_t dim, const std::vector<int32_t>& 
         d_end.reserve(nseg, s);
         d_a.reserve(nseg, s);
         d_b.reserve(nseg, s);
+        d_far.reserve(nseg, s);
         UMAPB_CUDA(cudaMemcpyAsync(d_start.get(), st.data(), nseg * sizeof(int32_t), cudaMemcpyHostToDevice, s));
         UMAPB_CUDA(cudaMemcpyAsync(d_end.get(), en.data(), nseg * sizeof(int32_t), cudaMemcpyHostToDevice, s));
         UMAPB_CUDA(cudaMemcpyAsync(d_a.get(), a.data(), nseg * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+        // b: the segment's point farthest from a
+        UMAPB_CUDA(cudaMemsetAsync(d_far.get(), 0, nseg * sizeof(unsigned long long), s));
+        far_point_kernel<<<grid_for(n, 256), 256, 0, s>>>(data, dim, n, perm.get(), nseg, d_start.get(), d_a.get(),
+                                                          d_far.get());
+        UMAPB_LAUNCH_CHECK();
+        std::vector<unsigned long long> far(nseg);
+        UMAPB_CUDA(cudaMemcpyAsync(far.data(), d_far.get(), nseg * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+        UMAPB_SYNC(s);   // also: st, en and a above are the copies' sources
+        for (int g : act) {
+            const int32_t p = static_cast<int32_t>(0xffffffffu - static_cast<uint32_t>(far[g] & 0xffffffffu));
+            b[g] = (far[g] != 0 && p >= st[g] && p < en[g]) ? p : st[g] + static_cast<int32_t>(next() % static_cast<uint64_t>(seg[g].len));
+        }
         UMAPB_CUDA(cudaMemcpyAsync(d_b.get(), b.data(), nseg * sizeof(int32_t), cudaMemcpyHostToDevice, s));
         rp_keys_kernel<<<grid_for(n, 256), 256, 0, s>>>(data, dim, n, perm.get(), nseg, d_start.get(), d_a.get(),
                                                         d_b.get(), keys.get());
@@ -324,7 +472,7 @@ void knn_tree_order(const float* data, int32_t dim, const std::vector<int32_t>& 
             ast[j] = st[act[j]];
             aen[j] = en[act[j]];
             const int32_t len = aen[j] - ast[j];
-            moff[j + 1] = moff[j] + ((3 * len) / 4 - std::max(1, len / 4) + 1);
+            moff[j + 1] = moff[j] + (gap_window_last(len) - gap_window_first(len) + 1);
         }
         DevArray<int32_t> d_ast(nact, s), d_aen(nact, s);
         DevArray<int64_t> d_moff(nact + 1, s);
@@ -450,9 +598,22 @@ void knn_tile_tasks(const float* data, int32_t dim, const KnnTiles& t, const std
     UMAPB_CUDA(cudaMemcpyAsync(d_ntl.get(), ntl.data(), ntiles * sizeof(int32_t), cudaMemcpyHostToDevice, s));
     UMAPB_CUDA(cudaMemcpyAsync(out.qlist_off.get(), ho.data(), ntiles * sizeof(int64_t), cudaMemcpyHostToDevice, s));
     const unsigned warps_grid = static_cast<unsigned>((ntiles + LIST_WARPS - 1) / LIST_WARPS);
+    DevArray<float> tkth;
+    if (prune && k <= KTH_MAX) {
+        tkth.allocate(ntiles, s);
+        const size_t smem = sizeof(float) * TREE_LEAF * dim;   // dim <= MAX_TREE_DIM: 64 KB at most
+        static std::once_flag once;
+        std::call_once(once, [] {
+            UMAPB_CUDA(cudaFuncSetAttribute(tile_kth_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            static_cast<int>(sizeof(float) * TREE_LEAF * MAX_TREE_DIM)));
+        });
+        tile_kth_kernel<<<ntiles, TREE_LEAF, smem, s>>>(data, dim, t.row_map.get(), tcnt.get(), k, tkth.get());
+        UMAPB_LAUNCH_CHECK();
+    }
     tile_lists_kernel<<<warps_grid, 32 * LIST_WARPS, 0, s>>>(ntiles, d_tile0.get(), d_ntl.get(), tcen_t.get(), ntiles,
-                                                             trad.get(), tcnt.get(), dim, k, prune, out.qlist_off.get(),
-                                                             out.qlist_len.get(), out.tile_list.get());
+                                                             trad.get(), tcnt.get(), tkth.get(), dim, k, prune,
+                                                             out.qlist_off.get(), out.qlist_len.get(),
+                                                             out.tile_list.get());
     UMAPB_LAUNCH_CHECK();
     std::vector<int32_t> hc(ntiles);
     UMAPB_CUDA(cudaMemcpyAsync(hc.data(), out.qlist_len.get(), ntiles * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
