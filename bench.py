@@ -417,6 +417,102 @@ def run_reference(args, rank: int) -> dict | None:
             "cpu_baseline": cb, "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def trustworthiness_dev(X: np.ndarray, Y: np.ndarray, k: int, queries: np.ndarray, batch: int = 8) -> float:
+    """Trustworthiness(k) of layout Y for data X over the query rows (FP64
+    squared distances, ranks with ties broken by index, the whole data set as
+    candidates), computed with torch on the GPU: a layout-quality measure."""
+    import torch
+
+    n = X.shape[0]
+    Xd = torch.as_tensor(np.ascontiguousarray(X), device="cuda").to(torch.float64)
+    Yd = torch.as_tensor(np.ascontiguousarray(Y), device="cuda").to(torch.float64)
+    ar = torch.arange(n, device="cuda")
+    total = 0.0
+    for s in range(0, len(queries), batch):
+        qi = torch.as_tensor(queries[s:s + batch], device="cuda", dtype=torch.long)
+        rows = torch.arange(len(qi), device="cuda")
+        dX = ((Xd[None, :, :] - Xd[qi][:, None, :]) ** 2).sum(-1)
+        dY = ((Yd[None, :, :] - Yd[qi][:, None, :]) ** 2).sum(-1)
+        dY[rows, qi] = float("inf")
+        cand = torch.sort(torch.topk(dY, min(k + 8, n - 1), dim=1, largest=False).indices, dim=1).values
+        nb = torch.gather(cand, 1, torch.argsort(torch.gather(dY, 1, cand), dim=1, stable=True))[:, :k]
+        dj = torch.gather(dX, 1, nb)
+        for t in range(k):
+            closer = (dX < dj[:, t:t + 1]) | ((dX == dj[:, t:t + 1]) & (ar[None, :] < nb[:, t:t + 1]))
+            closer[rows, qi] = False
+            total += float(torch.clamp(closer.sum(1) + 1 - k, min=0).sum())
+    return 1.0 - 2.0 / (len(queries) * k * (2.0 * n - 3.0 * k - 1.0)) * total
+
+
+def precision_study(cfg: str) -> dict:
+    """Per-stage error of the FP32 path against the FP64 device path on the
+    benchmark workload (same data, rounded once to float32):
+    - kNN: the 3xFP16 (default) and 3xTF32 tensor-core searches on float32
+      data against the FP64 search of the same points: rows and entries with
+      the same neighbour indices, largest relative distance error;
+    - similarities, union, schedule: float32 and float64 runs of each stage on
+      the same FP64 neighbour lists: largest relative weight difference, edge
+      counts, largest relative epochs_per_sample difference;
+    - layout: the full float32 pipeline (FP32 2-d SGD kernel) and the full
+      float64 pipeline (FP64 generic kernel), each scored by the fuzzy
+      cross-entropy over the FP64 union graph (device loss, with its constant)
+      and trustworthiness (k = 15, 10,000 seeded queries)."""
+    import umappp_b200 as U
+
+    n, dim, _, _, _, k, epochs = CONFIGS[cfg]
+    X32 = make_data(cfg)
+    X64 = X32.astype(np.float64)
+    out = {"workload": cfg}
+    t0 = time.time()
+    idx64, d64 = U.knn(X64, k)
+    out["knn_fp64_s"] = round(time.time() - t0, 2)
+    knn = {}
+    for kind, env in (("fp16x3", None), ("tf32x3", "tf32")):
+        if env:
+            os.environ["UMAPB_KNN_TC_KIND"] = env
+        try:
+            t0 = time.time()
+            idx, d = U.knn(X32, k)
+            secs = time.time() - t0
+        finally:
+            os.environ.pop("UMAPB_KNN_TC_KIND", None)
+        rel = np.abs(d.astype(np.float64) - d64) / np.maximum(d64, 1e-300)
+        knn[kind] = {"rows_equal": round(float(np.mean(np.all(idx == idx64, axis=1))), 6),
+                     "entries_equal": round(float(np.mean(idx == idx64)), 7),
+                     "max_rel_distance_error": float(rel[idx == idx64].max()), "seconds": round(secs, 2)}
+    out["knn"] = knn
+    nl32 = (idx64, d64.astype(np.float32))
+    p, i, w32 = U.neighbor_similarities(nl32)
+    _, _, w64 = U.neighbor_similarities((idx64, d64))
+    out["similarities_max_rel_error"] = float(np.max(np.abs(w32 - w64) / np.maximum(w64, 1e-300)))
+    g32 = U.combine_neighbor_sets((p, i, w32))
+    g64 = U.combine_neighbor_sets((p, i, w64))
+    e32 = U.similarities_to_epochs(g32, epochs, 5.0)
+    e64 = U.similarities_to_epochs(g64, epochs, 5.0)
+    same = (len(e32.edge_targets) == len(e64.edge_targets) and np.array_equal(e32.edge_targets, e64.edge_targets))
+    out["union_edges"] = {"fp32": int(len(g32[1])), "fp64": int(len(g64[1]))}
+    out["schedule"] = {"edges_fp32": int(len(e32.edge_targets)), "edges_fp64": int(len(e64.edge_targets)),
+                       "same_edges": bool(same)}
+    if same:
+        out["schedule"]["max_rel_epochs_per_sample_error"] = float(np.max(
+            np.abs(e32.epochs_per_sample.astype(np.float64) - e64.epochs_per_sample) / e64.epochs_per_sample))
+    a, b = U.find_ab(1.0, 0.1)
+    queries = np.sort(np.random.default_rng(123).choice(n, size=min(10000, n), replace=False))
+    layout = {}
+    for name, X, dt in (("fp32", X32, np.float32), ("fp64", X64, np.float64)):
+        Y = np.zeros((n, 2), dt)
+        st = U.initialize_from_data(X, 2, Y, U.Options(num_neighbors=k, num_epochs=epochs))
+        st.run(Y)
+        ms = st.stage_ms()
+        ce = U.loss_grad(g64, Y.astype(np.float64), a, b, with_constant=True)[0]
+        layout[name] = {"cross_entropy": ce, "trustworthiness": round(trustworthiness_dev(X64, Y, 15, queries), 6),
+                        "sgd_ms": round(ms["sgd"], 1), "knn_ms": round(ms["knn"], 1)}
+    layout["fp32_vs_fp64_cross_entropy"] = round(
+        (layout["fp32"]["cross_entropy"] - layout["fp64"]["cross_entropy"]) / layout["fp64"]["cross_entropy"], 6)
+    out["layout"] = layout
+    return out
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -426,7 +522,13 @@ def main() -> None:
     ap.add_argument("--config", default="mixture_1m", choices=sorted(CONFIGS) + ["batch64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batch64 sub-object of the default line")
+    ap.add_argument("--precision-study", action="store_true",
+                    help="print the per-stage FP32-vs-FP64 comparison on the workload and exit")
+    ap.add_argument("--no-precision", action="store_true", help="skip the precision sub-object of the default line")
     args = ap.parse_args()
+    if args.precision_study:
+        print(json.dumps({"precision_study": precision_study(args.config)}), flush=True)
+        return
 
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -453,6 +555,9 @@ def main() -> None:
             out["batch64"] = {k_: b[k_] for k_ in ("value", "unit", "sequential_plain_s", "speedup_vs_sequential",
                                                    "gpu_launches", "sequential_gpu_launches")}
             out["batch64"]["workload"] = b["config"]["workload"]
+        if world == 1 and args.config == "mixture_1m" and not args.no_precision and out is not None:
+            # per-stage error of the FP32 path against the FP64 device path (after the timed region)
+            out["precision"] = precision_study(args.config)
         if rank == 0 and out is not None:
             if world == 1 and not args.no_cpu_baseline and args.config != "batch64":
                 out["cpu_baseline"] = cpu_sample(args.config)

@@ -259,6 +259,34 @@ int umapb_knn_shard(int dtype, size_t data_dim, int32_t num_obs, const void* dat
 int umapb_knn(int dtype, size_t data_dim, int32_t num_obs, const void* data, int k, int32_t* out_indices,
               void* out_distances);
 
+/* Exact Euclidean neighbours of num_query query points among num_ref reference
+ * points (row-major data_dim columns each): out_indices / out_distances are
+ * num_query x k, reference indices sorted by (distance, index).  The
+ * knncolle search of initialize.hpp:138-142 with the query and reference sets
+ * apart (the search the transform below makes). */
+int umapb_knn_query(int dtype, size_t data_dim, int32_t num_ref, const void* ref_data, int32_t num_query,
+                    const void* query_data, int k, int32_t* out_indices, void* out_distances);
+
+/* Out-of-sample embedding (an extension: the reference has no transform).
+ * new_embedding (num_new x num_dim) receives the positions of new points in a
+ * finished layout of num_ref reference points (ref_data: num_ref x data_dim,
+ * ref_embedding: num_ref x num_dim, neither changed):
+ *   1. each new point's options->num_neighbors nearest reference points
+ *      (umapb_knn_query) and their similarities (neighbor_similarities.hpp with
+ *      the options' local_connectivity and bandwidth);
+ *   2. start at the similarity-weighted mean of those neighbours' positions;
+ *   3. the schedule of similarities_to_epochs over these edges and
+ *      optimize_layout's per-row steps (optimize_layout.hpp:136-180) in which
+ *      only the new point moves and the negative samples are reference points
+ *      (seeded by optimize_seed), at a quarter of learning_rate.
+ * num_epochs <= 0 picks the count: a third of options->num_epochs when that is
+ * set, else 100 for up to 10,000 new points and 30 above
+ * (umapb_transform_epochs).  The result does not depend on launch shapes. */
+int umapb_transform(int dtype, size_t data_dim, int32_t num_ref, const void* ref_data, const void* ref_embedding,
+                    int32_t num_new, const void* new_data, size_t num_dim, const umapb_options* options,
+                    int num_epochs, void* new_embedding);
+int umapb_transform_epochs(const umapb_options* options, int num_epochs, int32_t num_new);
+
 /* Queries of the last F32 neighbour search in this process whose candidate
  * set could not be certified by the error bound and were recomputed in FP64. */
 int umapb_knn_last_fp64_recomputed(void);

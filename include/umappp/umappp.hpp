@@ -5,13 +5,14 @@
  * @file umappp.hpp
  * @brief Umbrella header of the GPU drop-in for libscran/umappp
  * (include/umappp/umappp.hpp:9-11): Options, Status, initialize() and the
- * stage functions, backed by libumappp_b200.so (C ABI in umapb.h).
+ * stage functions (and the transform extension), backed by libumappp_b200.so (C ABI in umapb.h).
  */
 
 #include "Options.hpp"
 #include "Status.hpp"
 #include "initialize.hpp"
 #include "stages.hpp"
+#include "transform.hpp"
 
 namespace umappp {}
 

@@ -73,6 +73,9 @@ def lib():
             getattr(L, f"oracle_optimize_layout_{suf}").argtypes = [
                 _c_int, fp, _c_int, _i64p, _i32p, fp, fp, fp, _c_dbl, _c_int, ctypes.POINTER(_c_int),
                 _c_dbl, _c_dbl, _c_dbl, _c_dbl, _c_u64, _c_int, _vp]
+            getattr(L, f"oracle_transform_layout_{suf}").argtypes = [
+                _c_int, fp, _c_int, _i64p, _i32p, fp, fp, fp, _c_dbl, _c_int, fp, _c_int, _c_int,
+                _c_dbl, _c_dbl, _c_dbl, _c_dbl, _c_u64]
             getattr(L, f"oracle_has_multiple_components_{suf}").argtypes = [_c_int, _i64p, _i32p]
             f = getattr(L, f"oracle_spectral_init_{suf}")
             f.argtypes = [_c_int, _i64p, _i32p, fp, _c_int, fp, _c_int, _c_int, _c_dbl, _c_dbl, _c_int, _c_dbl,
@@ -84,6 +87,9 @@ def lib():
         L.oracle_mt64_stream.argtypes = [_c_u64, _c_i64, _u64p]
         L.oracle_knn_f64.argtypes = [_c_int, _c_int, _f64p, _c_int, _c_int, _c_int, _i32p, _f64p]
         L.oracle_knn_f32.argtypes = [_c_int, _c_int, _f32p, _c_int, _c_int, _c_int, _i32p, _f64p]
+        L.oracle_knn_query_f64.argtypes = [_c_int, _c_int, _c_int, _f64p, _f64p, _c_int, _i32p, _f64p]
+        L.oracle_negstream_draws.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _c_u64,
+                                             ctypes.c_uint32, _c_int, _i32p]
         L.oracle_trustworthiness.argtypes = [_c_int, _c_int, _f64p, _c_int, _f64p, _c_int, _c_int, _i32p]
         L.oracle_trustworthiness.restype = _c_dbl
         L.oracle_cross_entropy.argtypes = [_c_int, _i64p, _i32p, _f64p, _c_int, _f64p, _c_dbl, _c_dbl]
@@ -530,3 +536,72 @@ def gaussian_mixture(n: int, dim: int, n_clusters: int, centre_sd: float, seed: 
     labels = rng.choice(n_clusters, size=n, p=p)
     pts = centres[labels] + rng.normal(0.0, 1.0, size=(n, dim))
     return np.ascontiguousarray(pts, dtype=dtype)
+
+
+def knn_query(ref: np.ndarray, queries: np.ndarray, k: int):
+    """Exact FP64 neighbours of every query row among the reference rows:
+    (idx int32 (nq, k), dist float64 (nq, k)), ties by index."""
+    ref64 = np.ascontiguousarray(ref, dtype=np.float64)
+    q64 = np.ascontiguousarray(queries, dtype=np.float64)
+    nq = q64.shape[0]
+    idx = np.zeros((nq, k), dtype=np.int32)
+    dist = np.zeros((nq, k), dtype=np.float64)
+    lib().oracle_knn_query_f64(ref64.shape[0], nq, ref64.shape[1], ref64, q64, k, idx.reshape(-1), dist.reshape(-1))
+    return idx, dist
+
+
+def negstream_draws(head: int, tail: int, epoch: int, seed: int, n: int, count: int) -> np.ndarray:
+    """'count' bounded draws in [0, n) of the negative-sample stream of one edge."""
+    out = np.zeros(count, dtype=np.int32)
+    lib().oracle_negstream_draws(head, tail, epoch, seed, n, count, out)
+    return out
+
+
+def transform_epochs(num_epochs: int, has_layout_epochs: bool, layout_epochs: int, num_new: int) -> int:
+    """Epoch count of a transform: the given count, else a third of the
+    layout's when set, else 100 up to 10,000 new points and 30 above."""
+    if num_epochs > 0:
+        return num_epochs
+    if has_layout_epochs and layout_epochs > 0:
+        return max(1, layout_epochs // 3)
+    return 100 if num_new <= 10000 else 30
+
+
+def transform(ref_data: np.ndarray, ref_embedding: np.ndarray, new_data: np.ndarray, k: int, num_epochs: int,
+              a: float, b: float, gamma: float = 1.0, learning_rate: float = 1.0, negative_sample_rate: float = 5.0,
+              seed: int = 1234567890, local_connectivity: float = 1.0, bandwidth: float = 1.0):
+    """The transform of new points into a finished layout, serially (the
+    device's umapb_transform): exact FP64 neighbours among the reference
+    points, their similarities, a start at the similarity-weighted mean of the
+    neighbours' positions (FP64 sums in edge order), the schedule of
+    similarities_to_epochs and the head-only steps of oracle_transform_layout
+    at a quarter of the learning rate.  Float type of ref_embedding.
+    Returns (embedding, init, idx, weights)."""
+    dt = np.asarray(ref_embedding).dtype
+    suf = _suf(dt)
+    nref = ref_data.shape[0]
+    nq = new_data.shape[0]
+    idx, dist = knn_query(ref_data, new_data, k)
+    nl = CSR(np.arange(0, (nq + 1) * k, k, dtype=np.int64), idx.reshape(-1).copy(),
+             dist.reshape(-1).astype(dt))
+    w, _, _ = neighbor_similarities(nl, local_connectivity, bandwidth)
+    yref = np.ascontiguousarray(ref_embedding, dtype=dt)
+    num_dim = yref.shape[1]
+    wv = w.val.astype(np.float64).reshape(nq, k)
+    init = np.zeros((nq, num_dim), dtype=np.float64)
+    for i in range(nq):
+        ws = 0.0
+        for j in range(k):
+            ws += wv[i, j]
+        for d in range(num_dim):
+            acc = 0.0
+            for j in range(k):
+                acc += (wv[i, j] if ws > 0 else 1.0) * float(yref[idx[i, j], d])
+            init[i, d] = acc / (ws if ws > 0 else k)
+    init = init.astype(dt)
+    ep = similarities_to_epochs(w, num_epochs, negative_sample_rate)
+    Y = init.copy()
+    getattr(lib(), f"oracle_transform_layout_{suf}")(
+        num_dim, Y.reshape(-1), nq, ep.ptr, ep.targets, ep.eps, ep.enext, ep.enneg, ep.rate, num_epochs,
+        yref.reshape(-1), nref, nref, a, b, gamma, learning_rate / 4.0, seed)
+    return Y, init, idx, w

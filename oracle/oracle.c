@@ -110,6 +110,83 @@ void oracle_mt64_stream(uint64_t seed, int64_t count, uint64_t* out) {
     for (int64_t i = 0; i < count; ++i) out[i] = oracle_mt64_next(&s);
 }
 
+/*
+ * The device's negative-sample stream (restated for the transform oracle):
+ * Philox4x32 with 7 rounds (Salmon, Moraes, Dror and Shaw, "Parallel random
+ * numbers: as easy as 1, 2, 3", SC 2011; multipliers 0xD2511F53 and
+ * 0xCD9E8D57, key increments 0x9E3779B9 and 0xBB67AE85), counter (head,
+ * tail, epoch, block), key (seed low word ^ stream tag, seed high word);
+ * bounded integers by Lemire's multiply-shift with rejection ("Fast random
+ * integer generation in an interval", ACM TOMACS 2019).
+ */
+#define ORACLE_RNG_NEGATIVE 0x4E454731u
+
+typedef struct {
+    uint32_t c0, c1, c2, c3, k0, k1;
+    uint32_t buf[4];
+    int used;
+} oracle_negstream;
+
+static void oracle_philox4x32_7(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1,
+                                uint32_t out[4]) {
+    for (int r = 0; r < 7; ++r) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+        const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0;
+        const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+        c0 = n0;
+        c1 = (uint32_t)p1;
+        c2 = n2;
+        c3 = (uint32_t)p0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0;
+    out[1] = c1;
+    out[2] = c2;
+    out[3] = c3;
+}
+
+static void oracle_negstream_init(oracle_negstream* s, uint32_t head, uint32_t tail, uint32_t epoch, uint32_t k0,
+                                  uint32_t k1) {
+    s->c0 = head;
+    s->c1 = tail;
+    s->c2 = epoch;
+    s->c3 = 0;
+    s->k0 = k0;
+    s->k1 = k1;
+    s->used = 4;
+}
+
+static uint32_t oracle_negstream_next(oracle_negstream* s) {
+    if (s->used == 4) {
+        oracle_philox4x32_7(s->c0, s->c1, s->c2, s->c3++, s->k0, s->k1, s->buf);
+        s->used = 0;
+    }
+    return s->buf[s->used++];
+}
+
+static int32_t oracle_negstream_bounded(oracle_negstream* s, uint32_t n) {
+    uint64_t m = (uint64_t)oracle_negstream_next(s) * n;
+    uint32_t l = (uint32_t)m;
+    if (l < n) {
+        const uint32_t thr = (0u - n) % n;
+        while (l < thr) {
+            m = (uint64_t)oracle_negstream_next(s) * n;
+            l = (uint32_t)m;
+        }
+    }
+    return (int32_t)(m >> 32);
+}
+
+/* 'count' bounded draws of one stream (for pinning the stream). */
+void oracle_negstream_draws(uint32_t head, uint32_t tail, uint32_t epoch, uint64_t seed, uint32_t n, int count,
+                            int32_t* out) {
+    oracle_negstream s;
+    oracle_negstream_init(&s, head, tail, epoch, (uint32_t)seed ^ ORACLE_RNG_NEGATIVE, (uint32_t)(seed >> 32));
+    for (int i = 0; i < count; ++i) out[i] = oracle_negstream_bounded(&s, n);
+}
+
 /* ------------------------------------------------------------- stages --- */
 
 #define FLOAT double
@@ -284,6 +361,45 @@ void oracle_knn_f64(int n, int dim, const double* data, int k, int qstart, int q
         for (int t = count; t < k; ++t) {
             out_idx[(size_t)(q - qstart) * k + t] = -1;
             out_dist[(size_t)(q - qstart) * k + t] = INFINITY;
+        }
+    }
+    free(best);
+}
+
+/* Queries against a separate reference set: the k nearest of the nref rows of
+ * 'ref' to each of the nq rows of 'qd' (FP64 sums in dimension order, ties by
+ * index); outputs nq x k. */
+void oracle_knn_query_f64(int nref, int nq, int dim, const double* ref, const double* qd, int k, int32_t* out_idx,
+                          double* out_dist) {
+    oracle_cand* best = (oracle_cand*)malloc(sizeof(oracle_cand) * (size_t)(k + 1));
+    for (int q = 0; q < nq; ++q) {
+        int count = 0;
+        const double* xq = qd + (size_t)q * dim;
+        for (int j = 0; j < nref; ++j) {
+            const double* xj = ref + (size_t)j * dim;
+            double d2 = 0;
+            for (int d = 0; d < dim; ++d) {
+                const double diff = xq[d] - xj[d];
+                d2 += diff * diff;
+            }
+            oracle_cand c = {d2, j};
+            int pos;
+            if (count < k) {
+                pos = count++;
+            } else if (k > 0 && oracle_cand_less(&c, &best[k - 1])) {
+                pos = k - 1;
+            } else {
+                continue;
+            }
+            while (pos > 0 && oracle_cand_less(&c, &best[pos - 1])) {
+                best[pos] = best[pos - 1];
+                --pos;
+            }
+            best[pos] = c;
+        }
+        for (int t = 0; t < k; ++t) {
+            out_idx[(size_t)q * k + t] = t < count ? best[t].j : -1;
+            out_dist[(size_t)q * k + t] = t < count ? sqrt(best[t].d2) : INFINITY;
         }
     }
     free(best);

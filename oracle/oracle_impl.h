@@ -371,6 +371,82 @@ void FN(oracle_optimize_layout)(int num_dim, FLOAT* embedding, int n, const int6
     if (epoch_limit > *current_epoch) *current_epoch = epoch_limit;
 }
 
+/*
+ * Transform (no counterpart in the reference: restates the device's
+ * umapb_transform): the rows of the transform graph -- new point i's edges to
+ * reference points -- are optimised one after another through all epochs
+ * with the steps of FN(oracle_optimize_layout) above (optimize_layout.hpp:
+ * 141-179), the coefficients written as the device writes them
+ * (neg2ab pd2b / (d2 (a pd2b + 1)) and gamma2b / ((0.001 + d2) (a d2^b + 1))),
+ * except that only the new point moves and the negative samples are
+ * reference points drawn from the device's stream (oracle_negstream, counter
+ * (head0 + i, tail, epoch)).  Ynew (nq x num_dim) holds the starting positions
+ * and receives the result; enext/enneg are advanced in place.
+ */
+void FN(oracle_transform_layout)(int num_dim, FLOAT* Ynew, int nq, const int64_t* ptr, const int32_t* targets,
+                                 const FLOAT* eps, FLOAT* enext, FLOAT* enneg, double rate, int total_epochs,
+                                 const FLOAT* Yref, int nref, int head0, double a_in, double b_in, double gamma_in,
+                                 double lr_in, uint64_t seed) {
+    const FLOAT a = (FLOAT)a_in, b = (FLOAT)b_in, gamma = (FLOAT)gamma_in, lr = (FLOAT)lr_in;
+    const FLOAT negative_sample_rate = (FLOAT)rate;
+    const FLOAT dist_eps = FLOAT_EPSILON;
+    const FLOAT neg2ab = (FLOAT)-2 * a * b, gamma2b = (FLOAT)2 * gamma * b;
+    const uint32_t k0 = (uint32_t)seed ^ ORACLE_RNG_NEGATIVE, k1 = (uint32_t)(seed >> 32);
+    for (int i = 0; i < nq; ++i) {
+        FLOAT* head = Ynew + (size_t)i * num_dim;
+        for (int ep = 0; ep < total_epochs; ++ep) {
+            const FLOAT epoch = (FLOAT)ep;
+            const FLOAT alpha = (FLOAT)((double)lr * (1.0 - (double)(epoch / (FLOAT)total_epochs)));
+            for (int64_t j = ptr[i]; j < ptr[i + 1]; ++j) {
+                if (!(enext[j] <= epoch)) continue;
+                const FLOAT e_p = eps[j];
+                const FLOAT epns = e_p / negative_sample_rate;
+                const FLOAT enn = enneg[j];
+                const int nn = (int)((epoch - enn) / epns);
+                enext[j] = enext[j] + e_p;
+                enneg[j] = enn + (FLOAT)nn * epns;
+                const FLOAT* yt = Yref + (size_t)targets[j] * num_dim;
+                FLOAT d2 = 0;
+                for (int d = 0; d < num_dim; ++d) {
+                    const FLOAT diff = head[d] - yt[d];
+                    d2 += diff * diff;
+                }
+                d2 = (dist_eps < d2) ? d2 : dist_eps;
+                {
+                    const FLOAT pd2b = POW(d2, b);
+                    const FLOAT c = (neg2ab * pd2b) / (d2 * (a * pd2b + (FLOAT)1));
+                    for (int d = 0; d < num_dim; ++d) {
+                        FLOAT g = c * (head[d] - yt[d]);
+                        g = (g < (FLOAT)-4) ? (FLOAT)-4 : g;
+                        g = ((FLOAT)4 < g) ? (FLOAT)4 : g;
+                        head[d] += alpha * g;
+                    }
+                }
+                if (nn > 0) {
+                    oracle_negstream rs;
+                    oracle_negstream_init(&rs, (uint32_t)(head0 + i), (uint32_t)targets[j], (uint32_t)ep, k0, k1);
+                    for (int q = 0; q < nn; ++q) {
+                        const FLOAT* yk = Yref + (size_t)oracle_negstream_bounded(&rs, (uint32_t)nref) * num_dim;
+                        FLOAT dd2 = 0;
+                        for (int d = 0; d < num_dim; ++d) {
+                            const FLOAT diff = head[d] - yk[d];
+                            dd2 += diff * diff;
+                        }
+                        dd2 = (dist_eps < dd2) ? dd2 : dist_eps;
+                        const FLOAT c = gamma2b / (((FLOAT)0.001 + dd2) * (a * POW(dd2, b) + (FLOAT)1));
+                        for (int d = 0; d < num_dim; ++d) {
+                            FLOAT g = c * (head[d] - yk[d]);
+                            g = (g < (FLOAT)-4) ? (FLOAT)-4 : g;
+                            g = ((FLOAT)4 < g) ? (FLOAT)4 : g;
+                            head[d] += alpha * g;
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
 /* Matrix-vector product with I + D^-1/2 W D^-1/2, values built as in
  * include/umappp/spectral_init.hpp:38-78 (FP64). */
 typedef struct {

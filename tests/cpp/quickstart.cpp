@@ -1,8 +1,9 @@
 // Drop-in check: the reference's quick-start usage (README "Quick start")
 // written against the GPU headers: 2000 observations x 10 dims of N(0, 1)
 // data, exact neighbours on the device, initialize() then run(), plus a
-// partial run, the NeighborList overload and a device-resident prebuilt
-// index.  Prints one line of results.
+// partial run, the NeighborList overload, a device-resident prebuilt index
+// and the transform of new points into the finished layout.  Prints one line
+// of results.
 #include <cmath>
 #include <cstdio>
 #include <random>
@@ -47,6 +48,13 @@ int main() {
     auto sa = umappp::initialize<int, double>(prebuilt, out_dim, e_a.data(), o2);
     auto sb = umappp::initialize(ndim, nobs, data.data(), umappp::DeviceBuilder(), out_dim, e_b.data(), o2);
     if (e_a != e_b || sa.get_epoch_data().edge_targets != sb.get_epoch_data().edge_targets) return 6;
+    // the transform extension: 100 new points into the finished layout
+    const int nnew = 100;
+    std::vector<double> fresh(static_cast<size_t>(ndim) * nnew), placed(nnew * out_dim);
+    for (auto& x : fresh) x = ndist(rng);
+    umappp::transform(ndim, nobs, data.data(), out_dim, embedding.data(), nnew, fresh.data(), placed.data(), opt, 20);
+    for (double v : placed)
+        if (!std::isfinite(v)) return 7;
     const auto ab = umappp::find_ab<double>(1.0, 0.1);
     std::printf("quickstart ok: epochs=%d edges=%zu a=%.6f b=%.6f y0=%.4f\n", status.epoch(), ep.edge_targets.size(),
                 ab.first, ab.second, embedding[0]);

@@ -37,6 +37,7 @@ __all__ = [
     "neighbor_similarities", "combine_neighbor_sets", "similarities_to_epochs", "has_multiple_components",
     "spectral_init", "random_init", "find_ab", "choose_num_epochs", "optimize_layout", "loss_grad", "UmapbError",
     "to_csr", "batch_run", "initialize_knn_matrix", "Prebuilt", "initialize_prebuilt", "knn_shard",
+    "knn_query", "transform", "transform_epochs",
 ]
 
 
@@ -346,6 +347,52 @@ def initialize_from_data(data, num_dim: int, embedding, options: Optional[Option
     check(lib().umapb_initialize_data(_dtype_code(dt), data_dim, num_obs, _ptr(data), num_dim, _ptr(embedding),
                                       ctypes.byref(copt), ctypes.byref(out)))
     return Status(out.value, dt)
+
+
+def knn_query(ref_data: np.ndarray, query_data: np.ndarray, k: int):
+    """Exact neighbours of every query row among the reference rows
+    (umapb_knn_query): (indices, distances), each (num_query, k)."""
+    ref_data = np.ascontiguousarray(ref_data)
+    query_data = np.ascontiguousarray(query_data, dtype=ref_data.dtype)
+    nr, dim = ref_data.shape
+    nq = query_data.shape[0]
+    if query_data.ndim != 2 or query_data.shape[1] != dim:
+        raise ValueError("query_data must have the reference data's columns")
+    idx = np.zeros((nq, k), dtype=np.int32)
+    dist = np.zeros((nq, k), dtype=ref_data.dtype)
+    check(lib().umapb_knn_query(_dtype_code(ref_data.dtype), dim, nr, _ptr(ref_data), nq, _ptr(query_data), k,
+                                _ptr(idx), _ptr(dist)))
+    return idx, dist
+
+
+def transform(ref_data: np.ndarray, ref_embedding: np.ndarray, new_data: np.ndarray,
+              options: Optional[Options] = None, num_epochs: int = 0) -> np.ndarray:
+    """Positions of new points in a finished layout (umapb_transform): their
+    nearest reference points, a start at the similarity-weighted mean of those
+    points' positions, then optimize_layout's steps with only the new points
+    moving.  Returns (num_new, num_dim) in the reference data's type."""
+    options = options or Options()
+    ref_data = np.ascontiguousarray(ref_data)
+    dt = ref_data.dtype
+    ref_embedding = np.ascontiguousarray(ref_embedding, dtype=dt)
+    new_data = np.ascontiguousarray(new_data, dtype=dt)
+    nr, dim = ref_data.shape
+    if ref_embedding.shape[0] != nr:
+        raise ValueError("ref_embedding must have one row per reference point")
+    if new_data.ndim != 2 or new_data.shape[1] != dim:
+        raise ValueError("new_data must have the reference data's columns")
+    num_dim = ref_embedding.shape[1]
+    out = np.zeros((new_data.shape[0], num_dim), dtype=dt)
+    copt = options.to_c()
+    check(lib().umapb_transform(_dtype_code(dt), dim, nr, _ptr(ref_data), _ptr(ref_embedding), new_data.shape[0],
+                                _ptr(new_data), num_dim, ctypes.byref(copt), int(num_epochs), _ptr(out)))
+    return out
+
+
+def transform_epochs(options: Optional[Options] = None, num_epochs: int = 0, num_new: int = 0) -> int:
+    """The epoch count umapb_transform uses for these arguments."""
+    copt = (options or Options()).to_c()
+    return int(lib().umapb_transform_epochs(ctypes.byref(copt), int(num_epochs), int(num_new)))
 
 
 def batch_run(data, sizes, num_dim: int, embedding, options: Optional[Options] = None) -> dict:

@@ -48,6 +48,9 @@ SIGNATURES = {
     "umapb_options_size": (_c_size, []),
     "umapb_launch_count": (_c_i64, []),
     "umapb_set_device_wait_limit": (_c_i64, [_c_i64]),
+    "umapb_knn_query": (_c_int, [_c_int, _c_size, _c_i32, _vp, _c_i32, _vp, _c_int, _vp, _vp]),
+    "umapb_transform": (_c_int, [_c_int, _c_size, _c_i32, _vp, _vp, _c_i32, _vp, _c_size, _P(UmapbOptions), _c_int, _vp]),
+    "umapb_transform_epochs": (_c_int, [_P(UmapbOptions), _c_int, _c_i32]),
     "umapb_knn_shard": (_c_int, [_c_int, _c_size, _c_i32, _vp, _c_int, _c_i32, _c_i32, _vp, _vp, _vp, _P(_c_i32)]),
     "umapb_initialize_knn_matrix": (_c_int, [_c_int, _c_i32, _c_i32, _vp, _vp, _c_int, _c_size, _vp,
                                              _P(UmapbOptions), _P(_vp)]),

@@ -506,7 +506,6 @@ int guarded(F&& f) {
     }
 }
 
-size_t dsize(int dtype) { return dtype == UMAPB_F64 ? sizeof(double) : sizeof(float); }
 
 int64_t host_nnz(const int64_t* row_ptr, int32_t n, cudaStream_t s) {
     require(row_ptr != nullptr, "row_ptr must not be NULL");
@@ -537,6 +536,64 @@ void check_device_status(Context& ctx) {
 }  // namespace umapb
 
 using namespace umapb;
+
+namespace {
+
+// Epochs of a transform when the caller passes none: a third of the layout's
+// epoch count when the options set one, else 100 for up to 10,000 new points
+// and 30 above (umap-learn's rule for its transform).
+int transform_epochs(const umapb_options& o, int requested, int32_t nq) {
+    if (requested > 0) return requested;
+    if (o.has_num_epochs && o.num_epochs > 0) return std::max(1, o.num_epochs / 3);
+    return nq <= 10000 ? 100 : 30;
+}
+
+template <typename T>
+void transform_impl(size_t data_dim, int32_t nref, const void* ref_data, const void* ref_embedding, int32_t nq,
+                    const void* new_data, size_t num_dim, const umapb_options& o, int num_epochs, void* new_embedding,
+                    cudaStream_t s) {
+    require(data_dim >= 1 && data_dim <= static_cast<size_t>(INT32_MAX), "data_dim must be positive");
+    require(num_dim >= 1 && num_dim <= 64, "num_dim must be between 1 and 64");
+    require(nref >= 1, "the transform needs at least one reference point");
+    require(nq >= 0, "num_new must not be negative");
+    const int k = o.num_neighbors;
+    require(k >= 1 && k <= nref, "num_neighbors must be in [1, num_ref]");
+    require(o.learning_rate > 0 && std::isfinite(o.learning_rate), "learning_rate must be positive");
+    require(o.negative_sample_rate >= 0 && std::isfinite(o.negative_sample_rate),
+            "negative_sample_rate must not be negative");
+    if (nq == 0) return;
+    const size_t D = data_dim, nr = static_cast<size_t>(nref), nn = static_cast<size_t>(nq);
+    DeviceIn<T> rd(static_cast<const T*>(ref_data), nr * D, s);
+    DeviceIn<T> nd(static_cast<const T*>(new_data), nn * D, s);
+    DeviceIn<T> ry(static_cast<const T*>(ref_embedding), nr * num_dim, s);
+    DeviceInOut<T> ny(static_cast<T*>(new_embedding), nn * num_dim, s, false);
+    // the reference rows, then the new rows, in one array
+    DevArray<T> data((nr + nn) * D, s);
+    UMAPB_CUDA(cudaMemcpyAsync(data.get(), rd.get(), nr * D * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    UMAPB_CUDA(cudaMemcpyAsync(data.get() + nr * D, nd.get(), nn * D * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    DevArray<int32_t> idx(nn * k, s);
+    DevArray<T> w(nn * k, s);
+    knn_query<T>(data.get(), nref, nq, static_cast<int32_t>(D), k, idx.get(), w.get(), s);
+    data.release();
+    DevArray<int64_t> ptr(nn + 1, s);
+    dense_row_ptr_kernel<<<grid_for(nn + 1, 256), 256, 0, s>>>(nq, k, ptr.get());
+    UMAPB_LAUNCH_CHECK();
+    // the new points' similarities to their neighbours (neighbor_similarities.hpp), in place
+    neighbor_similarities<T>(nq, ptr.get(), w.get(), o.local_connectivity, o.bandwidth, 1e-3, true, nullptr, nullptr, s);
+    transform_init<T>(nq, static_cast<int>(num_dim), ptr.get(), idx.get(), w.get(), ry.get(), ny.get(), s);
+    double a = o.a, b = o.b;
+    if (!o.has_a || !o.has_b) find_ab(o.spread, o.min_dist, &a, &b);
+    DeviceEpochs<T> ep;
+    similarities_to_epochs<T>(nq, ptr.get(), idx.get(), w.get(), static_cast<int64_t>(nn * k),
+                              transform_epochs(o, num_epochs, nq), o.negative_sample_rate, ep, s);
+    // a quarter of the layout's learning rate, as umap-learn's transform uses
+    transform_layout<T>(ep, static_cast<int>(num_dim), ry.get(), nref, ny.get(), nref, a, b, o.repulsion_strength,
+                        o.learning_rate / 4.0, o.optimize_seed, s);
+    ny.finish();
+    UMAPB_SYNC(s);
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -774,6 +831,55 @@ int umapb_knn_shard(int dtype, size_t data_dim, int32_t num_obs, const void* dat
             }
             UMAPB_SYNC(s);
             *out_count = nrows;
+        };
+        if (dtype == UMAPB_F64) body(double{}); else body(float{});
+    });
+}
+
+int umapb_transform(int dtype, size_t data_dim, int32_t num_ref, const void* ref_data, const void* ref_embedding,
+                    int32_t num_new, const void* new_data, size_t num_dim, const umapb_options* opt, int num_epochs,
+                    void* new_embedding) {
+    return guarded([&] {
+        require_device();
+        require(opt != nullptr, "options must not be NULL");
+        Context& c = thread_context();
+        if (dtype == UMAPB_F64)
+            transform_impl<double>(data_dim, num_ref, ref_data, ref_embedding, num_new, new_data, num_dim, *opt,
+                                   num_epochs, new_embedding, c.stream);
+        else
+            transform_impl<float>(data_dim, num_ref, ref_data, ref_embedding, num_new, new_data, num_dim, *opt,
+                                  num_epochs, new_embedding, c.stream);
+    });
+}
+
+int umapb_transform_epochs(const umapb_options* opt, int num_epochs, int32_t num_new) {
+    if (!opt) return -1;
+    return transform_epochs(*opt, num_epochs, num_new);
+}
+
+int umapb_knn_query(int dtype, size_t data_dim, int32_t num_ref, const void* ref_data, int32_t num_query,
+                    const void* query_data, int k, int32_t* out_indices, void* out_distances) {
+    return guarded([&] {
+        require_device();
+        require(data_dim >= 1 && data_dim <= static_cast<size_t>(INT32_MAX), "data_dim must be positive");
+        require(num_ref >= 1 && num_query >= 0, "bad point counts");
+        Context& c = thread_context();
+        cudaStream_t s = c.stream;
+        const size_t D = data_dim, nr = static_cast<size_t>(num_ref), nq = static_cast<size_t>(num_query);
+        const size_t nk = nq * static_cast<size_t>(k > 0 ? k : 0);
+        auto body = [&](auto tag) {
+            using T = decltype(tag);
+            DeviceIn<T> rd(static_cast<const T*>(ref_data), nr * D, s);
+            DeviceIn<T> qd(static_cast<const T*>(query_data), nq * D, s);
+            DevArray<T> data((nr + nq) * D, s);
+            UMAPB_CUDA(cudaMemcpyAsync(data.get(), rd.get(), nr * D * sizeof(T), cudaMemcpyDeviceToDevice, s));
+            if (nq) UMAPB_CUDA(cudaMemcpyAsync(data.get() + nr * D, qd.get(), nq * D * sizeof(T), cudaMemcpyDeviceToDevice, s));
+            DeviceInOut<int32_t> oi(out_indices, nk, s, false);
+            DeviceInOut<T> od(static_cast<T*>(out_distances), nk, s, false);
+            knn_query<T>(data.get(), num_ref, num_query, static_cast<int32_t>(D), k, oi.get(), od.get(), s);
+            oi.finish();
+            od.finish();
+            UMAPB_SYNC(s);
         };
         if (dtype == UMAPB_F64) body(double{}); else body(float{});
     });

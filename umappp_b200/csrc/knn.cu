@@ -16,9 +16,11 @@
 // Double data: the FP64 kernel directly, with multiply and add kept separate
 // so the sums round exactly as a sequential FP64 loop.
 #include <algorithm>
-#include <cstring>
 #include <cfloat>
+#include <climits>
 #include <cstdlib>
+#include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "stages.cuh"
@@ -100,7 +102,8 @@ __device__ __forceinline__ void insert_sorted(A (&bd)[KCAP], int (&bi)[KCAP], A 
 
 // Brute-force candidate kernel.  T = storage type, A = accumulation type.
 // If 'queries' is non-null the block's threads take their query ids from it
-// (nq entries), else queries are 0..n-1.
+// (nq entries), else queries are 0..nq-1.  The candidates are the data rows
+// [0, n) other than the query itself.
 template <typename T, typename A, int KCAP>
 __global__ void __launch_bounds__(KNN_BLOCK) knn_bruteforce_kernel(const T* __restrict__ data, int32_t n, int32_t dim,
                                                                    const int32_t* __restrict__ queries, int32_t nq,
@@ -163,8 +166,8 @@ __global__ void __launch_bounds__(KNN_BLOCK) knn_bruteforce_kernel(const T* __re
 // (FP64 distance, index) and flags queries whose candidate set may miss a
 // true neighbour.
 template <int KCAP>
-__global__ void knn_rescore_kernel(const float* __restrict__ data, int32_t n, int32_t dim, int32_t k,
-                                   const int32_t* __restrict__ queries, int32_t nq, int cand_by_slot,
+__global__ void knn_rescore_kernel(const float* __restrict__ data, int32_t others, int32_t dim, int32_t k,
+                                   const int32_t* __restrict__ queries, int32_t nq, int cand_by_slot, int out_by_slot,
                                    const int32_t* __restrict__ cand_idx, const float* __restrict__ cand_d2,
                                    int32_t* __restrict__ out_idx, float* __restrict__ out_dist,
                                    double* __restrict__ out_dist64, int32_t* __restrict__ redo,
@@ -221,7 +224,7 @@ __global__ void knn_rescore_kernel(const float* __restrict__ data, int32_t n, in
     const float last32 = cand_d2[crow * KCAP + KCAP - 1];
     const double rel = (dim + 2) * 1.2e-7 * 2.0;
     const double kth = d64[k - 1];
-    const bool full_list = (n - 1) <= KCAP;   // every other point is a candidate
+    const bool full_list = others <= KCAP;   // every candidate point is in the list
     bool certain;
     if (norms) {
         const double bound = tc_rel * (static_cast<double>(norms[q]) + static_cast<double>(__uint_as_float(*norm_max_bits)));
@@ -230,27 +233,29 @@ __global__ void knn_rescore_kernel(const float* __restrict__ data, int32_t n, in
         certain = static_cast<double>(last32) * (1.0 - rel) > kth * (1.0 + rel);
     }
     if (!full_list && !certain) {
-        const int32_t slot = atomicAdd(redo_count, 1);
-        redo[slot] = q;
+        const int32_t r = atomicAdd(redo_count, 1);
+        redo[r] = out_by_slot ? slot : q;   // a slot when the output is by slot, else the data row
     }
     if (err_scale > 0.0 && worst > 0.0f) atomicMax(tc_err_bits, __float_as_uint(worst));
+    const size_t orow = static_cast<size_t>(out_by_slot ? slot : q);
     for (int c = 0; c < k; ++c) {
-        out_idx[static_cast<size_t>(q) * k + c] = id[c];
+        out_idx[orow * k + c] = id[c];
         const double dd = sqrt(d64[c]);
-        out_dist[static_cast<size_t>(q) * k + c] = static_cast<float>(dd);
-        if (out_dist64) out_dist64[static_cast<size_t>(q) * k + c] = dd;
+        out_dist[orow * k + c] = static_cast<float>(dd);
+        if (out_dist64) out_dist64[orow * k + c] = dd;
     }
 }
 
 // Writes the first k entries of FP64 candidate lists (sqrt of squared distance).
+// Output row of entry 'slot': out_rows[slot] if given, else the query's data row.
 template <typename T, int KCAP>
-__global__ void knn_emit_f64_kernel(int32_t nq, const int32_t* __restrict__ queries, int32_t k,
-                                    const int32_t* __restrict__ cand_idx, const double* __restrict__ cand_d2,
+__global__ void knn_emit_f64_kernel(int32_t nq, const int32_t* __restrict__ queries, const int32_t* __restrict__ out_rows,
+                                    int32_t k, const int32_t* __restrict__ cand_idx, const double* __restrict__ cand_d2,
                                     int32_t* __restrict__ out_idx, T* __restrict__ out_dist,
                                     double* __restrict__ out_dist64) {
     const int32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= nq) return;
-    const int32_t q = queries ? queries[slot] : slot;
+    const int32_t q = out_rows ? out_rows[slot] : queries ? queries[slot] : slot;
     for (int c = 0; c < k; ++c) {
         out_idx[static_cast<size_t>(q) * k + c] = cand_idx[static_cast<size_t>(slot) * KCAP + c];
         const double dd = sqrt(cand_d2[static_cast<size_t>(slot) * KCAP + c]);
@@ -259,17 +264,19 @@ __global__ void knn_emit_f64_kernel(int32_t nq, const int32_t* __restrict__ quer
     }
 }
 
+// FP64 search of the queries (data rows 'queries') among the data rows [0, n);
+// results go to the queries' own rows, or to rows out_rows[slot] if given.
 template <typename T, int KCAP>
 void run_f64(const T* data, int32_t n, int32_t dim, int32_t k, const int32_t* queries, int32_t nq, int32_t* out_idx,
-             T* out_dist, double* out_dist64, cudaStream_t s) {
+             T* out_dist, double* out_dist64, cudaStream_t s, const int32_t* out_rows = nullptr) {
     if (nq <= 0) return;
     DevArray<int32_t> ci(static_cast<size_t>(nq) * KCAP, s);
     DevArray<double> cd(static_cast<size_t>(nq) * KCAP, s);
     knn_bruteforce_kernel<T, double, KCAP><<<(nq + KNN_BLOCK - 1) / KNN_BLOCK, KNN_BLOCK, 0, s>>>(
         data, n, dim, queries, nq, ci.get(), cd.get());
     UMAPB_LAUNCH_CHECK();
-    knn_emit_f64_kernel<T, KCAP><<<(nq + 127) / 128, 128, 0, s>>>(nq, queries, k, ci.get(), cd.get(), out_idx, out_dist,
-                                                                  out_dist64);
+    knn_emit_f64_kernel<T, KCAP><<<(nq + 127) / 128, 128, 0, s>>>(nq, queries, out_rows, k, ci.get(), cd.get(), out_idx,
+                                                                  out_dist, out_dist64);
     UMAPB_LAUNCH_CHECK();
 }
 
@@ -311,6 +318,7 @@ void run_f32(const float* data, int32_t n, int32_t dim, int32_t k, int32_t* out_
     // slot of the shard's row list (sharded brute force)
     DevArray<int32_t> ci;
     DevArray<float> cd;
+    DevArray<int32_t> tree_rows;
     int32_t nq = n;
     const int32_t* queries = nullptr;
     bool by_slot = false;
@@ -321,7 +329,10 @@ void run_f32(const float* data, int32_t n, int32_t dim, int32_t k, int32_t* out_
         norms.allocate(n_pad, s);
         DevArray<int> err(1, s);
         err.zero(s);
-        tc = knn_tc_candidates(data, n, dim, KCAP, ci.get(), cd.get(), norms.get(), err.get(), s, shard, rows, nrows);
+        // unsharded: the rows in tree order, so that the rescoring walks the
+        // queries with nearby ones together (their candidates share L2 lines)
+        tc = knn_tc_candidates(data, n, dim, KCAP, ci.get(), cd.get(), norms.get(), err.get(), s, shard, rows, nrows,
+                               sharded ? nullptr : &tree_rows);
         int h_err = 0;
         UMAPB_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
         UMAPB_SYNC(s);
@@ -333,6 +344,8 @@ void run_f32(const float* data, int32_t n, int32_t dim, int32_t k, int32_t* out_
             if (sharded) {
                 nq = *nrows;
                 queries = rows->get();
+            } else if (tree_rows.get()) {
+                queries = tree_rows.get();   // nq = n; candidates and output by data row
             }
         }
     }
@@ -363,7 +376,7 @@ void run_f32(const float* data, int32_t n, int32_t dim, int32_t k, int32_t* out_
     DevArray<unsigned int> tc_err(1, s);
     tc_err.zero(s);
     if (nq > 0) {
-        knn_rescore_kernel<KCAP><<<(nq + 127) / 128, 128, 0, s>>>(data, n, dim, k, queries, nq, by_slot ? 1 : 0, ci.get(),
+        knn_rescore_kernel<KCAP><<<(nq + 127) / 128, 128, 0, s>>>(data, n - 1, dim, k, queries, nq, by_slot ? 1 : 0, 0, ci.get(),
                                                                   cd.get(), out_idx, out_dist, out_dist64, redo.get(),
                                                                   redo_count.get(), tc ? norms.get() : nullptr,
                                                                   norm_max.get(), TC_REL_BOUND, tc_err.get());
@@ -431,7 +444,8 @@ void run_f32_batched(const float* data, const std::vector<int32_t>& inst, int32_
     redo_count.zero(s);
     DevArray<unsigned int> tc_err(1, s);
     tc_err.zero(s);
-    knn_rescore_kernel<KCAP><<<(n + 127) / 128, 128, 0, s>>>(data, n, dim, k, nullptr, n, 0, ci.get(), cd.get(), out_idx,
+    knn_rescore_kernel<KCAP><<<(n + 127) / 128, 128, 0, s>>>(data, n - 1, dim, k, nullptr, n, 0, 0, ci.get(), cd.get(),
+                                                             out_idx,
                                                              out_dist,
                                                              nullptr, redo.get(), redo_count.get(), norms.get(),
                                                              norm_max.get(), TC_REL_BOUND, tc_err.get());
@@ -539,6 +553,76 @@ template void knn_exact_shard<float>(const float*, int32_t, int32_t, int32_t, Kn
                                      DevArray<int32_t>&, int32_t&, cudaStream_t);
 template void knn_exact_shard<double>(const double*, int32_t, int32_t, int32_t, KnnShard, int32_t*, double*,
                                       DevArray<int32_t>&, int32_t&, cudaStream_t);
+
+__global__ void add_offset_kernel(int32_t count, const int32_t* __restrict__ src, int32_t add,
+                                  int32_t* __restrict__ dst) {
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) dst[i] = src[i] + add;
+}
+
+// Float queries against reference rows: FP32 brute-force candidates (from
+// differences), FP64 rescoring and certification, FP64 search of the
+// uncertain queries.  rows[slot] = nref + slot are the queries' data rows;
+// results are written by slot.
+template <int KCAP>
+void run_query_f32(const float* data, int32_t nref, int32_t nq, int32_t dim, int32_t k, const int32_t* rows,
+                   int32_t* out_idx, float* out_dist, cudaStream_t s) {
+    DevArray<int32_t> ci(static_cast<size_t>(nq) * KCAP, s);
+    DevArray<float> cd(static_cast<size_t>(nq) * KCAP, s);
+    knn_bruteforce_kernel<float, float, KCAP><<<(nq + KNN_BLOCK - 1) / KNN_BLOCK, KNN_BLOCK, 0, s>>>(
+        data, nref, dim, rows, nq, ci.get(), cd.get());
+    UMAPB_LAUNCH_CHECK();
+    DevArray<int32_t> redo(nq, s), redo_count(1, s);
+    redo_count.zero(s);
+    knn_rescore_kernel<KCAP><<<(nq + 127) / 128, 128, 0, s>>>(data, nref, dim, k, rows, nq, 1, 1, ci.get(), cd.get(),
+                                                              out_idx, out_dist, nullptr, redo.get(), redo_count.get(),
+                                                              nullptr, nullptr, TC_REL_BOUND, nullptr);
+    UMAPB_LAUNCH_CHECK();
+    int32_t nredo = 0;
+    UMAPB_CUDA(cudaMemcpyAsync(&nredo, redo_count.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    UMAPB_SYNC(s);
+    last_knn_redo_count() = nredo;
+    if (nredo > 0) {   // redo holds slots: their data rows are nref + slot
+        DevArray<int32_t> redo_rows(nredo, s);
+        add_offset_kernel<<<grid_for(nredo, 256), 256, 0, s>>>(nredo, redo.get(), nref, redo_rows.get());
+        UMAPB_LAUNCH_CHECK();
+        if (k + 8 <= 32) run_f64<float, 32>(data, nref, dim, k, redo_rows.get(), nredo, out_idx, out_dist, nullptr, s, redo.get());
+        else if (k + 8 <= 64) run_f64<float, 64>(data, nref, dim, k, redo_rows.get(), nredo, out_idx, out_dist, nullptr, s, redo.get());
+        else run_f64<float, 128>(data, nref, dim, k, redo_rows.get(), nredo, out_idx, out_dist, nullptr, s, redo.get());
+    }
+}
+
+template <typename T>
+void knn_query(const T* data, int32_t nref, int32_t nq, int32_t dim, int32_t k, int32_t* out_idx, T* out_dist,
+               cudaStream_t s) {
+    require(nref >= 1, "the search needs at least one reference point");
+    require(dim >= 1, "data_dim must be positive");
+    require(nq >= 0, "the number of query points must not be negative");
+    require(k >= 1 && k <= nref, "num_neighbors must be in [1, number of reference points]");
+    require(k <= 120, "num_neighbors above 120 is not supported by the device search");
+    require(static_cast<int64_t>(nref) + nq <= INT32_MAX, "too many points for 32-bit indices");
+    if (nq == 0) return;
+    DevArray<int32_t> rows(nq, s);
+    iota_kernel<<<grid_for(nq, 256), 256, 0, s>>>(nq, nref, rows.get());
+    UMAPB_LAUNCH_CHECK();
+    if constexpr (std::is_same<T, float>::value) {
+        if (k + 8 <= 16) run_query_f32<16>(data, nref, nq, dim, k, rows.get(), out_idx, out_dist, s);
+        else if (k + 8 <= 24) run_query_f32<24>(data, nref, nq, dim, k, rows.get(), out_idx, out_dist, s);
+        else if (k + 8 <= 32) run_query_f32<32>(data, nref, nq, dim, k, rows.get(), out_idx, out_dist, s);
+        else if (k + 8 <= 64) run_query_f32<64>(data, nref, nq, dim, k, rows.get(), out_idx, out_dist, s);
+        else run_query_f32<128>(data, nref, nq, dim, k, rows.get(), out_idx, out_dist, s);
+    } else {
+        DevArray<int32_t> slots(nq, s);
+        iota_kernel<<<grid_for(nq, 256), 256, 0, s>>>(nq, 0, slots.get());
+        UMAPB_LAUNCH_CHECK();
+        if (k <= 16) run_f64<double, 16>(data, nref, dim, k, rows.get(), nq, out_idx, out_dist, nullptr, s, slots.get());
+        else if (k <= 32) run_f64<double, 32>(data, nref, dim, k, rows.get(), nq, out_idx, out_dist, nullptr, s, slots.get());
+        else if (k <= 64) run_f64<double, 64>(data, nref, dim, k, rows.get(), nq, out_idx, out_dist, nullptr, s, slots.get());
+        else run_f64<double, 128>(data, nref, dim, k, rows.get(), nq, out_idx, out_dist, nullptr, s, slots.get());
+    }
+}
+
+template void knn_query<float>(const float*, int32_t, int32_t, int32_t, int32_t, int32_t*, float*, cudaStream_t);
+template void knn_query<double>(const double*, int32_t, int32_t, int32_t, int32_t, int32_t*, double*, cudaStream_t);
 
 template <typename T>
 void knn_exact(const T* data, int32_t n, int32_t dim, int32_t k, int32_t* out_idx, T* out_dist, cudaStream_t s,

@@ -467,10 +467,11 @@ bool prune_enabled() {
 void run_f16_pruned(const float* data, const std::vector<int32_t>& inst, int32_t dim, int kcap, float scale,
                     int32_t* cand_idx, float* cand_d2, float* norms_by_row, int* d_err, cudaStream_t s,
                     KnnShard shard = KnnShard(), DevArray<int32_t>* shard_rows = nullptr,
-                    int32_t* shard_count = nullptr) {
+                    int32_t* shard_count = nullptr, DevArray<int32_t>* tree_rows = nullptr) {
     const bool prune = prune_enabled();
     KnnTiles tiles;
     knn_tree_order(data, dim, inst, prune, tiles, s);
+    if (tree_rows) knn_tree_rows(tiles, inst.back(), *tree_rows, s);
     KnnTasks tasks;
     knn_tile_tasks(data, dim, tiles, inst, knn_tc16_query_tiles(dim), kcap, prune, tasks, s, shard);
     if (shard_rows) knn_task_rows(tiles, tasks, inst.back(), *shard_rows, *shard_count, s);
@@ -505,13 +506,13 @@ static float f16_scale_or_zero(const float* data, size_t count, int32_t dim, int
 // FP64 rescoring.
 bool knn_tc_candidates(const float* data, int32_t n, int32_t dim, int kcap, int32_t* cand_idx, float* cand_d2,
                        float* norms_out, int* d_err, cudaStream_t s, KnnShard shard, DevArray<int32_t>* shard_rows,
-                       int32_t* shard_count) {
+                       int32_t* shard_count, DevArray<int32_t>* tree_rows) {
     require(knn_tc_supported(dim, kcap), "tensor-core kNN: unsupported dimension or candidate count");
     const int32_t n_pad = ((n + TC_M - 1) / TC_M) * TC_M;
     const float scale = f16_scale_or_zero(data, static_cast<size_t>(n) * dim, dim, kcap, s);
     if (scale > 0.0f) {
         run_f16_pruned(data, {0, n}, dim, kcap, scale, cand_idx, cand_d2, norms_out, d_err, s, shard, shard_rows,
-                       shard_count);
+                       shard_count, tree_rows);
         return true;
     }
     if (shard.count > 1) return false;   // the TF32 search covers every query: the caller shards by rows instead

@@ -26,6 +26,7 @@
 // neighbour is lost); for data without cluster structure the lists simply
 // cover every tile.
 #include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
 
 #include <algorithm>
 #include <cmath>
@@ -55,30 +56,16 @@ __device__ __forceinline__ float order_bits_float(uint32_t u) {
     return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
 }
 
-// Sort key of every position: its segment's index in the high bits, the
-// point's projection on the difference of two points of the segment in the
-// low 32 bits (0 in segments that are leaves).  One radix sort of these keys
-// sorts every segment at once and keeps the segments in place.
-__global__ void rp_keys_kernel(const float* __restrict__ data, int32_t dim, int32_t n,
-                               const int32_t* __restrict__ perm, int32_t nseg, const int32_t* __restrict__ seg_start,
-                               const int32_t* __restrict__ seg_a, const int32_t* __restrict__ seg_b,
-                               unsigned long long* __restrict__ keys) {
-    for (int32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
-        int lo = 0, hi = nseg - 1;   // segment of position p: last start <= p
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (seg_start[mid] <= p) lo = mid; else hi = mid - 1;
-        }
-        const int32_t a = seg_a[lo], b = seg_b[lo];
-        float key = 0.0f;
-        if (a >= 0) {
-            const float* x = data + static_cast<size_t>(perm[p]) * dim;
-            const float* xa = data + static_cast<size_t>(perm[a]) * dim;
-            const float* xb = data + static_cast<size_t>(perm[b]) * dim;
-            for (int d = 0; d < dim; ++d) key = fmaf(x[d], xa[d] - xb[d], key);
-        }
-        keys[p] = (static_cast<unsigned long long>(lo) << 32) | float_order_bits(key);
+// The points of the segments split at a level ("active"), concatenated: item
+// i belongs to active segment j = the last with aoff[j] <= i and sits at
+// position ast[j] + i - aoff[j] of perm.
+__device__ __forceinline__ int active_segment(int64_t i, int32_t nact, const int32_t* __restrict__ aoff) {
+    int lo = 0, hi = nact - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (aoff[mid] <= i) lo = mid; else hi = mid - 1;
     }
+    return lo;
 }
 
 // The window of a segment of len points in which a hard cut may fall.
@@ -102,39 +89,65 @@ __device__ __forceinline__ void warp_segment_max(unsigned long long* __restrict_
     if (seg >= 0 && (lane == 0 || prev != seg)) atomicMax(&best[seg], key);
 }
 
-// The point of every active segment farthest from its point a (squared FP32
-// distance): each position folds (distance bits, reversed position) into its
-// segment's 64-bit maximum, so that ties go to the smallest position.  The
-// loop runs whole warps (warp_segment_max).
-__global__ void far_point_kernel(const float* __restrict__ data, int32_t dim, int32_t n,
-                                 const int32_t* __restrict__ perm, int32_t nseg, const int32_t* __restrict__ seg_start,
-                                 const int32_t* __restrict__ seg_a, unsigned long long* __restrict__ best) {
+// The point of every active segment farthest from its point a (position
+// aa[j]; squared FP32 distance): each item folds (distance bits, reversed
+// position) into its segment's 64-bit maximum, so that ties go to the
+// smallest position.  The loop runs whole warps (warp_segment_max).
+__global__ void far_point_kernel(const float* __restrict__ data, int32_t dim, const int32_t* __restrict__ perm,
+                                 int32_t nact, const int32_t* __restrict__ aoff, const int32_t* __restrict__ ast,
+                                 const int32_t* __restrict__ aa, int64_t total, unsigned long long* __restrict__ best) {
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-    for (int64_t base = static_cast<int64_t>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
-        const int32_t p = static_cast<int32_t>(base + (threadIdx.x & 31));
+    for (int64_t base = static_cast<int64_t>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31); base < total;
+         base += stride) {
+        const int64_t i = base + (threadIdx.x & 31);
         int seg = -1;
         unsigned long long key = 0;
-        if (p < n) {
-            int lo = 0, hi = nseg - 1;   // segment of position p: last start <= p
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (seg_start[mid] <= p) lo = mid; else hi = mid - 1;
+        if (i < total) {
+            const int j = active_segment(i, nact, aoff);
+            const int32_t p = ast[j] + static_cast<int32_t>(i - aoff[j]);
+            const float* x = data + static_cast<size_t>(perm[p]) * dim;
+            const float* xa = data + static_cast<size_t>(perm[aa[j]]) * dim;
+            float d2 = 0.0f;
+            for (int d = 0; d < dim; ++d) {
+                const float v = x[d] - xa[d];
+                d2 = fmaf(v, v, d2);
             }
-            const int32_t a = seg_a[lo];
-            if (a >= 0) {
-                const float* x = data + static_cast<size_t>(perm[p]) * dim;
-                const float* xa = data + static_cast<size_t>(perm[a]) * dim;
-                float d2 = 0.0f;
-                for (int d = 0; d < dim; ++d) {
-                    const float v = x[d] - xa[d];
-                    d2 = fmaf(v, v, d2);
-                }
-                seg = lo;
-                key = (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) |
-                      static_cast<unsigned long long>(0xffffffffu - static_cast<uint32_t>(p));
-            }
+            seg = j;
+            key = (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) |
+                  static_cast<unsigned long long>(0xffffffffu - static_cast<uint32_t>(p));
         }
         warp_segment_max(best, seg, key);
+    }
+}
+
+// Sort key of every active item: its active segment in the high bits, the
+// point's projection on x_a - x_b (b: the segment's far point, from
+// far_point_kernel) in the low 32 bits; the item's point goes to vals.  One
+// radix sort of these keys sorts every active segment at once.
+__global__ void rp_keys_kernel(const float* __restrict__ data, int32_t dim, const int32_t* __restrict__ perm,
+                               int32_t nact, const int32_t* __restrict__ aoff, const int32_t* __restrict__ ast,
+                               const int32_t* __restrict__ aa, const unsigned long long* __restrict__ far,
+                               int64_t total, unsigned long long* __restrict__ keys, int32_t* __restrict__ vals) {
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x) {
+        const int j = active_segment(i, nact, aoff);
+        const int32_t p = ast[j] + static_cast<int32_t>(i - aoff[j]);
+        const int32_t b = static_cast<int32_t>(0xffffffffu - static_cast<uint32_t>(far[j] & 0xffffffffu));
+        const float* x = data + static_cast<size_t>(perm[p]) * dim;
+        const float* xa = data + static_cast<size_t>(perm[aa[j]]) * dim;
+        const float* xb = data + static_cast<size_t>(perm[b]) * dim;
+        float key = 0.0f;
+        for (int d = 0; d < dim; ++d) key = fmaf(x[d], xa[d] - xb[d], key);
+        keys[i] = (static_cast<unsigned long long>(j) << 32) | float_order_bits(key);
+        vals[i] = perm[p];
+    }
+}
+
+// perm at the active positions from the sorted items.
+__global__ void scatter_active_kernel(int32_t nact, const int32_t* __restrict__ aoff, const int32_t* __restrict__ ast,
+                                      int64_t total, const int32_t* __restrict__ vals, int32_t* __restrict__ perm) {
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x) {
+        const int j = active_segment(i, nact, aoff);
+        perm[ast[j] + static_cast<int32_t>(i - aoff[j])] = vals[i];
     }
 }
 
@@ -316,72 +329,110 @@ __global__ void __launch_bounds__(TREE_LEAF)
     }
 }
 
-// Squared distance between the centroid cb (shared memory) and tile t's
-// centroid, read from the [dim][tiles] copy ct (coalesced across a warp), in
-// FP32: relative error below dim * 2^-23, covered by the margins below.
-__device__ __forceinline__ float centroid_d2(const float* __restrict__ cb, const float* __restrict__ ct, int32_t ntiles,
-                                             int32_t t, int dim) {
-    float s = 0.0f;
-    for (int d = 0; d < dim; ++d) {
-        const float v = cb[d] - ct[static_cast<size_t>(d) * ntiles + t];
-        s = fmaf(v, v, s);
-    }
-    return s;
-}
-
-// One warp per query tile b (tiles [t0, t0 + nt) of its instance).
-// Radius rho of b's k-neighbourhoods: every query q of b has at least k other
-// points within rho --
+// One warp per LIST_QB consecutive query tiles b (each with tiles
+// [t0_b, t0_b + nt_b) of its instance); a centroid read serves all of them.
+// Radius rho_b of b's k-neighbourhoods: every query q of b has at least k
+// other points within rho_b --
 //   kth_b (tile_kth_kernel)              if b holds k + 1 or more points,
 //   2 R_b                                likewise (never below kth_b),
 //   R_b + |c_b - c_w| + R_w (upper)      for any tile w with k + 1 or more points,
 // the smallest of these (infinite if none applies).  Tile t is needed unless
-// |c_b - c_t| - R_b - R_t > rho.  The needed tiles are written in ascending
-// order from lists[slot[b]] (room for nt entries), their number to counts[b].
+// |c_b - c_t| - R_b - R_t > rho_b.  The needed tiles are written in ascending
+// order from lists[slot[b]] (room for nt_b entries), their number to counts[b].
 constexpr int LIST_WARPS = 8;
+constexpr int LIST_QB = 8;
 constexpr int MAX_TREE_DIM = 128;
 __global__ void __launch_bounds__(32 * LIST_WARPS)
     tile_lists_kernel(int32_t nq, const int32_t* __restrict__ q_tile0, const int32_t* __restrict__ q_ntiles,
                       const float* __restrict__ ct, int32_t ntiles, const float* __restrict__ tr,
                       const int32_t* __restrict__ tcount, const float* __restrict__ tkth, int32_t dim, int32_t k,
-                      bool prune,
-                      const int64_t* __restrict__ slot, int32_t* __restrict__ counts, int32_t* __restrict__ lists) {
-    __shared__ float cbs[LIST_WARPS][MAX_TREE_DIM];
+                      bool prune, const int64_t* __restrict__ slot, int32_t* __restrict__ counts,
+                      int32_t* __restrict__ lists) {
+    __shared__ float cbs[LIST_WARPS][MAX_TREE_DIM][LIST_QB];   // [d][q]: one 32-byte read per d
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int32_t b = blockIdx.x * LIST_WARPS + wib;
-    if (b >= nq) return;   // whole warps
-    float* cb = cbs[wib];
-    for (int d = lane; d < dim; d += 32) cb[d] = ct[static_cast<size_t>(d) * ntiles + b];
+    const int32_t b0 = (blockIdx.x * LIST_WARPS + wib) * LIST_QB;
+    if (b0 >= nq) return;   // whole warps
+    const int nb = min(LIST_QB, nq - b0);
+    float (*cb)[LIST_QB] = cbs[wib];
+    for (int e = lane; e < dim * LIST_QB; e += 32) {
+        const int d = e / LIST_QB, q = e - d * LIST_QB;
+        cb[d][q] = q < nb ? ct[static_cast<size_t>(d) * ntiles + b0 + q] : 0.0f;
+    }
     __syncwarp();
-    const int32_t t0 = q_tile0[b], nt = q_ntiles[b];
-    const float rb = tr[b];
-    float rho = (tcount[b] >= k + 1) ? (tkth ? fminf(2.0f * rb, tkth[b]) : 2.0f * rb) : CUDART_INF_F;
-    if (prune) {
-        for (int32_t base = 0; base < nt; base += 32) {
-            const int32_t w = t0 + base + lane;
-            if (base + lane < nt && w != b && tcount[w] >= k + 1) {
-                const float dist_up = sqrtf(centroid_d2(cb, ct, ntiles, w, dim) * D2_HIGH) * D2_HIGH;
-                rho = fminf(rho, __fadd_ru(__fadd_ru(rb, dist_up), tr[w]));
+    int32_t t0[LIST_QB], t1[LIST_QB];
+    float rb[LIST_QB], rho[LIST_QB];
+    int32_t lo = INT32_MAX, hi = 0;
+#pragma unroll
+    for (int q = 0; q < LIST_QB; ++q) {
+        const int32_t b = b0 + q;
+        t0[q] = q < nb ? q_tile0[b] : 0;
+        t1[q] = q < nb ? t0[q] + q_ntiles[b] : 0;
+        rb[q] = q < nb ? tr[b] : 0.0f;
+        rho[q] = (q < nb && tcount[b] >= k + 1) ? (tkth ? fminf(2.0f * rb[q], tkth[b]) : 2.0f * rb[q]) : CUDART_INF_F;
+        if (q < nb) {
+            lo = min(lo, t0[q]);
+            hi = max(hi, t1[q]);
+        }
+    }
+    // squared centroid distances from every query tile of the group to tile t
+    auto dist2 = [&](int32_t t, float (&s)[LIST_QB]) {
+#pragma unroll
+        for (int q = 0; q < LIST_QB; ++q) s[q] = 0.0f;
+        for (int d = 0; d < dim; ++d) {
+            const float c = ct[static_cast<size_t>(d) * ntiles + t];
+#pragma unroll
+            for (int q = 0; q < LIST_QB; ++q) {
+                const float v = cb[d][q] - c;
+                s[q] = fmaf(v, v, s[q]);
             }
         }
-        for (int o = 16; o > 0; o >>= 1) rho = fminf(rho, __shfl_xor_sync(0xffffffffu, rho, o));
-    }
-    const bool all = !prune || !(rho < CUDART_INF_F);
-    int32_t* out = lists + slot[b];
-    int32_t total = 0;
-    for (int32_t base = 0; base < nt; base += 32) {
-        const int32_t t = t0 + base + lane;
-        bool need = false;
-        if (base + lane < nt) {
-            // needed unless |c_b - c_t| > rho + R_b + R_t (all non-negative: compare squares)
-            const float reach = rho + rb + tr[t];
-            need = all || t == b || centroid_d2(cb, ct, ntiles, t, dim) * D2_LOW <= reach * reach * D2_HIGH;
+    };
+    if (prune) {
+        for (int32_t base = lo; base < hi; base += 32) {
+            const int32_t w = base + lane;
+            if (w < hi && tcount[w] >= k + 1) {
+                float s[LIST_QB];
+                dist2(w, s);
+#pragma unroll
+                for (int q = 0; q < LIST_QB; ++q) {
+                    if (w >= t0[q] && w < t1[q] && w != b0 + q) {
+                        const float dist_up = sqrtf(s[q] * D2_HIGH) * D2_HIGH;
+                        rho[q] = fminf(rho[q], __fadd_ru(__fadd_ru(rb[q], dist_up), tr[w]));
+                    }
+                }
+            }
         }
-        const unsigned m = __ballot_sync(0xffffffffu, need);
-        if (need) out[total + __popc(m & ((1u << lane) - 1u))] = t;
-        total += __popc(m);
+#pragma unroll
+        for (int q = 0; q < LIST_QB; ++q)
+            for (int o = 16; o > 0; o >>= 1) rho[q] = fminf(rho[q], __shfl_xor_sync(0xffffffffu, rho[q], o));
     }
-    if (lane == 0) counts[b] = total;
+    int32_t total[LIST_QB];
+#pragma unroll
+    for (int q = 0; q < LIST_QB; ++q) total[q] = 0;
+    for (int32_t base = lo; base < hi; base += 32) {
+        const int32_t t = base + lane;
+        float s[LIST_QB];
+        if (t < hi) dist2(t, s);
+        const float rt = t < hi ? tr[t] : 0.0f;
+#pragma unroll
+        for (int q = 0; q < LIST_QB; ++q) {
+            bool need = false;
+            if (q < nb && t >= t0[q] && t < t1[q]) {
+                // needed unless |c_b - c_t| > rho + R_b + R_t (all non-negative: compare squares)
+                const bool all = !prune || !(rho[q] < CUDART_INF_F);
+                const float reach = rho[q] + rb[q] + rt;
+                need = all || t == b0 + q || s[q] * D2_LOW <= reach * reach * D2_HIGH;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, need);
+            if (need) lists[slot[b0 + q] + total[q] + __popc(m & ((1u << lane) - 1u))] = t;
+            total[q] += __popc(m);
+        }
+    }
+    if (lane < nb) {
+#pragma unroll
+        for (int q = 0; q < LIST_QB; ++q)
+            if (q == lane) counts[b0 + q] = total[q];
+    }
 }
 
 }  // namespace
@@ -390,7 +441,7 @@ void knn_tree_order(const float* data, int32_t dim, const std::vector<int32_t>& 
                     cudaStream_t s) {
     const int ninst = static_cast<int>(inst.size()) - 1;
     const int32_t n = inst[ninst];
-    DevArray<int32_t> perm(n, s), perm2(n, s);
+    DevArray<int32_t> perm(n, s);
     DevArray<unsigned long long> keys(n, s), keys2(n, s);
     iota_kernel<<<grid_for(n, 256), 256, 0, s>>>(perm.get(), n);
     UMAPB_LAUNCH_CHECK();
@@ -413,83 +464,63 @@ void knn_tree_order(const float* data, int32_t dim, const std::vector<int32_t>& 
         z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
         return z ^ (z >> 31);
     };
-    DevArray<int32_t> d_start, d_end, d_a, d_b;
-    DevArray<unsigned long long> d_far;
+    DevArray<int32_t> vals(n, s), vals2(n, s);
     for (int level = 0; tree && level < 64; ++level) {
         const int nseg = static_cast<int>(seg.size());
-        std::vector<int32_t> st(nseg), en(nseg), a(nseg, -1), b(nseg, -1);
-        std::vector<int32_t> act;   // segments split at this level
+        // the segments split at this level, concatenated (active_segment)
+        std::vector<int32_t> ast, aoff(1, 0), aa;
+        std::vector<int64_t> moff(1, 0);
         for (int g = 0; g < nseg; ++g) {
-            st[g] = seg[g].start;
-            en[g] = seg[g].start + seg[g].len;
-            if (seg[g].len > TREE_LEAF) {
-                act.push_back(g);
-                a[g] = st[g] + static_cast<int32_t>(next() % static_cast<uint64_t>(seg[g].len));
-            }
+            if (seg[g].len <= TREE_LEAF) continue;
+            ast.push_back(seg[g].start);
+            aa.push_back(seg[g].start + static_cast<int32_t>(next() % static_cast<uint64_t>(seg[g].len)));
+            aoff.push_back(aoff.back() + seg[g].len);
+            moff.push_back(moff.back() + (gap_window_last(seg[g].len) - gap_window_first(seg[g].len) + 1));
         }
-        if (act.empty()) break;
-        d_start.reserve(nseg, s);
-        d_end.reserve(nseg, s);
-        d_a.reserve(nseg, s);
-        d_b.reserve(nseg, s);
-        d_far.reserve(nseg, s);
-        UMAPB_CUDA(cudaMemcpyAsync(d_start.get(), st.data(), nseg * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-        UMAPB_CUDA(cudaMemcpyAsync(d_end.get(), en.data(), nseg * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-        UMAPB_CUDA(cudaMemcpyAsync(d_a.get(), a.data(), nseg * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-        // b: the segment's point farthest from a
-        UMAPB_CUDA(cudaMemsetAsync(d_far.get(), 0, nseg * sizeof(unsigned long long), s));
-        far_point_kernel<<<grid_for(n, 256), 256, 0, s>>>(data, dim, n, perm.get(), nseg, d_start.get(), d_a.get(),
-                                                          d_far.get());
-        UMAPB_LAUNCH_CHECK();
-        std::vector<unsigned long long> far(nseg);
-        UMAPB_CUDA(cudaMemcpyAsync(far.data(), d_far.get(), nseg * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-        UMAPB_SYNC(s);   // also: st, en and a above are the copies' sources
-        for (int g : act) {
-            const int32_t p = static_cast<int32_t>(0xffffffffu - static_cast<uint32_t>(far[g] & 0xffffffffu));
-            b[g] = (far[g] != 0 && p >= st[g] && p < en[g]) ? p : st[g] + static_cast<int32_t>(next() % static_cast<uint64_t>(seg[g].len));
-        }
-        UMAPB_CUDA(cudaMemcpyAsync(d_b.get(), b.data(), nseg * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-        rp_keys_kernel<<<grid_for(n, 256), 256, 0, s>>>(data, dim, n, perm.get(), nseg, d_start.get(), d_a.get(),
-                                                        d_b.get(), keys.get());
-        UMAPB_LAUNCH_CHECK();
-        int seg_bits = 1;
-        while ((1 << seg_bits) < nseg) ++seg_bits;
-        size_t tb = 0;
-        UMAPB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys.get(), keys2.get(), perm.get(), perm2.get(), n, 0,
-                                                   32 + seg_bits, s));
-        {
-            DevArray<unsigned char> temp(tb, s);
-            UMAPB_CUDA(cub::DeviceRadixSort::SortPairs(temp.get(), tb, keys.get(), keys2.get(), perm.get(), perm2.get(),
-                                                       n, 0, 32 + seg_bits, s));
-        }
-        std::swap(perm, perm2);
-        // widest gap of the sorted projections in the middle half of each split segment
-        const int nact = static_cast<int>(act.size());
-        std::vector<int32_t> ast(nact), aen(nact);
-        std::vector<int64_t> moff(nact + 1, 0);
-        std::vector<float> spread(nact);
-        for (int j = 0; j < nact; ++j) {
-            ast[j] = st[act[j]];
-            aen[j] = en[act[j]];
-            const int32_t len = aen[j] - ast[j];
-            moff[j + 1] = moff[j] + (gap_window_last(len) - gap_window_first(len) + 1);
-        }
-        DevArray<int32_t> d_ast(nact, s), d_aen(nact, s);
+        const int nact = static_cast<int>(ast.size());
+        if (nact == 0) break;
+        const int64_t total = aoff[nact];
+        DevArray<int32_t> d_ast(nact, s), d_aoff(nact + 1, s), d_aa(nact, s);
         DevArray<int64_t> d_moff(nact + 1, s);
-        DevArray<unsigned long long> d_best(nact, s);
+        DevArray<unsigned long long> d_far(nact, s), d_best(nact, s);
         DevArray<float> d_lo(nact, s), d_hi(nact, s);
         UMAPB_CUDA(cudaMemcpyAsync(d_ast.get(), ast.data(), nact * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-        UMAPB_CUDA(cudaMemcpyAsync(d_aen.get(), aen.data(), nact * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+        UMAPB_CUDA(cudaMemcpyAsync(d_aoff.get(), aoff.data(), (nact + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+        UMAPB_CUDA(cudaMemcpyAsync(d_aa.get(), aa.data(), nact * sizeof(int32_t), cudaMemcpyHostToDevice, s));
         UMAPB_CUDA(cudaMemcpyAsync(d_moff.get(), moff.data(), (nact + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+        // direction: from a to the segment's point farthest from a
+        d_far.zero(s);
+        far_point_kernel<<<grid_for(static_cast<size_t>(total), 256), 256, 0, s>>>(
+            data, dim, perm.get(), nact, d_aoff.get(), d_ast.get(), d_aa.get(), total, d_far.get());
+        UMAPB_LAUNCH_CHECK();
+        rp_keys_kernel<<<grid_for(static_cast<size_t>(total), 256), 256, 0, s>>>(
+            data, dim, perm.get(), nact, d_aoff.get(), d_ast.get(), d_aa.get(), d_far.get(), total, keys.get(),
+            vals.get());
+        UMAPB_LAUNCH_CHECK();
+        int seg_bits = 1;
+        while ((1 << seg_bits) < nact) ++seg_bits;
+        size_t tb = 0;
+        UMAPB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys.get(), keys2.get(), vals.get(), vals2.get(),
+                                                   static_cast<int>(total), 0, 32 + seg_bits, s));
+        {
+            DevArray<unsigned char> temp(tb, s);
+            UMAPB_CUDA(cub::DeviceRadixSort::SortPairs(temp.get(), tb, keys.get(), keys2.get(), vals.get(), vals2.get(),
+                                                       static_cast<int>(total), 0, 32 + seg_bits, s));
+        }
+        scatter_active_kernel<<<grid_for(static_cast<size_t>(total), 256), 256, 0, s>>>(nact, d_aoff.get(), d_ast.get(),
+                                                                                      total, vals2.get(), perm.get());
+        UMAPB_LAUNCH_CHECK();
+        // widest gap of the sorted projections in each active segment's window,
+        // on the sorted items (segment j: items [aoff[j], aoff[j + 1]))
         d_best.zero(s);
         widest_gap_kernel<<<grid_for(static_cast<size_t>(moff[nact]), 256), 256, 0, s>>>(
-            keys2.get(), nact, d_ast.get(), d_aen.get(), d_moff.get(), moff[nact], d_best.get());
+            keys2.get(), nact, d_aoff.get(), d_aoff.get() + 1, d_moff.get(), moff[nact], d_best.get());
         UMAPB_LAUNCH_CHECK();
-        middle_spread_kernel<<<grid_for(nact, 128), 128, 0, s>>>(keys2.get(), nact, d_ast.get(), d_aen.get(), d_lo.get(),
-                                                                 d_hi.get());
+        middle_spread_kernel<<<grid_for(nact, 128), 128, 0, s>>>(keys2.get(), nact, d_aoff.get(), d_aoff.get() + 1,
+                                                                 d_lo.get(), d_hi.get());
         UMAPB_LAUNCH_CHECK();
         std::vector<unsigned long long> best(nact);
-        std::vector<float> klo(nact), khi(nact);
+        std::vector<float> klo(nact), khi(nact), spread(nact);
         UMAPB_CUDA(cudaMemcpyAsync(best.data(), d_best.get(), nact * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
         UMAPB_CUDA(cudaMemcpyAsync(klo.data(), d_lo.get(), nact * sizeof(float), cudaMemcpyDeviceToHost, s));
         UMAPB_CUDA(cudaMemcpyAsync(khi.data(), d_hi.get(), nact * sizeof(float), cudaMemcpyDeviceToHost, s));
@@ -597,7 +628,7 @@ void knn_tile_tasks(const float* data, int32_t dim, const KnnTiles& t, const std
     UMAPB_CUDA(cudaMemcpyAsync(d_tile0.get(), tile0.data(), ntiles * sizeof(int32_t), cudaMemcpyHostToDevice, s));
     UMAPB_CUDA(cudaMemcpyAsync(d_ntl.get(), ntl.data(), ntiles * sizeof(int32_t), cudaMemcpyHostToDevice, s));
     UMAPB_CUDA(cudaMemcpyAsync(out.qlist_off.get(), ho.data(), ntiles * sizeof(int64_t), cudaMemcpyHostToDevice, s));
-    const unsigned warps_grid = static_cast<unsigned>((ntiles + LIST_WARPS - 1) / LIST_WARPS);
+    const unsigned warps_grid = static_cast<unsigned>((ntiles + LIST_WARPS * LIST_QB - 1) / (LIST_WARPS * LIST_QB));
     DevArray<float> tkth;
     if (prune && k <= KTH_MAX) {
         tkth.allocate(ntiles, s);
@@ -674,6 +705,21 @@ __global__ void task_rows_flag_kernel(const int4* __restrict__ tasks, const int3
 }
 }  // namespace
 
+namespace {
+struct IsRow {
+    __device__ __forceinline__ bool operator()(int32_t r) const { return r >= 0; }
+};
+}  // namespace
+
+void knn_tree_rows(const KnnTiles& t, int32_t n, DevArray<int32_t>& rows, cudaStream_t s) {
+    rows.allocate(std::max<int32_t>(n, 1), s);
+    DevArray<int32_t> d_count(1, s);
+    size_t tb = 0;
+    UMAPB_CUDA(cub::DeviceSelect::If(nullptr, tb, t.row_map.get(), rows.get(), d_count.get(), t.n_pad, IsRow(), s));
+    DevArray<unsigned char> temp(tb, s);
+    UMAPB_CUDA(cub::DeviceSelect::If(temp.get(), tb, t.row_map.get(), rows.get(), d_count.get(), t.n_pad, IsRow(), s));
+}
+
 void knn_task_rows(const KnnTiles& t, const KnnTasks& tk, int32_t n, DevArray<int32_t>& rows, int32_t& count,
                    cudaStream_t s) {
     DevArray<uint8_t> flag(n, s);
@@ -685,7 +731,7 @@ void knn_task_rows(const KnnTiles& t, const KnnTasks& tk, int32_t n, DevArray<in
     }
     rows.allocate(std::max<int32_t>(n, 1), s);
     DevArray<int32_t> d_count(1, s);
-    cub::CountingInputIterator<int32_t> it(0);
+    thrust::counting_iterator<int32_t> it(0);
     size_t tb = 0;
     UMAPB_CUDA(cub::DeviceSelect::Flagged(nullptr, tb, it, flag.get(), rows.get(), d_count.get(), n, s));
     DevArray<unsigned char> temp(tb, s);

@@ -150,6 +150,36 @@ __global__ void row_order_key_kernel(int32_t n, const int64_t* __restrict__ ptr,
     if ((threadIdx.x & 31) == 0 && hubs) atomicAdd(nhub, hubs);
 }
 
+// The non-hub rows of one epoch in claim order: every chunk of ORDER_GROUP
+// consecutive positions of the run's order (hub rows left out) sorted by
+// descending number of edges that fire in this epoch -- counted by the
+// previous epoch's kernel while it scanned the rows (RowArgs::next_count) --,
+// equal counts in the run's order (a stable sort).  A chunk keeps its
+// positions, so the rows in flight together still come from one index range,
+// while the 32 rows a warp takes fire the same number of edges (and rows that
+// fire none come last).
+constexpr int EPOCH_ORDER_THREADS = 512;
+constexpr int EPOCH_ORDER_ITEMS = ORDER_GROUP / EPOCH_ORDER_THREADS;
+__global__ void __launch_bounds__(EPOCH_ORDER_THREADS)
+    epoch_bulk_order_kernel(const int32_t* __restrict__ run_order, int32_t nbulk, const uint16_t* __restrict__ count,
+                            int32_t* __restrict__ bulk) {
+    using Sort = cub::BlockRadixSort<uint32_t, EPOCH_ORDER_THREADS, EPOCH_ORDER_ITEMS, int32_t>;
+    __shared__ typename Sort::TempStorage tmp;
+    const int64_t first = static_cast<int64_t>(blockIdx.x) * ORDER_GROUP + threadIdx.x * EPOCH_ORDER_ITEMS;
+    uint32_t key[EPOCH_ORDER_ITEMS];
+    int32_t row[EPOCH_ORDER_ITEMS];
+#pragma unroll
+    for (int i = 0; i < EPOCH_ORDER_ITEMS; ++i) {   // blocked: item rank = position in the chunk
+        const int64_t pos = first + i;
+        row[i] = pos < nbulk ? run_order[pos] : -1;
+        key[i] = pos < nbulk ? 0xffffu - count[row[i]] : 0x10000u;   // past the end: last
+    }
+    Sort(tmp).Sort(key, row, 0, 17);
+#pragma unroll
+    for (int i = 0; i < EPOCH_ORDER_ITEMS; ++i)
+        if (first + i < nbulk) bulk[first + i] = row[i];
+}
+
 // ---------------------------------------------------------- epoch kernels --
 
 template <typename T>
@@ -184,6 +214,8 @@ struct RowArgs {
     int* counter;              // claims so far in this epoch: [0] hub rows (or row groups), [1] other rows
     unsigned long long* totals;   // optional: [firing edges, negative samples drawn] of this epoch
     int32_t nhub;              // 2-d kernel: order[0, nhub) are hub rows, one warp each
+    const int32_t* bulk;       // 2-d kernel: the other rows in this epoch's claim order (null: order + nhub)
+    uint16_t* next_count;      // 2-d kernel, optional: receives each non-hub row's firing edges in the next epoch
 };
 
 // Observation range [base, base + size) of the instance that owns h.
@@ -331,6 +363,8 @@ struct RowScan {
     float* w;                  // this lane's column: w[(buffer * BULK_CHUNK + q) * 32]
     unsigned cm;               // firing edges of the current window not yet taken
     int cur;                   // buffer of the current window
+    int n1;                    // edges seen so far that fire at the next epoch (their new state counted
+                               // by lane_row_step for the ones that fire now)
     __device__ __forceinline__ void load(int buf, const float* __restrict__ enext, int64_t b) {
 #pragma unroll
         for (int q = 0; q < BULK_CHUNK; ++q) {
@@ -340,18 +374,32 @@ struct RowScan {
         cp_async_commit();
     }
     __device__ __forceinline__ unsigned fire_mask(int buf, int64_t b, float ef) {
-        unsigned m = 0;
+        // b < r1 here; edges past the row's end are masked off
+        unsigned m = 0, m1 = 0;
+        const float ef1 = ef + 1.0f;   // the next epoch (an integer: exact)
 #pragma unroll
-        for (int q = 0; q < BULK_CHUNK; ++q) m |= (b + q < r1 && w[(buf * BULK_CHUNK + q) * 32] <= ef ? 1u : 0u) << q;
+        for (int q = 0; q < BULK_CHUNK; ++q) {
+            const float v = w[(buf * BULK_CHUNK + q) * 32];
+            m |= (v <= ef ? 1u : 0u) << q;
+            m1 |= (v <= ef1 ? 1u : 0u) << q;
+        }
+        const int64_t left = r1 - b;
+        const unsigned valid = left >= BULK_CHUNK ? (1u << BULK_CHUNK) - 1u : (1u << static_cast<int>(left)) - 1u;
+        m &= valid;
+        n1 += __popc(m1 & valid) - __popc(m);   // fire at the next epoch, not at this one
         return m;
     }
     __device__ __forceinline__ void start(float* column, const float* __restrict__ enext, int64_t j0, int64_t end,
                                           float ef) {
+        // the lane's previous row may have left a window copy in flight into
+        // these buffers: let it land before they are refilled
+        cp_async_wait<0>();
         w = column;
         r1 = end;
         cb = j0;
         nb = j0 + BULK_CHUNK;
         cur = 0;
+        n1 = 0;
         load(0, enext, cb);
         load(1, enext, nb);
         cp_async_wait<1>();
@@ -411,9 +459,15 @@ __device__ __forceinline__ bool lane_row_start(LaneRow& L, int32_t h, const RowA
                                                const P& p, float* column) {
     const float ef = p.epoch;
     const int64_t j0 = r.ptr[h], r1 = r.ptr[h + 1];
-    if (j0 >= r1) return false;
+    if (j0 >= r1) {
+        if (r.next_count) r.next_count[h] = 0;
+        return false;
+    }
     L.sc.start(column, r.enext, j0, r1, ef);
-    if (!lane_row_fetch(L, L.cur, r, ef)) return false;
+    if (!lane_row_fetch(L, L.cur, r, ef)) {   // the whole row scanned: nothing fires now
+        if (r.next_count) r.next_count[h] = static_cast<uint16_t>(min(L.sc.n1, 65535));
+        return false;
+    }
     L.has_nxt = lane_row_fetch(L, L.nxt, r, ef);
     L.h = h;
     const float2 y0 = __ldcg(&Y[h]);
@@ -453,8 +507,10 @@ __device__ __forceinline__ bool lane_row_step(LaneRow& L, const RowArgs<float>& 
             yk[b] = __ldcg(&Y[ks[b]]);
         }
     }
-    r.enext[L.cur.j] = L.cur.en + L.cur.ep;                    // :178-179
+    const float en_new = L.cur.en + L.cur.ep;                 // :178-179
+    r.enext[L.cur.j] = en_new;
     r.enneg[L.cur.j] = L.cur.enn + static_cast<float>(nn) * epns;
+    L.sc.n1 += en_new <= ef + 1.0f ? 1 : 0;
     ++fired;
     drawn += remaining;
     // rotate: nxt becomes cur; fetch the one after
@@ -499,6 +555,8 @@ __device__ __forceinline__ bool lane_row_step(LaneRow& L, const RowArgs<float>& 
     atomicAdd(&Y[h], make_float2(hx - yh.x, hy - yh.y));
     L.hx = hx;
     L.hy = hy;
+    // the row's last firing edge: every window has been scanned
+    if (!more && r.next_count) r.next_count[h] = static_cast<uint16_t>(min(L.sc.n1, 65535));
     return more;
 }
 
@@ -630,7 +688,8 @@ __device__ __forceinline__ void hub_row(int32_t h, const RowArgs<float>& r, floa
 // The epoch: warps first take the hub rows, one per warp, from counter[0];
 // then the other rows 32 at a time from counter[1], one per lane, each loop
 // iteration applying one firing edge of every lane's row (the rows a warp
-// takes have similar lengths, row_order_key_kernel).
+// takes have similar lengths: row_order_key_kernel, and per epoch
+// epoch_bulk_order_kernel).
 template <int NB, int MINB, bool FRESH>
 __global__ void __launch_bounds__(256, MINB) sgd_rows_2d_f32(RowArgs<float> r, float2* __restrict__ Y,
                                                              SgdParams<float> p) {
@@ -647,6 +706,7 @@ __global__ void __launch_bounds__(256, MINB) sgd_rows_2d_f32(RowArgs<float> r, f
         __syncwarp();
     }
     const int32_t nbulk = r.nrows - r.nhub;
+    const int32_t* bulk = r.bulk ? r.bulk : r.order + r.nhub;
     while (true) {
         int32_t base = 0;
         if (lane == 0) base = atomicAdd(&r.counter[1], 32);
@@ -655,7 +715,7 @@ __global__ void __launch_bounds__(256, MINB) sgd_rows_2d_f32(RowArgs<float> r, f
         LaneRow L;
         L.h = -1;
         const int32_t idx = base + lane;
-        if (idx < nbulk && !lane_row_start(L, r.order[r.nhub + idx], r, Y, p, &scan_win[warp][lane])) L.h = -1;
+        if (idx < nbulk && !lane_row_start(L, bulk[idx], r, Y, p, &scan_win[warp][lane])) L.h = -1;
         while (__any_sync(0xffffffffu, L.h >= 0)) {
             if (L.h >= 0 && !lane_row_step<NB, FRESH>(L, r, Y, p, fired, drawn)) L.h = -1;
         }
@@ -749,6 +809,100 @@ __global__ void __launch_bounds__(128) sgd_rows_generic(RowArgs<T> r, T* __restr
         __syncwarp();
     }
     add_totals(r.totals, fired, drawn);
+}
+
+// ------------------------------------------------------------ transform --
+// Out-of-sample embedding (no counterpart in the reference: optimize_layout
+// applied to points added to a finished layout).  Row i of the transform
+// graph holds new point i's nearest reference points with their smoothed
+// similarities; it is optimised like a row of optimize_layout
+// (optimize_layout.hpp:136-180: schedule, attractive step, negative samples,
+// the same arithmetic as sgd_rows_generic) except that only the new point
+// moves: the reference points it is pulled to and the negative samples,
+// drawn among the reference points, stay fixed.  Rows then share nothing that
+// changes, so one thread takes one row through all epochs in one launch and
+// the result does not depend on the launch shape.
+
+// Initial position of every new point: the mean of its neighbours' reference
+// positions weighted by the similarities (FP64 sums in edge order; plain mean
+// if the weights sum to zero).
+template <typename T>
+__global__ void transform_init_kernel(int32_t nq, int dim, const int64_t* __restrict__ ptr,
+                                      const int32_t* __restrict__ idx, const T* __restrict__ w,
+                                      const T* __restrict__ Yref, T* __restrict__ Ynew) {
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) {
+        const int64_t r0 = ptr[i], r1 = ptr[i + 1];
+        double ws = 0;
+        for (int64_t j = r0; j < r1; ++j) ws += static_cast<double>(w[j]);
+        const bool weighted = ws > 0;
+        const double den = weighted ? ws : static_cast<double>(r1 - r0);
+        for (int d = 0; d < dim; ++d) {
+            double acc = 0;
+            for (int64_t j = r0; j < r1; ++j) {
+                const double wj = weighted ? static_cast<double>(w[j]) : 1.0;
+                acc += wj * static_cast<double>(Yref[static_cast<size_t>(idx[j]) * dim + d]);
+            }
+            Ynew[static_cast<size_t>(i) * dim + d] = static_cast<T>(den > 0 ? acc / den : 0.0);
+        }
+    }
+}
+
+// All epochs of every new point's row (thread i: row i).  head0 + i is the
+// point's index in the negative-sample stream's counter; lr is the learning
+// rate in the layout's type.
+template <typename T>
+__global__ void __launch_bounds__(128)
+    transform_sgd_kernel(int32_t nq, int dim, const int64_t* __restrict__ ptr, const int32_t* __restrict__ targets,
+                         const T* __restrict__ eps, T* __restrict__ enext, T* __restrict__ enneg,
+                         const T* __restrict__ Yref, int32_t nref, T* __restrict__ Ynew, int32_t head0, int num_epochs,
+                         T lr, SgdParams<T> p) {
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nq) return;
+    T head[MAX_GENERIC_DIM];
+    T* yh = Ynew + static_cast<size_t>(i) * dim;
+    for (int d = 0; d < dim; ++d) head[d] = yh[d];
+    const int64_t r0 = ptr[i], r1 = ptr[i + 1];
+    const uint32_t hid = static_cast<uint32_t>(head0 + i);
+    for (int e = 0; e < num_epochs; ++e) {
+        const T ef = static_cast<T>(e);
+        // alpha as in the layout's epochs (optimize_layout.hpp:132-133)
+        const T alpha = static_cast<T>(static_cast<double>(lr) *
+                                       (1.0 - static_cast<double>(ef / static_cast<T>(num_epochs))));
+        for (int64_t j = r0; j < r1; ++j) {
+            if (!(enext[j] <= ef)) continue;
+            const T ep = eps[j];
+            const T epns = ep / p.rate;
+            const T enn = enneg[j];
+            const int nn = static_cast<int>((ef - enn) / epns);
+            enext[j] = enext[j] + ep;
+            enneg[j] = enn + static_cast<T>(nn) * epns;
+            const int32_t t = targets[j];
+            const T* yt = Yref + static_cast<size_t>(t) * dim;
+            T d2 = 0;
+            for (int d = 0; d < dim; ++d) {
+                const T diff = head[d] - yt[d];
+                d2 += diff * diff;
+            }
+            {
+                const T c = attract_coef(floor_eps(d2), p);
+                for (int d = 0; d < dim; ++d) head[d] += alpha * clamp4(c * (head[d] - yt[d]));
+            }
+            if (nn > 0) {
+                NegStream rng(hid, static_cast<uint32_t>(t), static_cast<uint32_t>(e), p.k0, p.k1);
+                for (int q = 0; q < nn; ++q) {
+                    const T* yk = Yref + static_cast<size_t>(rng.bounded(static_cast<uint32_t>(nref))) * dim;
+                    T dd2 = 0;
+                    for (int d = 0; d < dim; ++d) {
+                        const T diff = head[d] - yk[d];
+                        dd2 += diff * diff;
+                    }
+                    const T c = repulse_coef(floor_eps(dd2), p);
+                    for (int d = 0; d < dim; ++d) head[d] += alpha * clamp4(c * (head[d] - yk[d]));
+                }
+            }
+        }
+    }
+    for (int d = 0; d < dim; ++d) yh[d] = head[d];
 }
 
 // UMAPB_CHECK_SCHEDULE=1: the epoch kernels count the firing edges and
@@ -940,6 +1094,11 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
         ? std::max<int64_t>(1, std::max<int64_t>(ep_->n / window_div, std::min<int64_t>(ep_->n / 8, 32768)))
         : int64_t(1) << 40;
 
+    const bool eorder = use_2d && epoch_order && ep_->n > nhub_;
+    if (eorder) {
+        next_count_.reserve(ep_->n, s);
+        bulk_.reserve(ep_->n - nhub_, s);
+    }
     // One epoch launch on (Yp, schedule state en/enn), claiming rows from 'counter'.
     auto launch = [&](T* Yp, T* en, T* enn, int* counter, unsigned long long* totals, int e_abs, int block,
                       int variant) {
@@ -959,6 +1118,19 @@ void SgdEngine<T>::run(T* Y, int num_dim, int first, int last, double a, double 
         r.counter = counter;
         r.totals = totals;
         r.nhub = use_2d ? nhub_ : 0;
+        r.bulk = nullptr;
+        r.next_count = nullptr;
+        if (eorder) {
+            r.next_count = next_count_.get();
+            if (e_abs > first) {   // counts from the previous epoch of this call
+                const int32_t nbulk = ep_->n - nhub_;
+                epoch_bulk_order_kernel<<<static_cast<unsigned>((nbulk + ORDER_GROUP - 1) / ORDER_GROUP),
+                                          EPOCH_ORDER_THREADS, 0, s>>>(order_.get() + nhub_, nbulk,
+                                                                      next_count_.get(), bulk_.get());
+                UMAPB_LAUNCH_CHECK();
+                r.bulk = bulk_.get();
+            }
+        }
         if (use_2d) {
             if constexpr (std::is_same<T, float>::value) {
                 int64_t g = static_cast<int64_t>(sm_count()) * sgd_2d_resident(variant, block);
@@ -1084,6 +1256,13 @@ int SgdEngine<T>::default_window_div() {
     return (x >= 0 && x <= 1 << 20) ? x : 12;
 }
 
+// UMAPB_SGD_EPOCH_ORDER=0 keeps the run's claim order in every epoch.
+template <typename T>
+bool SgdEngine<T>::default_epoch_order() {
+    const char* e = std::getenv("UMAPB_SGD_EPOCH_ORDER");
+    return !(e && std::atoi(e) == 0);
+}
+
 // UMAPB_SGD_PUBLISH_EVERY: firing edges between publications of a row's head
 // (default 1: after every firing edge).
 template <typename T>
@@ -1095,5 +1274,52 @@ int SgdEngine<T>::default_publish_every() {
 
 template class SgdEngine<float>;
 template class SgdEngine<double>;
+
+template <typename T>
+void transform_init(int32_t nq, int num_dim, const int64_t* ptr, const int32_t* idx, const T* w, const T* Yref,
+                    T* Ynew, cudaStream_t s) {
+    if (nq <= 0) return;
+    transform_init_kernel<T><<<grid_for(nq, 128), 128, 0, s>>>(nq, num_dim, ptr, idx, w, Yref, Ynew);
+    UMAPB_LAUNCH_CHECK();
+}
+
+template <typename T>
+void transform_layout(const DeviceEpochs<T>& ep, int num_dim, const T* Yref, int32_t nref, T* Ynew, int32_t head0,
+                      double a, double b, double gamma, double learning_rate, uint64_t seed, cudaStream_t s) {
+    require(num_dim >= 1 && num_dim <= MAX_GENERIC_DIM, "num_dim must be between 1 and 64");
+    require(nref >= 1, "the transform needs at least one reference point");
+    const int32_t nq = ep.n;
+    if (nq <= 0) return;
+    SgdParams<T> p{};
+    p.a = static_cast<T>(a);
+    p.b = static_cast<T>(b);
+    p.neg2ab = T(-2) * p.a * p.b;
+    p.gamma2b = T(2) * static_cast<T>(gamma) * p.b;
+    p.rate = ep.negative_sample_rate;
+    p.k0 = static_cast<uint32_t>(seed) ^ RNG_NEGATIVE;
+    p.k1 = static_cast<uint32_t>(seed >> 32);
+    p.n = nref;
+    p.publish_every = 1;
+    p.inst_start = nullptr;
+    p.num_inst = 1;
+    DevArray<T> en(std::max<int64_t>(ep.nnz, 1), s), enn(std::max<int64_t>(ep.nnz, 1), s);
+    if (ep.nnz) {
+        UMAPB_CUDA(cudaMemcpyAsync(en.get(), ep.enext0.get(), ep.nnz * sizeof(T), cudaMemcpyDeviceToDevice, s));
+        UMAPB_CUDA(cudaMemcpyAsync(enn.get(), ep.enneg0.get(), ep.nnz * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    }
+    transform_sgd_kernel<T><<<static_cast<unsigned>((nq + 127) / 128), 128, 0, s>>>(
+        nq, num_dim, ep.ptr.get(), ep.targets.get(), ep.eps.get(), en.get(), enn.get(), Yref, nref, Ynew, head0,
+        ep.total_epochs, static_cast<T>(learning_rate), p);
+    UMAPB_LAUNCH_CHECK();
+}
+
+template void transform_init<float>(int32_t, int, const int64_t*, const int32_t*, const float*, const float*, float*,
+                                    cudaStream_t);
+template void transform_init<double>(int32_t, int, const int64_t*, const int32_t*, const double*, const double*,
+                                     double*, cudaStream_t);
+template void transform_layout<float>(const DeviceEpochs<float>&, int, const float*, int32_t, float*, int32_t, double,
+                                      double, double, double, uint64_t, cudaStream_t);
+template void transform_layout<double>(const DeviceEpochs<double>&, int, const double*, int32_t, double*, int32_t,
+                                       double, double, double, double, uint64_t, cudaStream_t);
 
 }  // namespace umapb

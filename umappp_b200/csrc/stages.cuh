@@ -62,7 +62,8 @@ bool knn_tc_supported(int32_t dim, int kcap);
 // the search in use cannot be sharded.
 bool knn_tc_candidates(const float* data, int32_t n, int32_t dim, int kcap, int32_t* cand_idx, float* cand_d2,
                        float* norms_out, int* d_err, cudaStream_t s, KnnShard shard = KnnShard(),
-                       DevArray<int32_t>* shard_rows = nullptr, int32_t* shard_count = nullptr);
+                       DevArray<int32_t>* shard_rows = nullptr, int32_t* shard_count = nullptr,
+                       DevArray<int32_t>* tree_rows = nullptr);
 // Batched: instance i is data rows [inst[i], inst[i + 1]) (host vector).
 void knn_tc_candidates_batched(const float* data, const std::vector<int32_t>& inst, int32_t dim, int kcap,
                                int32_t* cand_idx, float* cand_d2, int* d_err, cudaStream_t s);
@@ -87,6 +88,8 @@ struct KnnTasks {
 };
 // Data rows of the query tiles of a task list (ascending): the rows a sharded
 // search computes.
+// The data rows in tree order (the operand rows without padding): n entries.
+void knn_tree_rows(const KnnTiles& t, int32_t n, DevArray<int32_t>& rows, cudaStream_t s);
 void knn_task_rows(const KnnTiles& t, const KnnTasks& tk, int32_t n, DevArray<int32_t>& rows, int32_t& count,
                    cudaStream_t s);
 // tree == false keeps each instance in data order.
@@ -122,6 +125,15 @@ double& last_knn_tc_error();
 
 // Exact kNN of every observation within its own instance (instance i is data
 // rows [inst[i], inst[i + 1]), host vector); indices are data rows.
+// Exact Euclidean neighbours of nq query points among nref reference points:
+// 'data' holds the reference rows [0, nref) followed by the query rows
+// [nref, nref + nq); out_idx/out_dist are nq x k in query order, reference
+// indices sorted by (distance, index).  Float data: FP32 candidates, FP64
+// rescoring and certification; double data: FP64 throughout.
+template <typename T>
+void knn_query(const T* data, int32_t nref, int32_t nq, int32_t dim, int32_t k, int32_t* out_idx, T* out_dist,
+               cudaStream_t s);
+
 template <typename T>
 void knn_exact_batched(const T* data, const std::vector<int32_t>& inst, int32_t dim, int32_t k, int32_t* out_idx,
                        T* out_dist, cudaStream_t s);
@@ -193,6 +205,10 @@ public:
     int publish_every = default_publish_every();
     // Rows in flight at most n / window_div (sgd.cu, run(); 0: no cap).
     int window_div = default_window_div();
+    // 2-d kernel: each epoch after the first of a run() call claims its rows
+    // sorted by this epoch's firing edges within chunks of the run's order
+    // (sgd.cu, epoch_bulk_order_kernel).
+    bool epoch_order = default_epoch_order();
     int block_size() const { return block_; }
     int variant() const { return variant_; }   // 2-d kernel variant (sgd.cu, SGD_2D_VARIANTS)
 
@@ -202,8 +218,11 @@ private:
     static int default_variant();
     static int default_publish_every();
     static int default_window_div();
+    static bool default_epoch_order();
     int block_ = 256, variant_ = default_variant();
     const DeviceEpochs<T>* ep_ = nullptr;
+    DevArray<uint16_t> next_count_;   // per row: firing edges in the next epoch
+    DevArray<int32_t> bulk_;          // this epoch's claim order of the non-hub rows
     const int32_t* inst_start_ = nullptr;
     int32_t num_inst_ = 1;
     int base_epoch_ = 0;
@@ -214,6 +233,20 @@ private:
 };
 
 // ---- adjoint (adjoint.cu) ----------------------------------------------------
+// ---- transform (sgd.cu) -------------------------------------------------------
+// Out-of-sample embedding of nq new points against a fixed reference layout
+// Yref (nref points): transform_init puts every new point at the
+// similarity-weighted mean of its neighbours' positions (CSR ptr/idx/w over
+// the new points, reference indices); transform_layout then runs the
+// schedule 'ep' (rows = new points, targets = reference points) with only the
+// new points moving and negative samples drawn among the reference points.
+template <typename T>
+void transform_init(int32_t nq, int num_dim, const int64_t* ptr, const int32_t* idx, const T* w, const T* Yref,
+                    T* Ynew, cudaStream_t s);
+template <typename T>
+void transform_layout(const DeviceEpochs<T>& ep, int num_dim, const T* Yref, int32_t nref, T* Ynew, int32_t head0,
+                      double a, double b, double gamma, double learning_rate, uint64_t seed, cudaStream_t s);
+
 template <typename T>
 void loss_grad(int32_t n, int num_dim, const T* Y, const int64_t* ptr, const int32_t* idx, const T* w, double a,
                double b, double eps_rep, bool with_constant, double* loss_out, T* grad_Y, double* grad_ab,
