@@ -31,6 +31,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 
 #include "stages.cuh"
@@ -463,6 +464,19 @@ bool prune_enabled() {
     return !(e && std::strcmp(e, "0") == 0);
 }
 
+// Launch-shape tuner of the FP16 search: per (K chunks, size class = log2 of
+// the operand tiles) the query tiles per CTA whose kernel ran fastest, timed
+// once on the first search of the class in the process; UMAPB_KNN_QT = 1 or
+// 2 forces a shape where it exists.
+struct ShapeTuner {
+    std::mutex mu;
+    std::map<std::pair<int, int>, int> best;
+};
+ShapeTuner& shape_tuner() {
+    static ShapeTuner t;
+    return t;
+}
+
 // FP16 search over the (pruned) tile lists of the instances 'inst'.
 void run_f16_pruned(const float* data, const std::vector<int32_t>& inst, int32_t dim, int kcap, float scale,
                     int32_t* cand_idx, float* cand_d2, float* norms_by_row, int* d_err, cudaStream_t s,
@@ -472,11 +486,49 @@ void run_f16_pruned(const float* data, const std::vector<int32_t>& inst, int32_t
     KnnTiles tiles;
     knn_tree_order(data, dim, inst, prune, tiles, s);
     if (tree_rows) knn_tree_rows(tiles, inst.back(), *tree_rows, s);
+    const std::vector<int> shapes = knn_tc16_shapes(dim);
+    int qt = shapes.front();
+    bool tune = false;
+    std::pair<int, int> key((dim + 1 + 63) / 64, 0);
+    while ((int64_t(1) << key.second) < tiles.n_pad / 128) ++key.second;
+    if (const char* e = std::getenv("UMAPB_KNN_QT")) {
+        const int want = std::atoi(e);
+        for (int c : shapes)
+            if (c == want) qt = c;
+    } else if (shapes.size() > 1 && shard.count == 1) {
+        ShapeTuner& t = shape_tuner();
+        std::lock_guard<std::mutex> lock(t.mu);
+        auto it = t.best.find(key);
+        if (it != t.best.end()) qt = it->second;
+        else tune = true;
+    }
+    if (tune) {
+        // every shape computes the same candidate lists: time each, keep the
+        // fastest for the class; the last run's lists are the result
+        float best_ms = 0.0f;
+        int best_qt = qt;
+        for (size_t i = 0; i < shapes.size(); ++i) {
+            KnnTasks tasks;
+            knn_tile_tasks(data, dim, tiles, inst, shapes[i], kcap, prune, tasks, s, shard);
+            knn_tc16_run_tasks(data, dim, kcap, scale, tiles, tasks, cand_idx, cand_d2, norms_by_row, d_err, s,
+                               &last_knn_kernel_ms(), shapes[i]);
+            last_knn_tiles_scanned() = tasks.total_tiles;
+            UMAPB_SYNC(s);
+            if (i == 0 || last_knn_kernel_ms() < best_ms) {
+                best_ms = last_knn_kernel_ms();
+                best_qt = shapes[i];
+            }
+        }
+        ShapeTuner& t = shape_tuner();
+        std::lock_guard<std::mutex> lock(t.mu);
+        t.best[key] = best_qt;
+        return;
+    }
     KnnTasks tasks;
-    knn_tile_tasks(data, dim, tiles, inst, knn_tc16_query_tiles(dim), kcap, prune, tasks, s, shard);
+    knn_tile_tasks(data, dim, tiles, inst, qt, kcap, prune, tasks, s, shard);
     if (shard_rows) knn_task_rows(tiles, tasks, inst.back(), *shard_rows, *shard_count, s);
     knn_tc16_run_tasks(data, dim, kcap, scale, tiles, tasks, cand_idx, cand_d2, norms_by_row, d_err, s,
-                       &last_knn_kernel_ms());
+                       &last_knn_kernel_ms(), qt);
     last_knn_tiles_scanned() = tasks.total_tiles;
     UMAPB_SYNC(s);   // the tile and task buffers are released below
 }
