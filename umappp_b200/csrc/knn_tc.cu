@@ -466,8 +466,8 @@ bool prune_enabled() {
 
 // Launch-shape tuner of the FP16 search: per (K chunks, size class = log2 of
 // the operand tiles) the query tiles per CTA whose kernel ran fastest, timed
-// once on the first search of the class in the process; UMAPB_KNN_QT = 1 or
-// 2 forces a shape where it exists.
+// once on the first unsharded search of the class in the process;
+// UMAPB_KNN_QT = 1 or 2 forces a shape where it exists.
 struct ShapeTuner {
     std::mutex mu;
     std::map<std::pair<int, int>, int> best;
@@ -496,6 +496,9 @@ void run_f16_pruned(const float* data, const std::vector<int32_t>& inst, int32_t
         for (int c : shapes)
             if (c == want) qt = c;
     } else if (shapes.size() > 1 && shard.count == 1) {
+        // (a sharded search keeps the default shape: the shards' task lists,
+        // and with them the rows each rank computes, must agree across ranks
+        // whatever each rank's tuner has seen)
         ShapeTuner& t = shape_tuner();
         std::lock_guard<std::mutex> lock(t.mu);
         auto it = t.best.find(key);

@@ -154,7 +154,7 @@ __global__ void row_order_key_kernel(int32_t n, const int64_t* __restrict__ ptr,
 // consecutive positions of the run's order (hub rows left out) sorted by
 // descending number of edges that fire in this epoch -- counted by the
 // previous epoch's kernel while it scanned the rows (RowArgs::next_count) --,
-// equal counts in the run's order (a stable sort).  A chunk keeps its
+// equal counts (and counts of 255 or more) in the run's order (a stable sort).  A chunk keeps its
 // positions, so the rows in flight together still come from one index range,
 // while the 32 rows a warp takes fire the same number of edges (and rows that
 // fire none come last).
@@ -172,9 +172,11 @@ __global__ void __launch_bounds__(EPOCH_ORDER_THREADS)
     for (int i = 0; i < EPOCH_ORDER_ITEMS; ++i) {   // blocked: item rank = position in the chunk
         const int64_t pos = first + i;
         row[i] = pos < nbulk ? run_order[pos] : -1;
-        key[i] = pos < nbulk ? 0xffffu - count[row[i]] : 0x10000u;   // past the end: last
+        // descending count, capped at 255 (non-hub rows fire fewer edges than
+        // that), in 8 bits; past the end: 256, last
+        key[i] = pos < nbulk ? 255u - min(static_cast<uint32_t>(count[row[i]]), 255u) : 256u;
     }
-    Sort(tmp).Sort(key, row, 0, 17);
+    Sort(tmp).Sort(key, row, 0, 9);
 #pragma unroll
     for (int i = 0; i < EPOCH_ORDER_ITEMS; ++i)
         if (first + i < nbulk) bulk[first + i] = row[i];
@@ -485,7 +487,7 @@ __device__ __forceinline__ bool lane_row_start(LaneRow& L, int32_t h, const RowA
 // gathers never wait for its own state); then the updates are applied in the
 // reference's order and the head's move is published.  Returns false when
 // the row has no firing edge left.
-template <int NB, bool FRESH>
+template <int NB, bool FRESH, bool BATCHED_NEG = false>
 __device__ __forceinline__ bool lane_row_step(LaneRow& L, const RowArgs<float>& r, float2* __restrict__ Y,
                                               const SgdParams<float>& p, unsigned long long& fired,
                                               unsigned long long& drawn) {
@@ -531,14 +533,33 @@ __device__ __forceinline__ bool lane_row_step(LaneRow& L, const RowArgs<float>& 
         atomicAdd(&Y[t], make_float2(-gx, -gy));
     }
     while (true) {   // negative samples (:157-176)
+        if constexpr (BATCHED_NEG) {
+            // every sample of the batch against the head as the batch found it
+            // (not the reference's order: a measured option, not the default)
+            float sx = 0.0f, sy = 0.0f;
+            const float bx = hx, by = hy;
 #pragma unroll
-        for (int b = 0; b < NB; ++b) {
-            if (b < m && ks[b] != h) {
-                const float dx = hx - yk[b].x, dy = hy - yk[b].y;
-                const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
-                const float cf = repulse_coef_fast(d2, p);
-                hx = __fmaf_rn(p.alpha, clamp4(cf * dx), hx);
-                hy = __fmaf_rn(p.alpha, clamp4(cf * dy), hy);
+            for (int b = 0; b < NB; ++b) {
+                if (b < m && ks[b] != h) {
+                    const float dx = bx - yk[b].x, dy = by - yk[b].y;
+                    const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
+                    const float cf = repulse_coef_fast(d2, p);
+                    sx += clamp4(cf * dx);
+                    sy += clamp4(cf * dy);
+                }
+            }
+            hx = __fmaf_rn(p.alpha, sx, hx);
+            hy = __fmaf_rn(p.alpha, sy, hy);
+        } else {
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                if (b < m && ks[b] != h) {
+                    const float dx = hx - yk[b].x, dy = hy - yk[b].y;
+                    const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
+                    const float cf = repulse_coef_fast(d2, p);
+                    hx = __fmaf_rn(p.alpha, clamp4(cf * dx), hx);
+                    hy = __fmaf_rn(p.alpha, clamp4(cf * dy), hy);
+                }
             }
         }
         remaining -= m;
@@ -690,7 +711,7 @@ __device__ __forceinline__ void hub_row(int32_t h, const RowArgs<float>& r, floa
 // iteration applying one firing edge of every lane's row (the rows a warp
 // takes have similar lengths: row_order_key_kernel, and per epoch
 // epoch_bulk_order_kernel).
-template <int NB, int MINB, bool FRESH>
+template <int NB, int MINB, bool FRESH, bool BATCHED_NEG = false>
 __global__ void __launch_bounds__(256, MINB) sgd_rows_2d_f32(RowArgs<float> r, float2* __restrict__ Y,
                                                              SgdParams<float> p) {
     __shared__ HubEvent<NB> hub_ev[256 / 32][32];
@@ -717,7 +738,7 @@ __global__ void __launch_bounds__(256, MINB) sgd_rows_2d_f32(RowArgs<float> r, f
         const int32_t idx = base + lane;
         if (idx < nbulk && !lane_row_start(L, bulk[idx], r, Y, p, &scan_win[warp][lane])) L.h = -1;
         while (__any_sync(0xffffffffu, L.h >= 0)) {
-            if (L.h >= 0 && !lane_row_step<NB, FRESH>(L, r, Y, p, fired, drawn)) L.h = -1;
+            if (L.h >= 0 && !lane_row_step<NB, FRESH, BATCHED_NEG>(L, r, Y, p, fired, drawn)) L.h = -1;
         }
     }
     add_totals(r.totals, fired, drawn);
@@ -737,6 +758,7 @@ const Sgd2dVariant SGD_2D_VARIANTS[] = {
     {sgd_rows_2d_f32<8, 2, false>, 8, 2},
     {sgd_rows_2d_f32<6, 2, true>, 6, 2},     // head re-read before every firing edge
     {sgd_rows_2d_f32<4, 2, false>, 4, 2},
+    {sgd_rows_2d_f32<5, 2, false, true>, 5, 2},   // a batch's negative samples against one head position
 };
 constexpr int NUM_SGD_2D_VARIANTS = sizeof(SGD_2D_VARIANTS) / sizeof(SGD_2D_VARIANTS[0]);
 
