@@ -487,7 +487,7 @@ __device__ __forceinline__ bool lane_row_start(LaneRow& L, int32_t h, const RowA
 // gathers never wait for its own state); then the updates are applied in the
 // reference's order and the head's move is published.  Returns false when
 // the row has no firing edge left.
-template <int NB, bool FRESH, bool BATCHED_NEG = false>
+template <int NB, bool FRESH>
 __device__ __forceinline__ bool lane_row_step(LaneRow& L, const RowArgs<float>& r, float2* __restrict__ Y,
                                               const SgdParams<float>& p, unsigned long long& fired,
                                               unsigned long long& drawn) {
@@ -533,33 +533,14 @@ __device__ __forceinline__ bool lane_row_step(LaneRow& L, const RowArgs<float>& 
         atomicAdd(&Y[t], make_float2(-gx, -gy));
     }
     while (true) {   // negative samples (:157-176)
-        if constexpr (BATCHED_NEG) {
-            // every sample of the batch against the head as the batch found it
-            // (not the reference's order: a measured option, not the default)
-            float sx = 0.0f, sy = 0.0f;
-            const float bx = hx, by = hy;
 #pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                if (b < m && ks[b] != h) {
-                    const float dx = bx - yk[b].x, dy = by - yk[b].y;
-                    const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
-                    const float cf = repulse_coef_fast(d2, p);
-                    sx += clamp4(cf * dx);
-                    sy += clamp4(cf * dy);
-                }
-            }
-            hx = __fmaf_rn(p.alpha, sx, hx);
-            hy = __fmaf_rn(p.alpha, sy, hy);
-        } else {
-#pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                if (b < m && ks[b] != h) {
-                    const float dx = hx - yk[b].x, dy = hy - yk[b].y;
-                    const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
-                    const float cf = repulse_coef_fast(d2, p);
-                    hx = __fmaf_rn(p.alpha, clamp4(cf * dx), hx);
-                    hy = __fmaf_rn(p.alpha, clamp4(cf * dy), hy);
-                }
+        for (int b = 0; b < NB; ++b) {
+            if (b < m && ks[b] != h) {
+                const float dx = hx - yk[b].x, dy = hy - yk[b].y;
+                const float d2 = floor_eps(__fmaf_rn(dx, dx, dy * dy));
+                const float cf = repulse_coef_fast(d2, p);
+                hx = __fmaf_rn(p.alpha, clamp4(cf * dx), hx);
+                hy = __fmaf_rn(p.alpha, clamp4(cf * dy), hy);
             }
         }
         remaining -= m;
@@ -711,7 +692,7 @@ __device__ __forceinline__ void hub_row(int32_t h, const RowArgs<float>& r, floa
 // iteration applying one firing edge of every lane's row (the rows a warp
 // takes have similar lengths: row_order_key_kernel, and per epoch
 // epoch_bulk_order_kernel).
-template <int NB, int MINB, bool FRESH, bool BATCHED_NEG = false>
+template <int NB, int MINB, bool FRESH>
 __global__ void __launch_bounds__(256, MINB) sgd_rows_2d_f32(RowArgs<float> r, float2* __restrict__ Y,
                                                              SgdParams<float> p) {
     __shared__ HubEvent<NB> hub_ev[256 / 32][32];
@@ -738,7 +719,7 @@ __global__ void __launch_bounds__(256, MINB) sgd_rows_2d_f32(RowArgs<float> r, f
         const int32_t idx = base + lane;
         if (idx < nbulk && !lane_row_start(L, bulk[idx], r, Y, p, &scan_win[warp][lane])) L.h = -1;
         while (__any_sync(0xffffffffu, L.h >= 0)) {
-            if (L.h >= 0 && !lane_row_step<NB, FRESH, BATCHED_NEG>(L, r, Y, p, fired, drawn)) L.h = -1;
+            if (L.h >= 0 && !lane_row_step<NB, FRESH>(L, r, Y, p, fired, drawn)) L.h = -1;
         }
     }
     add_totals(r.totals, fired, drawn);
@@ -758,7 +739,6 @@ const Sgd2dVariant SGD_2D_VARIANTS[] = {
     {sgd_rows_2d_f32<8, 2, false>, 8, 2},
     {sgd_rows_2d_f32<6, 2, true>, 6, 2},     // head re-read before every firing edge
     {sgd_rows_2d_f32<4, 2, false>, 4, 2},
-    {sgd_rows_2d_f32<5, 2, false, true>, 5, 2},   // a batch's negative samples against one head position
 };
 constexpr int NUM_SGD_2D_VARIANTS = sizeof(SGD_2D_VARIANTS) / sizeof(SGD_2D_VARIANTS[0]);
 
