@@ -63,17 +63,18 @@ def test_knn_shards_partition_and_reproduce_full_search(umap, workload, dtype, n
 
 
 def test_knn_launch_shapes_agree_and_are_exact(umap, monkeypatch):
-    """Both launch shapes of the FP16 search for dim <= 63 (two query tiles per
-    CTA, or one per CTA with two CTAs per SM; UMAPB_KNN_QT forces one) give
-    the same lists, equal to the FP64 oracle on sampled rows."""
+    """The launch shapes of the FP16 search for dim <= 63 (UMAPB_KNN_SHAPE: 24
+    = two query tiles per CTA, 4-stage ring; 12 = one query tile, 2-stage
+    ring, two CTAs per SM) give the same lists, equal to the FP64 oracle on
+    sampled rows."""
     X = bench.make_data("mixture_100k")
     k = bench.CONFIGS["mixture_100k"][5]
     out = {}
-    for qt in ("1", "2"):
-        monkeypatch.setenv("UMAPB_KNN_QT", qt)
-        out[qt] = umap.knn(X, k)
-    monkeypatch.delenv("UMAPB_KNN_QT")
-    assert np.array_equal(out["1"][0], out["2"][0]) and np.array_equal(out["1"][1], out["2"][1])
+    for shape in ("24", "12"):
+        monkeypatch.setenv("UMAPB_KNN_SHAPE", shape)
+        out[shape] = umap.knn(X, k)
+    monkeypatch.delenv("UMAPB_KNN_SHAPE")
+    assert np.array_equal(out["12"][0], out["24"][0]) and np.array_equal(out["12"][1], out["24"][1])
     rows = sampled_rows(X.shape[0], 4, 125, seed=9)
     ridx, rdist = oracle_knn_rows(X, k, rows, 125)
-    assert same_neighbors(out["1"][0][rows], ridx, rdist) == 0
+    assert same_neighbors(out["12"][0][rows], ridx, rdist) == 0

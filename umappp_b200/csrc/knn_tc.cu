@@ -465,9 +465,9 @@ bool prune_enabled() {
 }
 
 // Launch-shape tuner of the FP16 search: per (K chunks, size class = log2 of
-// the operand tiles) the query tiles per CTA whose kernel ran fastest, timed
-// once on the first unsharded search of the class in the process;
-// UMAPB_KNN_QT = 1 or 2 forces a shape where it exists.
+// the operand tiles) the launch shape whose kernel ran fastest, timed once on
+// the first unsharded search of the class in the process; UMAPB_KNN_SHAPE
+// (24 or 12) or UMAPB_KNN_QT (2 or 1) forces one where it exists.
 struct ShapeTuner {
     std::mutex mu;
     std::map<std::pair<int, int>, int> best;
@@ -487,14 +487,16 @@ void run_f16_pruned(const float* data, const std::vector<int32_t>& inst, int32_t
     knn_tree_order(data, dim, inst, prune, tiles, s);
     if (tree_rows) knn_tree_rows(tiles, inst.back(), *tree_rows, s);
     const std::vector<int> shapes = knn_tc16_shapes(dim);
-    int qt = shapes.front();
+    int shape = shapes.front();
     bool tune = false;
     std::pair<int, int> key((dim + 1 + 63) / 64, 0);
     while ((int64_t(1) << key.second) < tiles.n_pad / 128) ++key.second;
-    if (const char* e = std::getenv("UMAPB_KNN_QT")) {
-        const int want = std::atoi(e);
+    int want = 0;
+    if (const char* e = std::getenv("UMAPB_KNN_SHAPE")) want = std::atoi(e);
+    else if (const char* e = std::getenv("UMAPB_KNN_QT")) want = std::atoi(e) == 1 ? 12 : std::atoi(e) == 2 ? 24 : 0;
+    if (want) {
         for (int c : shapes)
-            if (c == want) qt = c;
+            if (c == want) shape = c;
     } else if (shapes.size() > 1 && shard.count == 1) {
         // (a sharded search keeps the default shape: the shards' task lists,
         // and with them the rows each rank computes, must agree across ranks
@@ -502,36 +504,36 @@ void run_f16_pruned(const float* data, const std::vector<int32_t>& inst, int32_t
         ShapeTuner& t = shape_tuner();
         std::lock_guard<std::mutex> lock(t.mu);
         auto it = t.best.find(key);
-        if (it != t.best.end()) qt = it->second;
+        if (it != t.best.end()) shape = it->second;
         else tune = true;
     }
     if (tune) {
         // every shape computes the same candidate lists: time each, keep the
         // fastest for the class; the last run's lists are the result
         float best_ms = 0.0f;
-        int best_qt = qt;
+        int best_shape = shape;
         for (size_t i = 0; i < shapes.size(); ++i) {
             KnnTasks tasks;
-            knn_tile_tasks(data, dim, tiles, inst, shapes[i], kcap, prune, tasks, s, shard);
+            knn_tile_tasks(data, dim, tiles, inst, shapes[i] / 10, kcap, prune, tasks, s, shard);
             knn_tc16_run_tasks(data, dim, kcap, scale, tiles, tasks, cand_idx, cand_d2, norms_by_row, d_err, s,
                                &last_knn_kernel_ms(), shapes[i]);
             last_knn_tiles_scanned() = tasks.total_tiles;
             UMAPB_SYNC(s);
             if (i == 0 || last_knn_kernel_ms() < best_ms) {
                 best_ms = last_knn_kernel_ms();
-                best_qt = shapes[i];
+                best_shape = shapes[i];
             }
         }
         ShapeTuner& t = shape_tuner();
         std::lock_guard<std::mutex> lock(t.mu);
-        t.best[key] = best_qt;
+        t.best[key] = best_shape;
         return;
     }
     KnnTasks tasks;
-    knn_tile_tasks(data, dim, tiles, inst, qt, kcap, prune, tasks, s, shard);
+    knn_tile_tasks(data, dim, tiles, inst, shape / 10, kcap, prune, tasks, s, shard);
     if (shard_rows) knn_task_rows(tiles, tasks, inst.back(), *shard_rows, *shard_count, s);
     knn_tc16_run_tasks(data, dim, kcap, scale, tiles, tasks, cand_idx, cand_d2, norms_by_row, d_err, s,
-                       &last_knn_kernel_ms(), qt);
+                       &last_knn_kernel_ms(), shape);
     last_knn_tiles_scanned() = tasks.total_tiles;
     UMAPB_SYNC(s);   // the tile and task buffers are released below
 }

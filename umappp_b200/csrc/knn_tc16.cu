@@ -461,11 +461,14 @@ void launch16(const Maps16& m, const float* norms, float s2, float inv_s2, int32
     UMAPB_LAUNCH_CHECK();
 }
 
-// Launch shapes (shared memory: QT * KC * 32 KB of query tiles plus
-// NS * KC * 32 KB of reference ring): KC = 1 takes two query tiles per CTA
-// with a 4-stage ring (160 KB: one CTA per SM, 512 TMEM columns) or one query
-// tile with a 2-stage ring (96 KB: two CTAs per SM, 256 columns each, tasks
-// of half the work); KC = 2 one query tile with a 2-stage ring.
+// Launch shapes, coded 10 QT + NS (shared memory: QT * KC * 32 KB of query
+// tiles plus NS * KC * 32 KB of reference ring): for KC = 1, 24 = two query
+// tiles per CTA with a 4-stage ring (160 KB: one CTA per SM, 512 TMEM
+// columns), 12 = one query tile with a 2-stage ring (96 KB: two CTAs per SM,
+// 256 columns each, tasks of half the work); KC = 2 takes 12 only.  (One
+// query tile with a 4-stage ring and one CTA per SM was measured slower than
+// both: 27.6 ms at 1M against 19.5 and 21.2 -- the two CTAs' overlapping
+// epilogues matter more than the ring's depth.)
 constexpr int qt_for(int kc) { return kc == 1 ? 2 : 1; }
 
 template <int KC, int QT, int NS>
@@ -481,7 +484,7 @@ void launch16_shape(int kcap, const Maps16& m, const float* norms, float s2, flo
 int knn_tc16_query_tiles(int32_t dim) { return qt_for((dim + 1 + H_KCHUNK - 1) / H_KCHUNK); }
 
 std::vector<int> knn_tc16_shapes(int32_t dim) {
-    return (dim + 1 + H_KCHUNK - 1) / H_KCHUNK == 1 ? std::vector<int>{2, 1} : std::vector<int>{1};
+    return (dim + 1 + H_KCHUNK - 1) / H_KCHUNK == 1 ? std::vector<int>{24, 12} : std::vector<int>{12};
 }
 
 bool knn_tc16_supported(int32_t dim, int kcap) {
@@ -512,7 +515,7 @@ float knn_tc16_scale(const float* data, size_t count, cudaStream_t s) {
 // rows for the caller.
 void knn_tc16_run_tasks(const float* data, int32_t dim, int kcap, float scale, const KnnTiles& tiles,
                         const KnnTasks& tasks, int32_t* cand_idx, float* cand_d2, float* norms_by_row, int* d_err,
-                        cudaStream_t s, float* kernel_ms, int qt) {
+                        cudaStream_t s, float* kernel_ms, int shape) {
     require(knn_tc16_supported(dim, kcap), "tensor-core kNN: unsupported dimension or candidate count");
     require(scale > 0.0f, "tensor-core kNN: no usable scale for the data");
     const int32_t n_pad = tiles.n_pad;
@@ -533,18 +536,16 @@ void knn_tc16_run_tasks(const float* data, int32_t dim, int kcap, float scale, c
     const float s2 = scale * scale, inv_s2 = 1.0f / s2;
     cudaEvent_t ev0 = event_get(), ev1 = event_get();
     UMAPB_CUDA(cudaEventRecord(ev0, s));
-    if (qt <= 0) qt = qt_for(kc);
-    require(kc == 1 ? (qt == 1 || qt == 2) : qt == 1, "tensor-core kNN: unsupported launch shape");
+    if (shape <= 0) shape = kc == 1 ? 24 : 12;
+    require(kc == 1 ? (shape == 24 || shape == 12) : shape == 12, "tensor-core kNN: unsupported launch shape");
     if (tasks.count > 0) {
-        if (kc == 1 && qt == 2)
-            launch16_shape<1, 2, 4>(kcap, m, onorm.get(), s2, inv_s2, tasks.count, tasks, tiles.row_map.get(), cand_idx,
-                                    cand_d2, d_err, s);
+        const int32_t* rm = tiles.row_map.get();
+        if (kc == 1 && shape == 24)
+            launch16_shape<1, 2, 4>(kcap, m, onorm.get(), s2, inv_s2, tasks.count, tasks, rm, cand_idx, cand_d2, d_err, s);
         else if (kc == 1)
-            launch16_shape<1, 1, 2>(kcap, m, onorm.get(), s2, inv_s2, tasks.count, tasks, tiles.row_map.get(), cand_idx,
-                                    cand_d2, d_err, s);
+            launch16_shape<1, 1, 2>(kcap, m, onorm.get(), s2, inv_s2, tasks.count, tasks, rm, cand_idx, cand_d2, d_err, s);
         else
-            launch16_shape<2, 1, 2>(kcap, m, onorm.get(), s2, inv_s2, tasks.count, tasks, tiles.row_map.get(), cand_idx,
-                                    cand_d2, d_err, s);
+            launch16_shape<2, 1, 2>(kcap, m, onorm.get(), s2, inv_s2, tasks.count, tasks, rm, cand_idx, cand_d2, d_err, s);
     }
     UMAPB_CUDA(cudaEventRecord(ev1, s));
     scatter_norms_kernel<<<grid_for(n_pad, 256), 256, 0, s>>>(tiles.row_map.get(), onorm.get(), n_pad, norms_by_row);

@@ -104,9 +104,10 @@ void knn_tile_tasks(const float* data, int32_t dim, const KnnTiles& t, const std
 // norm outputs are indexed by data row.
 void knn_tc16_run_tasks(const float* data, int32_t dim, int kcap, float scale, const KnnTiles& tiles,
                         const KnnTasks& tasks, int32_t* cand_idx, float* cand_d2, float* norms_by_row, int* d_err,
-                        cudaStream_t s, float* kernel_ms = nullptr, int qt = 0);
-// Query tiles per CTA of the launch shapes of the FP16 search for 'dim'
-// (the first is the default; the tasks must be built with the shape's count).
+                        cudaStream_t s, float* kernel_ms = nullptr, int shape = 0);
+// Launch shapes of the FP16 search for 'dim', coded 10 * query tiles per CTA +
+// reference-ring stages (the first is the default; the tasks must be built
+// with the shape's query tiles, shape / 10).
 std::vector<int> knn_tc16_shapes(int32_t dim);
 
 // FP16-operand variant (knn_tc16.cu): power-of-two scale of the data (0 when
