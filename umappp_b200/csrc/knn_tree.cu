@@ -33,6 +33,7 @@
 #include <cstdint>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "stages.cuh"
@@ -274,9 +275,10 @@ constexpr float D2_HIGH = 1.0f + 1.0e-4f;   // upper-bound factor
 // other points of the tile -- the largest over the tile's points of the
 // distance to the k-th nearest other point (FP32 sums of squares, relative
 // error below (dim + 2) 2^-24, rounded up through the D2_HIGH margins) --, or
-// infinity when the tile holds k points or fewer or k exceeds KTH_MAX.
+// infinity when the tile holds k points or fewer or k exceeds KM (<= KTH_MAX).
 // One block of TREE_LEAF threads per tile, one thread per row; the tile's
 // points are staged in shared memory ([TREE_LEAF][dim]).
+template <int KM>
 __global__ void __launch_bounds__(TREE_LEAF)
     tile_kth_kernel(const float* __restrict__ data, int32_t dim, const int32_t* __restrict__ row_map,
                     const int32_t* __restrict__ count, int32_t k, float* __restrict__ kth_out) {
@@ -285,7 +287,7 @@ __global__ void __launch_bounds__(TREE_LEAF)
     __shared__ float red[TREE_LEAF / 32];
     const int32_t g = blockIdx.x;
     const int r = threadIdx.x;
-    if (k > KTH_MAX || count[g] < k + 1) {   // uniform over the block
+    if (k > KM || count[g] < k + 1) {   // uniform over the block
         if (r == 0) kth_out[g] = CUDART_INF_F;
         return;
     }
@@ -297,9 +299,9 @@ __global__ void __launch_bounds__(TREE_LEAF)
         pts[i] = src >= 0 ? data[static_cast<size_t>(src) * dim + (i - rr * dim)] : 0.0f;
     }
     __syncthreads();
-    float top[KTH_MAX];   // the smallest squared distances so far, ascending
+    float top[KM];   // the KM smallest squared distances so far, ascending (KM >= k)
 #pragma unroll
-    for (int i = 0; i < KTH_MAX; ++i) top[i] = CUDART_INF_F;
+    for (int i = 0; i < KM; ++i) top[i] = CUDART_INF_F;
     float kth2 = 0.0f;
     if (valid[r]) {
         const float* x = pts + r * dim;
@@ -311,12 +313,13 @@ __global__ void __launch_bounds__(TREE_LEAF)
                 const float v = x[d] - y[d];
                 d2 = fmaf(v, v, d2);
             }
+            if (!(d2 < top[KM - 1])) continue;   // not among the KM nearest so far
 #pragma unroll
-            for (int i = KTH_MAX - 1; i > 0; --i) top[i] = d2 < top[i - 1] ? top[i - 1] : fminf(top[i], d2);
+            for (int i = KM - 1; i > 0; --i) top[i] = d2 < top[i - 1] ? top[i - 1] : fminf(top[i], d2);
             top[0] = fminf(top[0], d2);
         }
 #pragma unroll
-        for (int i = 0; i < KTH_MAX; ++i)
+        for (int i = 0; i < KM; ++i)
             if (i == k - 1) kth2 = top[i];
     }
     for (int o = 16; o > 0; o >>= 1) kth2 = fmaxf(kth2, __shfl_xor_sync(0xffffffffu, kth2, o));
@@ -633,12 +636,19 @@ void knn_tile_tasks(const float* data, int32_t dim, const KnnTiles& t, const std
     if (prune && k <= KTH_MAX) {
         tkth.allocate(ntiles, s);
         const size_t smem = sizeof(float) * TREE_LEAF * dim;   // dim <= MAX_TREE_DIM: 64 KB at most
-        static std::once_flag once;
-        std::call_once(once, [] {
-            UMAPB_CUDA(cudaFuncSetAttribute(tile_kth_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            static_cast<int>(sizeof(float) * TREE_LEAF * MAX_TREE_DIM)));
-        });
-        tile_kth_kernel<<<ntiles, TREE_LEAF, smem, s>>>(data, dim, t.row_map.get(), tcnt.get(), k, tkth.get());
+        // the insertion list as short as k allows
+        auto launch = [&](auto km) {
+            constexpr int KM = decltype(km)::value;
+            static std::once_flag once;
+            std::call_once(once, [] {
+                UMAPB_CUDA(cudaFuncSetAttribute(tile_kth_kernel<KM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                static_cast<int>(sizeof(float) * TREE_LEAF * MAX_TREE_DIM)));
+            });
+            tile_kth_kernel<KM><<<ntiles, TREE_LEAF, smem, s>>>(data, dim, t.row_map.get(), tcnt.get(), k, tkth.get());
+        };
+        if (k <= 16) launch(std::integral_constant<int, 16>());
+        else if (k <= 24) launch(std::integral_constant<int, 24>());
+        else launch(std::integral_constant<int, KTH_MAX>());
         UMAPB_LAUNCH_CHECK();
     }
     tile_lists_kernel<<<warps_grid, 32 * LIST_WARPS, 0, s>>>(ntiles, d_tile0.get(), d_ntl.get(), tcen_t.get(), ntiles,
