@@ -77,3 +77,120 @@ def knn_sharded(data: np.ndarray, k: int, group=None, local: Optional[Callable] 
             return local_shard(x, kk, r, w)
     rows, idx, dst = local(data, k, rank, world)
     return gather_shards(rows, idx, dst, data.shape[0], group=group, device=device)
+
+
+# ------------------------------------------------- batched instances ---
+#
+# The batched mode's instances are independent runs, so a batch splits over
+# ranks with nothing exchanged while it runs: each rank runs a balanced subset
+# of the instances in one batch_run of its own, and an optional all-gather
+# afterwards gives every rank every instance's layout.
+
+
+def partition_instances(sizes, world: int) -> list:
+    """Instances of a batch dealt to 'world' ranks: the largest first, each to
+    the rank with the fewest observations so far (ties: the lower rank), so
+    that the ranks' shares of the observations -- and of the edges the epochs
+    process, k per observation -- are balanced.  Returns one ascending int64
+    array of instance numbers per rank; the arrays partition range(len(sizes)).
+    The same on every rank (no randomness, no communication)."""
+    sizes = np.asarray(sizes, dtype=np.int64)
+    if world < 1:
+        raise ValueError("world must be at least 1")
+    if sizes.ndim != 1 or np.any(sizes < 0):
+        raise ValueError("sizes must be a 1-d array of non-negative counts")
+    load = np.zeros(world, dtype=np.int64)
+    owner = np.empty(len(sizes), dtype=np.int64)
+    for i in sorted(range(len(sizes)), key=lambda j: (-int(sizes[j]), j)):
+        r = int(np.argmin(load))
+        owner[i] = r
+        load[r] += sizes[i]
+    return [np.nonzero(owner == r)[0].astype(np.int64) for r in range(world)]
+
+
+def _take_rows(a, offs, inst):
+    """Rows of instances 'inst' of 'a' (numpy array or torch tensor), concatenated in order."""
+    parts = [a[int(offs[i]):int(offs[i + 1])] for i in inst]
+    if isinstance(a, np.ndarray):
+        return np.ascontiguousarray(np.concatenate(parts) if parts else a[:0])
+    import torch
+
+    return torch.cat(parts).contiguous() if parts else a[:0].contiguous()
+
+
+def batch_sharded(data, sizes, num_dim: int, embedding, options=None, group=None, run: Optional[Callable] = None,
+                  gather: bool = True, device=None) -> dict:
+    """A batch of independent UMAP runs (batch_run's arguments: instance i is
+    the next sizes[i] rows of 'data' and of 'embedding') split over the ranks
+    of 'group'.  Every rank holds the whole batch's data; this rank runs the
+    instances partition_instances gives it, in one call of
+    'run(data, sizes, num_dim, embedding, options)' (default: batch_run on the
+    current GPU) over their rows, and writes their layouts into 'embedding'.
+    With 'gather', one all-gather of the ranks' layouts (padded to the largest
+    share) then fills every instance's rows on every rank; without it only this
+    rank's instances are written.  Returns {"instances": this rank's instance
+    numbers, "stage_ms": run's result (None for a rank with no instances)}.
+    If any rank's run raises, every rank raises (that rank its own error, the
+    others a RuntimeError) after one all-reduce of a failure flag, so that no
+    rank is left waiting in the gather."""
+    import torch
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    sizes = np.asarray(sizes, dtype=np.int64)
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    if int(data.shape[0]) != int(offs[-1]) or int(embedding.shape[0]) != int(offs[-1]):
+        raise ValueError("data and embedding must have sum(sizes) rows")
+    shares = partition_instances(sizes, world)
+    mine = shares[rank]
+    if run is None:
+        from . import batch_run as run
+    stage_ms = None
+    local = None
+    error = None
+    if len(mine):
+        try:
+            sub_data = _take_rows(data, offs, mine)
+            local = _take_rows(embedding, offs, mine)
+            stage_ms = run(sub_data, sizes[mine], num_dim, local, options)
+            pos = 0
+            for i in mine:
+                m = int(sizes[i])
+                embedding[int(offs[i]):int(offs[i]) + m] = local[pos:pos + m]
+                pos += m
+        except Exception as e:  # reported after every rank has learnt of it
+            error = e
+    if device is None and world > 1:
+        device = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" \
+            else torch.device("cpu")
+    if world > 1:
+        # every rank takes the same collectives: first whether any rank failed
+        failed = torch.tensor([1 if error is not None else 0], dtype=torch.int32, device=device)
+        dist.all_reduce(failed, op=dist.ReduceOp.MAX, group=group)
+        if int(failed.item()):
+            if error is not None:
+                raise error
+            raise RuntimeError("batch_sharded: another rank's instances failed")
+    elif error is not None:
+        raise error
+    if gather and world > 1:
+        rows = [int(sizes[s].sum()) for s in shares]
+        m = max(rows + [1])
+        is_np = isinstance(embedding, np.ndarray)
+        tdtype = torch.from_numpy(np.zeros(1, dtype=embedding.dtype)).dtype if is_np else embedding.dtype
+        buf = torch.zeros((m, num_dim), dtype=tdtype, device=device)
+        if local is not None and rows[rank]:
+            buf[:rows[rank]] = torch.as_tensor(local, device=device).reshape(rows[rank], num_dim)
+        parts = [torch.empty_like(buf) for _ in range(world)]
+        dist.all_gather(parts, buf, group=group)
+        for r in range(world):
+            if r == rank:
+                continue
+            blk = parts[r].cpu().numpy() if is_np else parts[r].to(embedding.device)
+            pos = 0
+            for i in shares[r]:
+                n_i = int(sizes[i])
+                embedding[int(offs[i]):int(offs[i]) + n_i] = blk[pos:pos + n_i]
+                pos += n_i
+    return {"instances": mine, "stage_ms": stage_ms}
