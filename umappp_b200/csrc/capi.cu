@@ -3,6 +3,7 @@
 // (include/umappp/initialize.hpp:69-177, include/umappp/Status.hpp:25-141)
 // driven as a sequence of device stages on one CUDA stream per status.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cmath>
 #include <cstring>
@@ -126,19 +127,41 @@ namespace umapb {
 namespace {
 
 enum Stage { ST_KNN = 0, ST_SIM, ST_UNION, ST_INIT, ST_EPOCHS, ST_SCHEDULE, ST_SGD };
+const char* const STAGE_RANGE[] = {"umapb knn", "umapb similarities", "umapb union", "umapb init",
+                                   "umapb epochs", "umapb schedule", "umapb sgd"};
 
-// Event pair per stage, resolved at the end of a call.
+// An NVTX range on the calling host thread for the life of the object: the
+// stages and calls show by name on a profiler's timeline (and ncu can filter
+// on them with --nvtx); without a tool attached the calls return at once.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
+// Event pair per stage, resolved at the end of a call; each stage is also an
+// NVTX range (closed by end(), or by the destructor when a stage throws).
 struct StageTimer {
     cudaStream_t s;
     float* out;
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
+    int open = 0;
     explicit StageTimer(cudaStream_t st, float* o) : s(st), out(o) {}
     void begin(int stage) {
         cudaEvent_t a = event_get(), b = event_get();
         UMAPB_CUDA(cudaEventRecord(a, s));
         marks.push_back({stage, {a, b}});
+        nvtxRangePushA(STAGE_RANGE[stage]);
+        ++open;
     }
-    void end() { UMAPB_CUDA(cudaEventRecord(marks.back().second.second, s)); }
+    void end() {
+        if (open > 0) {
+            nvtxRangePop();
+            --open;
+        }
+        UMAPB_CUDA(cudaEventRecord(marks.back().second.second, s));
+    }
     void resolve() {
         UMAPB_SYNC(s);
         for (auto& m : marks) {
@@ -148,6 +171,7 @@ struct StageTimer {
         }
     }
     ~StageTimer() {
+        for (; open > 0; --open) nvtxRangePop();
         for (auto& m : marks) {
             event_put(m.second.first);
             event_put(m.second.second);
@@ -733,6 +757,7 @@ int umapb_status_run(umapb_status* st, void* embedding, int epoch_limit) {
     return guarded([&] {
         require(st != nullptr && st->impl, "invalid status");
         UMAPB_CUDA(cudaSetDevice(st->device));
+        NvtxRange range("umapb run");
         st->impl->run(embedding, epoch_limit < 0 ? st->num_epochs : epoch_limit);
     });
 }
