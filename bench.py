@@ -123,6 +123,23 @@ def sgd_roofline(nnz: int, epochs: int, firing: float, negs: float, sgd_ms: floa
                     "the fraction of the ceiling that binds"}
 
 
+def stage_rooflines(n: int, k: int, nnz: int, stages: dict, peaks: dict, float_bytes: int = 4) -> dict:
+    """HBM fractions of the two small graph stages by their algorithmic bytes:
+    similarities n k (4 read + 4 write) + 16 n (rho and sigma in FP64);
+    union n k 8 read (index and weight) + nnz 8 + (n + 1) 8 written (the CSR
+    out; its sort passes are not counted).  nnz is the stored edges after the
+    epochs filter, within 0.1 % of the union's output at the benchmark sizes."""
+    out = {}
+    for name, nbytes in (("similarities", n * k * (2 * float_bytes) + 16 * n),
+                         ("union", n * k * (4 + float_bytes) + nnz * (4 + float_bytes) + (n + 1) * 8)):
+        ms = float(stages.get(name, 0.0))
+        gbs = nbytes / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
+        out[name] = {"bound": "hbm", "achieved": round(gbs, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": round(gbs / peaks["hbm_gbs"], 4), "algorithmic_bytes": int(nbytes),
+                     "time_ms": round(ms, 3)}
+    return out
+
+
 def load_peaks() -> dict:
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -292,6 +309,7 @@ def run_ours(args, rank: int, world: int) -> dict | None:
         "roofline": dominant,
         "roofline_knn": roof_knn,
         "roofline_sgd": roof_sgd,
+        "roofline_stages": stage_rooflines(n, k, nnz, stages, peaks),
         "e2e": {"value": round(e2e_ms / 1e3, 4), "unit": "s", "h2d_bytes_per_step": int(n * dim * 4 + n * 2 * 4),
                 "d2h_bytes_per_step": int(2 * n * 2 * 4)},
         "gpu_launches": int(launches // max(args.steps, 1)),

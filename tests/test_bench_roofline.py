@@ -21,3 +21,18 @@ def test_sgd_roofline_reproduces_a_measured_line():
     assert r["traffic"] == 610_600_000.0
     expect = (4 * 25_953_500 * 200 + 56 * 1_449_480_438 + 8 * 7_226_298_288) / 200
     assert abs(r["algorithmic_bytes_per_launch"] - expect) <= 1
+
+
+def test_stage_rooflines_bytes_and_fractions():
+    peaks = {"hbm_gbs": 6454.3, "source": "measured"}
+    r = bench.stage_rooflines(1_000_000, 15, 25_953_500, {"similarities": 2.108, "union": 2.523}, peaks)
+    json.dumps(r)
+    sim, uni = r["similarities"], r["union"]
+    assert sim["algorithmic_bytes"] == 1_000_000 * 15 * 8 + 16 * 1_000_000
+    assert uni["algorithmic_bytes"] == 1_000_000 * 15 * 8 + 25_953_500 * 8 + 1_000_001 * 8
+    for x in (sim, uni):
+        assert x["bound"] == "hbm" and x["unit"] == "GB/s"
+        assert abs(x["achieved"] - x["algorithmic_bytes"] / (x["time_ms"] * 1e-3) / 1e9) <= 0.1
+        assert abs(x["frac"] - x["achieved"] / 6454.3) <= 1e-4
+    # a stage that did not run reports zero, not a division error
+    assert bench.stage_rooflines(10, 3, 20, {}, peaks)["union"]["achieved"] == 0.0
