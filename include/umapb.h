@@ -89,15 +89,20 @@ typedef struct umapb_options {
 /* Fills the reference's defaults (Options.hpp:37-218). */
 void umapb_options_init(umapb_options* opt);
 
-/* Message of the last failing call on this thread ("" if none). */
+/* Message of the last failing call on this thread ("" if none).  The reference
+ * throws C++ exceptions instead (e.g. include/umappp/optimize_layout.hpp:29,89);
+ * here every call returns a status code and leaves its message here. */
 const char* umapb_last_error(void);
 
+/* Version of this library.  No reference counterpart (a header-only library). */
 int umapb_version(void);
 
-/* sizeof(umapb_options), for bindings that mirror the struct. */
+/* sizeof(umapb_options), for bindings that mirror the struct.  No reference
+ * counterpart: a binding check. */
 size_t umapb_options_size(void);
 
-/* Number of kernels this library has launched in this process (all threads). */
+/* Number of kernels this library has launched in this process (all threads).
+ * No reference counterpart: a measurement hook. */
 int64_t umapb_launch_count(void);
 
 /*
@@ -171,7 +176,8 @@ int umapb_initialize_knn_matrix(int dtype, int32_t num_obs, int32_t k, const int
 
 /*
  * A neighbour-search index resident on the device, the role of
- * knncolle::Prebuilt: the data (num_obs x data_dim of dtype, observation i at
+ * knncolle::Prebuilt that include/umappp/initialize.hpp:138-142 takes: the data
+ * (num_obs x data_dim of dtype, observation i at
  * [i * data_dim, (i + 1) * data_dim)) copied to the current device once and
  * searched by every umapb_initialize_prebuilt, without copying it again.
  */
@@ -200,8 +206,12 @@ int umapb_status_epoch(const umapb_status* st);                 /* Status.hpp:63
 int umapb_status_num_epochs(const umapb_status* st);            /* Status.hpp:71-73 */
 int32_t umapb_status_num_observations(const umapb_status* st);  /* Status.hpp:78-80 */
 size_t umapb_status_num_dimensions(const umapb_status* st);     /* Status.hpp:56-58 */
-double umapb_status_a(const umapb_status* st);                  /* the a and b in use */
+/* The a and b in use: Options::a / Options::b (Options.hpp:79,87) or the fit of
+ * find_ab.hpp:44-168 made by initialize (initialize.hpp:105-110). */
+double umapb_status_a(const umapb_status* st);
 double umapb_status_b(const umapb_status* st);
+/* Edges of the status' EpochData, the last entry of cumulative_num_edges
+ * (optimize_layout.hpp:27-45). */
 int64_t umapb_status_num_edges(const umapb_status* st);
 
 /*
@@ -217,16 +227,21 @@ int umapb_status_get_epoch_data(const umapb_status* st, int64_t* row_ptr, int32_
  * Exact per-epoch counts of the deterministic schedule over [first, last):
  * counts[2 * e] = firing edges, counts[2 * e + 1] = negative samples drawn
  * (self-samples included, as the reference draws and then skips them).
+ * No reference counterpart: the counts of the schedule that
+ * optimize_layout.hpp:136-180 walks, for measurement and checks.
  */
 int umapb_status_schedule_counts(const umapb_status* st, int first, int last, int64_t* counts);
 
 /*
  * Device milliseconds of the stages of the last initialize / run on this
  * status, in the order: knn, similarities, union, init, epochs, schedule,
- * sgd.  'count' entries are written (at most 7).
+ * sgd.  'count' entries are written (at most 7).  No reference counterpart:
+ * a measurement hook.
  */
 int umapb_status_stage_ms(const umapb_status* st, double* ms, int count);
 
+/* Releases the status and its device state (the end of a umappp::Status,
+ * Status.hpp:25-141). */
 void umapb_status_free(umapb_status* st);
 
 /* ----------------------------------------------------------- stage entries */
@@ -239,6 +254,9 @@ void umapb_status_free(umapb_status* st);
  * split-precision tensor-core distances and the k-th boundary is rescored in
  * FP64; for F64 data distances are computed in FP64.  k must be below num_obs.
  */
+int umapb_knn(int dtype, size_t data_dim, int32_t num_obs, const void* data, int k, int32_t* out_indices,
+              void* out_distances);
+
 /*
  * One shard of umapb_knn, for a neighbour search split across GPUs (every
  * rank holds the whole data and computes its shard; an all-gather of the
@@ -255,9 +273,6 @@ void umapb_status_free(umapb_status* st);
 int umapb_knn_shard(int dtype, size_t data_dim, int32_t num_obs, const void* data, int k, int32_t shard,
                     int32_t num_shards, int32_t* out_rows, int32_t* out_indices, void* out_distances,
                     int32_t* out_count);
-
-int umapb_knn(int dtype, size_t data_dim, int32_t num_obs, const void* data, int k, int32_t* out_indices,
-              void* out_distances);
 
 /* Exact Euclidean neighbours of num_query query points among num_ref reference
  * points (row-major data_dim columns each): out_indices / out_distances are
@@ -285,10 +300,13 @@ int umapb_knn_query(int dtype, size_t data_dim, int32_t num_ref, const void* ref
 int umapb_transform(int dtype, size_t data_dim, int32_t num_ref, const void* ref_data, const void* ref_embedding,
                     int32_t num_new, const void* new_data, size_t num_dim, const umapb_options* options,
                     int num_epochs, void* new_embedding);
+/* The epoch count umapb_transform uses for these arguments (an extension, as
+ * umapb_transform). */
 int umapb_transform_epochs(const umapb_options* options, int num_epochs, int32_t num_new);
 
 /* Queries of the last F32 neighbour search in this process whose candidate
- * set could not be certified by the error bound and were recomputed in FP64. */
+ * set could not be certified by the error bound and were recomputed in FP64.
+ * No reference counterpart: a diagnostic of the search. */
 int umapb_knn_last_fp64_recomputed(void);
 
 /* Largest error of the tensor-core squared distances of the last float kNN
