@@ -202,10 +202,10 @@ int umapb_initialize_prebuilt(const umapb_prebuilt* prebuilt, size_t num_dim, vo
  */
 int umapb_status_run(umapb_status* st, void* embedding, int epoch_limit);
 
-int umapb_status_epoch(const umapb_status* st);                 /* Status.hpp:63-65 */
-int umapb_status_num_epochs(const umapb_status* st);            /* Status.hpp:71-73 */
-int32_t umapb_status_num_observations(const umapb_status* st);  /* Status.hpp:78-80 */
-size_t umapb_status_num_dimensions(const umapb_status* st);     /* Status.hpp:56-58 */
+int umapb_status_epoch(const umapb_status* st);                 /* Status.hpp:70-72 */
+int umapb_status_num_epochs(const umapb_status* st);            /* Status.hpp:78-80 */
+int32_t umapb_status_num_observations(const umapb_status* st);  /* Status.hpp:85-87 */
+size_t umapb_status_num_dimensions(const umapb_status* st);     /* Status.hpp:63-65 */
 /* The a and b in use: Options::a / Options::b (Options.hpp:79,87) or the fit of
  * find_ab.hpp:44-168 made by initialize (initialize.hpp:105-110). */
 double umapb_status_a(const umapb_status* st);

@@ -39,17 +39,21 @@ public:
         : my_handle(handle, &umapb_status_free), my_rate(negative_sample_rate) {}
     /** @endcond */
 
+    /** Status::num_dimensions() (Status.hpp:63-65). */
     std::size_t num_dimensions() const { return umapb_status_num_dimensions(my_handle.get()); }
+    /** Status::epoch() (Status.hpp:70-72): epochs completed so far. */
     int epoch() const { return umapb_status_epoch(my_handle.get()); }
+    /** Status::num_epochs() (Status.hpp:78-80). */
     int num_epochs() const { return umapb_status_num_epochs(my_handle.get()); }
+    /** Status::num_observations() (Status.hpp:85-87). */
     Index_ num_observations() const { return static_cast<Index_>(umapb_status_num_observations(my_handle.get())); }
 
-    /** Status::run(embedding, epoch_limit): advances to epoch_limit. */
+    /** Status::run(embedding, epoch_limit) (Status.hpp:101-128): advances to epoch_limit. */
     void run(Float_* const embedding, int epoch_limit) {
         detail::check(umapb_status_run(my_handle.get(), embedding, epoch_limit));
     }
 
-    /** Status::run(embedding): advances to num_epochs(). */
+    /** Status::run(embedding) (Status.hpp:138-140): advances to num_epochs(). */
     void run(Float_* const embedding) { run(embedding, num_epochs()); }
 
     /** The schedule at the current epoch (a copy; the reference returns a reference). */

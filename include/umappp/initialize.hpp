@@ -58,6 +58,12 @@ private:
     umapb_prebuilt* pb_ = nullptr;
 };
 
+/**
+ * initialize(NeighborList x, num_dim, embedding, Options)
+ * (include/umappp/initialize.hpp:69-119): similarities, union, initial layout
+ * and epoch schedule on the device; the initial layout is written to
+ * 'embedding' (n x num_dim, row-major) as in the reference.
+ */
 template <typename Index_, typename Float_>
 Status<Index_, Float_> initialize(const NeighborList<Index_, Float_>& x, const std::size_t num_dim, Float_* const embedding,
                                   Options options) {
@@ -69,6 +75,12 @@ Status<Index_, Float_> initialize(const NeighborList<Index_, Float_>& x, const s
     return Status<Index_, Float_>(st, options.negative_sample_rate);
 }
 
+/**
+ * initialize(data_dim, num_obs, data, builder, num_dim, embedding, Options)
+ * (include/umappp/initialize.hpp:165-177) with the device's exact Euclidean
+ * neighbour search as the builder (data: observation i at
+ * [i * data_dim, (i + 1) * data_dim)).
+ */
 template <typename Index_, typename Float_>
 Status<Index_, Float_> initialize(const std::size_t data_dim, const Index_ num_obs, const Float_* const data,
                                   const DeviceBuilder&, const std::size_t num_dim, Float_* const embedding,
