@@ -167,7 +167,9 @@ void combine_neighbor_sets(int32_t n, const int64_t* ptr, const int32_t* idx, co
     UMAPB_CUDA(cudaMemcpyAsync(&last_keep, keep.get() + (m - 1), sizeof(int), cudaMemcpyDeviceToHost, s));
     UMAPB_CUDA(cudaMemcpyAsync(&st, status.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
     UMAPB_SYNC(s);
-    require(st == DEV_OK, "neighbour list has an out-of-range index, a self edge or a duplicate neighbour");
+    require(st == DEV_OK,
+            "neighbour list has an out-of-range index, a self edge or a duplicate neighbour (when the list comes from "
+            "a neighbour search of the data: a NaN or infinite coordinate leaves rows without neighbours, index -1)");
     const int64_t nnz = last_pos + last_keep;
 
     out.nnz = nnz;
