@@ -88,3 +88,16 @@ def test_cpp_dropin_headers_compile(umap, tmp_path):
     # user code written for the reference's API compiles and links against the GPU headers
     _compile_quickstart(str(tmp_path / "quickstart"))
     assert (tmp_path / "quickstart").exists()
+
+
+def test_cpp_extension_headers_compile(umap, tmp_path):
+    # batch_run and loss_grad through the C++ headers: compiled and linked here, run on a GPU only
+    import subprocess
+    src = os.path.join(ROOT, "tests", "cpp", "extensions.cpp")
+    out = str(tmp_path / "extensions")
+    cmd = ["g++", "-std=c++17", "-O1", "-Wall", "-Werror", "-I" + os.path.join(ROOT, "include"), src,
+           "-L" + os.path.join(ROOT, "umappp_b200"), "-lumappp_b200",
+           "-Wl,-rpath," + os.path.join(ROOT, "umappp_b200"), "-o", out]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert os.path.exists(out)
