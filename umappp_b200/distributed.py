@@ -15,6 +15,36 @@ from typing import Callable, Optional
 import numpy as np
 
 
+def _collective_device(group, device):
+    import torch
+    import torch.distributed as dist
+
+    if device is not None:
+        return device
+    return torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" \
+        else torch.device("cpu")
+
+
+def agree_on_failure(error: Optional[BaseException], group=None, device=None) -> None:
+    """One all-reduce of a failure flag over the ranks of 'group', taken by
+    every rank whether or not its own step failed, so that no rank is left
+    waiting in a later collective: if any rank failed, every rank raises --
+    the failing rank its own error, the others a RuntimeError."""
+    import torch
+    import torch.distributed as dist
+
+    if dist.get_world_size(group) <= 1:
+        if error is not None:
+            raise error
+        return
+    failed = torch.tensor([1 if error is not None else 0], dtype=torch.int32, device=_collective_device(group, device))
+    dist.all_reduce(failed, op=dist.ReduceOp.MAX, group=group)
+    if int(failed.item()):
+        if error is not None:
+            raise error
+        raise RuntimeError("another rank's step failed")
+
+
 def gather_shards(rows: np.ndarray, indices: np.ndarray, distances: np.ndarray, num_obs: int, group=None,
                   device=None):
     """All-gather every rank's (rows, indices, distances) block and assemble
@@ -75,8 +105,30 @@ def knn_sharded(data: np.ndarray, k: int, group=None, local: Optional[Callable] 
 
         def local(x, kk, r, w):
             return local_shard(x, kk, r, w)
-    rows, idx, dst = local(data, k, rank, world)
+    error = None
+    try:
+        rows, idx, dst = local(data, k, rank, world)
+    except Exception as e:  # reported after every rank has learnt of it
+        error = e
+    agree_on_failure(error, group, device)
     return gather_shards(rows, idx, dst, data.shape[0], group=group, device=device)
+
+
+def initialize_sharded(data, num_dim: int, embedding, options=None, group=None, local: Optional[Callable] = None,
+                       init: Optional[Callable] = None, device=None):
+    """initialize(data, builder, ...) of one data set with the neighbour
+    search split over the ranks of 'group': knn_sharded for
+    options.num_neighbors neighbours, then, on every rank, the rest of the
+    pipeline from the gathered lists by 'init(indices, distances, num_dim,
+    embedding, options)' (default: initialize_knn_matrix on the current GPU).
+    Every rank returns its own Status over the same graph; the stages after
+    the search replicate (each SGD step gathers random embedding rows)."""
+    from . import Options
+    from . import initialize_knn_matrix
+
+    options = options or Options()
+    idx, dst = knn_sharded(data, options.num_neighbors, group=group, local=local, device=device)
+    return (init or initialize_knn_matrix)(idx, dst, num_dim, embedding, options)
 
 
 # ------------------------------------------------- batched instances ---
@@ -161,20 +213,9 @@ def batch_sharded(data, sizes, num_dim: int, embedding, options=None, group=None
                 pos += m
         except Exception as e:  # reported after every rank has learnt of it
             error = e
-    if device is None and world > 1:
-        device = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" \
-            else torch.device("cpu")
-    if world > 1:
-        # every rank takes the same collectives: first whether any rank failed
-        failed = torch.tensor([1 if error is not None else 0], dtype=torch.int32, device=device)
-        dist.all_reduce(failed, op=dist.ReduceOp.MAX, group=group)
-        if int(failed.item()):
-            if error is not None:
-                raise error
-            raise RuntimeError("batch_sharded: another rank's instances failed")
-    elif error is not None:
-        raise error
+    agree_on_failure(error, group, device)
     if gather and world > 1:
+        device = _collective_device(group, device)
         rows = [int(sizes[s].sum()) for s in shares]
         m = max(rows + [1])
         is_np = isinstance(embedding, np.ndarray)
