@@ -5,8 +5,10 @@ computes its shard of the exact kNN (umapb_knn_shard: a balanced range of the
 search's tree-ordered query tiles), and one all-gather of the shards' rows
 gives every rank the full neighbour lists, from which each rank can continue
 with initialize_knn_matrix (the later stages replicate: every SGD step gathers
-random embedding rows).  The collective is torch.distributed's all_gather --
-NCCL between GPUs, gloo on CPUs -- over tensors padded to the largest shard.
+random embedding rows).  The collectives are torch.distributed's -- NCCL
+between GPUs, gloo on CPUs: one all-reduce of a failure flag (a search that
+raises on one rank raises on all) and one all_gather of the rows, indices and
+distances, padded to the largest shard.
 """
 from __future__ import annotations
 
