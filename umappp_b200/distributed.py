@@ -1,6 +1,7 @@
-"""The neighbour search split across ranks (one process per GPU).
+"""Work split across ranks (one process per GPU): the neighbour search of one
+data set, and the instances of a batch (at the end of this file).
 
-The only stage of the pipeline that shards: every rank holds the whole data,
+The search is the only stage of a single run that shards: every rank holds the whole data,
 computes its shard of the exact kNN (umapb_knn_shard: a balanced range of the
 search's tree-ordered query tiles), and one all-gather of the shards' rows
 gives every rank the full neighbour lists, from which each rank can continue
